@@ -1,0 +1,90 @@
+"""Runs the compiled reference oracle (oracle/_ref/ref_<NS>x<NT>_l<LEVELS>) on given inputs.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by tests/golden/make_golden.py and by the
+CPU-baseline leg of bench.py; never by the product package.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REF_DIR = HERE / "_ref"
+
+
+def binary(ns: int, nt: int, levels: int) -> Path:
+    return REF_DIR / f"ref_{ns}x{nt}_l{levels}"
+
+
+def build(ns: int, nt: int, levels: int, refdir: str = "/root/reference") -> Path:
+    b = binary(ns, nt, levels)
+    if not b.exists():
+        subprocess.run([str(HERE / "build_ref.sh"), str(ns), str(nt), str(levels), refdir],
+                       check=True, capture_output=True)
+    return b
+
+
+def params_text(rows) -> str:
+    return "\n".join(" ".join(str(int(v)) for v in r) for r in rows) + "\n"
+
+
+def read_outputs(workdir: Path) -> dict:
+    out = {}
+    man = workdir / "manifest.txt"
+    if man.exists():
+        for line in man.read_text().split("\n"):
+            if not line.strip():
+                continue
+            name, dt, *shape = line.split()
+            dtype = {"c16": np.complex128, "i4": np.int32}[dt]
+            a = np.fromfile(workdir / f"{name}.bin", dtype=dtype)
+            out[name] = a.reshape([int(s) for s in shape])
+    info = workdir / "info.txt"
+    if info.exists():
+        for line in info.read_text().split("\n"):
+            if line.strip():
+                k, v = line.split()
+                out["info:" + k] = float(v)
+    return out
+
+
+def run(ns: int, nt: int, rows, gauge: np.ndarray, rhs: np.ndarray, *, m0: float,
+        cycle: int = 1, nit: int = 0, sap_tv_iters: int = 4, nu1: int = 0, nu2: int = 2,
+        solve: int = 1, phases: int = 0, dump_hierarchy: int = 1, dphi_reps: int = 0,
+        dphi_only: int = 0, probes=None, workdir: str | None = None, timeout: float = 3600) -> dict:
+    """Writes the job, runs the binary for (ns, nt, len(rows)+1 levels), returns its dumps."""
+    levels = len(rows) + 1
+    b = binary(ns, nt, levels)
+    if not b.exists():
+        raise FileNotFoundError(f"{b} not built (oracle/build_ref.sh {ns} {nt} {levels})")
+    tmp = None
+    if workdir is None:
+        tmp = tempfile.TemporaryDirectory(prefix="oracle_")
+        workdir = tmp.name
+    wd = Path(workdir)
+    wd.mkdir(parents=True, exist_ok=True)
+    (wd / "params.dat").write_text(params_text(rows))
+    job = dict(m0=repr(float(m0)), cycle=cycle, nit=nit, sap_tv_iters=sap_tv_iters, nu1=nu1,
+               nu2=nu2, solve=solve, phases=phases, dump_hierarchy=dump_hierarchy,
+               dphi_reps=dphi_reps, dphi_only=dphi_only)
+    (wd / "job.txt").write_text("".join(f"{k} {v}\n" for k, v in job.items()))
+    np.ascontiguousarray(gauge, dtype=np.complex128).tofile(wd / "gauge.bin")
+    np.ascontiguousarray(rhs, dtype=np.complex128).tofile(wd / "rhs.bin")
+    for l, p in (probes or {}).items():
+        np.ascontiguousarray(p, dtype=np.complex128).tofile(wd / f"probe_l{l}.bin")
+    proc = subprocess.run([str(b), str(wd)], cwd=str(wd), capture_output=True, text=True,
+                          timeout=timeout)
+    if proc.returncode != 0:
+        raise RuntimeError(f"oracle failed ({proc.returncode}): {proc.stderr[-2000:]}")
+    out = read_outputs(wd)
+    out["stdout"] = proc.stdout
+    res = list(wd.glob("Residuals_FGMRES_*.res"))
+    if res:
+        out["residual_history"] = np.loadtxt(res[0])[:, 1].reshape(-1)
+    if tmp is not None:
+        tmp.cleanup()
+    return out

@@ -1,0 +1,86 @@
+"""Generates the golden fixtures in this directory from the compiled reference oracle.
+
+Run in a container that has the reference sources (it builds oracle/_ref binaries with
+oracle/build_ref.sh) from the repository root:
+
+    python tests/golden/make_golden.py
+
+Each fixture is one .npz holding the inputs (gauge field, source, probe vectors) and the
+reference's outputs on them: index maps, D_phi / D_dagger_phi, the set-up hierarchy (test
+vectors and coarse links), per-level operator / P / P^dagger / SAP / GMRES probes, one
+preconditioner application, and the outer solve (x, iteration count, residual history).
+Large arrays are dropped for the bigger lattices to keep the files small.
+"""
+from __future__ import annotations
+
+import json
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+
+from amg_schwingermodel_b200.inputs import gauge_field, gaussian_spinor  # noqa: E402
+from oracle import ref_runner  # noqa: E402
+from oracle.restatement import read_parameters  # noqa: E402
+
+CONFIGS = {
+    # name: (ns, rows, beta, m0, seed, job overrides, keep large arrays)
+    "c16_l2_k": (16, [[0, 4, 4, 4, 2, 2]], 2.0, -0.1, 11, {}, True),
+    "c32_l3_k": (32, [[0, 4, 4, 8, 4, 4], [1, 2, 2, 8, 2, 2]], 3.0, -0.1, 12, {}, True),
+    "c32_l3_v_nu1": (32, [[0, 4, 4, 8, 4, 4], [1, 2, 2, 8, 2, 2]], 3.0, -0.1, 13,
+                     {"cycle": 0, "nu1": 1}, False),
+    "c32_l3_k_nit1": (32, [[0, 4, 4, 6, 2, 2], [1, 2, 2, 6, 2, 2]], 2.0, -0.1, 14, {"nit": 1}, False),
+    "c64_l2_k": (64, [[0, 8, 8, 10, 4, 4]], 2.0, -0.1, 1, {}, False),
+    "c64_l4_k": (64, [[0, 8, 8, 8, 4, 4], [1, 4, 4, 8, 4, 4], [2, 2, 2, 8, 2, 2]], 4.0, -0.05, 15, {}, False),
+}
+
+SMALL_KEYS_ALWAYS = ("dphi", "ddagphi", "x", "cycle0_rhs")
+
+
+def make(name: str, cfg) -> dict:
+    ns, rows, beta, m0, seed, over, keep_large = cfg
+    lps = read_parameters(ns, ns, rows)
+    L = len(lps)
+    ref_runner.build(ns, ns, L)
+    U = gauge_field(ns, ns, beta, seed)
+    b = gaussian_spinor(ns * ns, 2, seed + 1000)
+    probes = {l: gaussian_spinor(lp.n, lp.dof, seed + 2000 + l) for l, lp in enumerate(lps)}
+    job = dict(cycle=1, nit=0, nu1=0, nu2=2, sap_tv_iters=4)
+    job.update(over)
+    out = ref_runner.run(ns, ns, rows, U, b, m0=m0, phases=1, probes=probes, **job)
+    arrays = {"gauge": U, "rhs": b}
+    for l, p in probes.items():
+        arrays[f"probe_l{l}"] = p
+    for k, v in out.items():
+        if not isinstance(v, np.ndarray) or k.startswith("init_tv"):
+            continue
+        if not keep_large and k.startswith("tv_l"):
+            continue
+        if not keep_large and k.startswith(("g1_l", "g2_l", "g3_l")) and v.nbytes > 300_000:
+            continue
+        arrays[k] = v
+    meta = dict(ns=ns, nt=ns, rows=rows, beta=beta, m0=m0, seed=seed, job=job,
+                iterations=int(out["info:iterations"]),
+                true_rel_residual=out["info:true_rel_residual"],
+                sap_ret={l: int(out.get(f"info:sap_ret_l{l}", -1)) for l in range(L - 1)},
+                gmres_iters={l: int(out.get(f"info:gmres_iters_l{l}", -1)) for l in range(1, L)},
+                kfgmres1_iters=int(out.get("info:kfgmres1_iters", -1)))
+    arrays["meta"] = np.array(json.dumps(meta))
+    return arrays
+
+
+def main(names=None):
+    here = Path(__file__).resolve().parent
+    for name, cfg in CONFIGS.items():
+        if names and name not in names:
+            continue
+        arrays = make(name, cfg)
+        np.savez_compressed(here / f"{name}.npz", **arrays)
+        print(name, (here / f"{name}.npz").stat().st_size // 1024, "KiB")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1:])
