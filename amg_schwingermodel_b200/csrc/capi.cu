@@ -1,0 +1,1305 @@
+// Host side of libschwinger_amg.so: the solver context, the set-up phase, the fine-level
+// cycle, the outer FGMRES and the C ABI declared in include/schwinger_amg.h.
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <complex>
+#include <cstdarg>
+#include <cstring>
+#include <fstream>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "kernels.h"
+#include "../../include/schwinger_amg.h"
+
+namespace amgb {
+
+static thread_local std::string g_last_error;
+void set_last_error(const char* msg, const char* file, int line) {
+    g_last_error = std::string(msg) + " (" + file + ":" + std::to_string(line) + ")";
+}
+static int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+#define CK(expr)                                                                   \
+    do {                                                                           \
+        cudaError_t _e = (expr);                                                   \
+        if (_e != cudaSuccess) {                                                   \
+            set_last_error(cudaGetErrorString(_e), __FILE__, __LINE__);            \
+            return _e == cudaErrorMemoryAllocation ? AMG_ERR_NOMEM : AMG_ERR_CUDA; \
+        }                                                                          \
+    } while (0)
+#define CKR(expr)              \
+    do {                       \
+        int _r = (expr);       \
+        if (_r < 0) return _r; \
+    } while (0)
+#define CKL()  CK(cudaGetLastError())
+
+// ---------------------------------------------------------------------------------
+// level geometry (readParameters, include/params.h:17-69; Level, include/level.h:147-157;
+// SAP_C::SchwarzBlocks, src/sap.cpp:3-39)
+// ---------------------------------------------------------------------------------
+struct LevelHost {
+    int nx, nt, n, colors, K;
+    int coarsest;
+    int bx = 1, bt = 1, xe = 1, te = 1, ntest = 1;
+    int sbx = 1, sbt = 1, sxe = 1, ste = 1, ncol = 1;
+    std::vector<int> red, black;
+};
+
+static int build_levels(int nx, int nt, int L, const int* rows, std::vector<LevelHost>& lv) {
+    if (L < 2 || L > kMaxLevels) return fail(AMG_ERR_INVALID, "levels must be in [2, %d], got %d", kMaxLevels, L);
+    if (nx < 2 || nt < 2) return fail(AMG_ERR_INVALID, "lattice %dx%d too small", nx, nt);
+    if (!rows) return fail(AMG_ERR_INVALID, "no parameter rows");
+    std::vector<std::array<int, 6>> r(L - 1);
+    std::vector<int> seen(L - 1, 0);
+    for (int i = 0; i < L - 1; i++) {
+        int l = rows[6 * i];
+        if (l < 0 || l >= L - 1) return fail(AMG_ERR_INVALID, "parameter row %d names level %d", i, l);
+        for (int k = 0; k < 6; k++) r[l][k] = rows[6 * i + k];
+        seen[l]++;
+    }
+    for (int l = 0; l < L - 1; l++)
+        if (seen[l] != 1) return fail(AMG_ERR_INVALID, "level %d needs exactly one parameter row", l);
+    lv.assign(L, LevelHost{});
+    for (int l = 0; l < L; l++) {
+        LevelHost& h = lv[l];
+        h.nx = l == 0 ? nx : r[l - 1][1];
+        h.nt = l == 0 ? nt : r[l - 1][2];
+        h.colors = l == 0 ? 1 : r[l - 1][3];
+        h.K = 2 * h.colors;
+        h.n = h.nx * h.nt;
+        h.coarsest = (l == L - 1);
+        if (h.coarsest) continue;
+        h.bx = r[l][1]; h.bt = r[l][2]; h.ntest = r[l][3]; h.sbx = r[l][4]; h.sbt = r[l][5];
+        if (h.bx <= 0 || h.bt <= 0 || h.ntest <= 0 || h.sbx <= 0 || h.sbt <= 0)
+            return fail(AMG_ERR_INVALID, "level %d: non-positive blocking", l);
+        if (h.nx % h.bx || h.nt % h.bt)
+            return fail(AMG_ERR_INVALID, "level %d: %dx%d lattice not divisible into %dx%d blocks", l, h.nx, h.nt, h.bx, h.bt);
+        if (h.nx % h.sbx || h.nt % h.sbt)
+            return fail(AMG_ERR_INVALID, "level %d: %dx%d lattice not divisible into %dx%d SAP blocks", l, h.nx, h.nt,
+                        h.sbx, h.sbt);
+        if (h.ntest > 32) return fail(AMG_ERR_UNSUPPORTED, "level %d: at most 32 test vectors", l);
+        h.xe = h.nx / h.bx; h.te = h.nt / h.bt;
+        h.sxe = h.nx / h.sbx; h.ste = h.nt / h.sbt;
+        const int nb = h.sbx * h.sbt;
+        if (nb != 1 && nb % 2)
+            return fail(AMG_ERR_UNSUPPORTED,
+                        "level %d: an odd number of SAP blocks (%d) leaves one block unsolved in the reference "
+                        "(include/sap.h:68)", l, nb);
+        h.ncol = nb == 1 ? 1 : nb / 2;
+        h.red.assign(h.ncol, 0);
+        h.black.assign(h.ncol, 0);
+        for (int X = 0; X < h.sbx; X++)
+            for (int T = 0; T < h.sbt; T++) {
+                const int b = X * h.sbt + T;
+                bool is_red;
+                if (h.sbt % 2 == 0) is_red = (X % 2 == 0) ? (b % 2 == 0) : (b % 2 == 1);
+                else is_red = (b % 2 == 0);
+                if (b / 2 < h.ncol) (is_red ? h.red : h.black)[b / 2] = b;
+            }
+    }
+    return AMG_OK;
+}
+
+// ---------------------------------------------------------------------------------
+// device buffers
+// ---------------------------------------------------------------------------------
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept : p(o.p), bytes(o.bytes) { o.p = nullptr; o.bytes = 0; }
+    ~DevBuf() { if (p) cudaFree(p); }
+    int alloc(size_t b) {
+        if (p && bytes >= b) return AMG_OK;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        if (b == 0) b = 16;
+        cudaError_t e = cudaMalloc(&p, b);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            p = nullptr;
+            return fail(AMG_ERR_NOMEM, "cudaMalloc(%zu) failed: %s", b, cudaGetErrorString(e));
+        }
+        bytes = b;
+        return AMG_OK;
+    }
+    template <typename X> X* as() const { return reinterpret_cast<X*>(p); }
+};
+
+// per-precision state of the fine-level cycle and the engine
+template <typename T>
+struct PrecSet {
+    DevBuf U;                      // [N][2]
+    DevBuf W0;                     // level-0 test vectors [ntest][N][2] (BF16 in the mixed form)
+    int w0_bf16 = 0;
+    std::vector<DevBuf> W;         // levels >= 1: [ntest][n][K]
+    std::vector<DevBuf> links;     // levels >= 1: [n][5][K][K]
+    DevBuf eng_args, eng_work, eng_status, red_black;
+    EngArgs<T> eh{};
+    int eng_smem = 0, eng_cap = 0;
+    DevBuf r0, eta1, psi1, rpart, sap_r, sap_scratch;
+    int ready = 0;
+};
+
+}  // namespace amgb
+
+using namespace amgb;
+
+struct amg_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    amg_params p{};
+    double m0 = 0;
+    int nx = 0, nt = 0, N = 0, L = 0;
+    std::vector<LevelHost> lv;
+    PrecSet<double> d;             // FP64 hierarchy (master)
+    PrecSet<float> f;              // FP32 / BF16 copy for the mixed form
+    DevBuf hops0, linkpart, zero, boot_a, boot_b;
+    std::vector<int> have_init;
+    int gauge_set = 0, setup_done = 0;
+    // outer FGMRES
+    DevBuf V, Z, w, x, b, partial, dots, scal, masks, etab, vf, zf, sap_flags, norms;
+    int Rcap = 0;
+    std::vector<double> history;
+    double last_setup_ms = 0, last_solve_ms = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace {
+
+using cd = std::complex<double>;
+
+long long vlen0(const amg_context* c) { return 2LL * c->N; }
+
+// elementwise helpers on FP64 [n] complex arrays
+__global__ void k_sub_d(double2* d, const double2* a, const double2* b, long long n) {
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+        d[e] = a[e] - b[e];
+}
+__global__ void k_add_d(double2* d, const double2* a, long long n) {
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+        d[e] += a[e];
+}
+__global__ void k_set_int(int* p, int v, int n) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) p[i] = v;
+}
+__global__ void k_sap_check(const double* norm2, const double* vnorm2, double tol, int* act, int* conv, int R) {
+    const int i = threadIdx.x;
+    if (i >= R || !act[i]) return;
+    if (sqrt(norm2[i]) < tol * sqrt(vnorm2[i])) { act[i] = 0; conv[i] = 1; }
+}
+// scale[r] = 1/sqrt(n2[r]) when positive; wmask[r] = arn[r] && n2[r] > 0
+__global__ void k_inv_norm(const double2* n2, int stride, int off, double* scale, const int* arn, int* wmask, int R) {
+    const int i = threadIdx.x;
+    if (i >= R) return;
+    const double v = n2[i * stride + off].x;
+    const double h = sqrt(v);
+    scale[i] = h > 0 ? 1.0 / h : 0.0;
+    wmask[i] = (arn[i] && h > 0) ? 1 : 0;
+}
+
+int ensure_capacity(amg_context* c, int R);
+
+// ---------------------------------------------------------------------------------
+// engine arguments for one precision
+// ---------------------------------------------------------------------------------
+template <typename T>
+int build_engine(amg_context* c, PrecSet<T>& ps, int nsrc) {
+    const amg_params& p = c->p;
+    EngArgs<T>& a = ps.eh;
+    memset(&a, 0, sizeof a);
+    a.nlev = c->L;
+    a.p.m0 = (T)c->m0;
+    a.p.cycle = p.cycle; a.p.nu1 = p.nu1; a.p.nu2 = p.nu2;
+    a.p.sap_m = p.sap_gmres_m; a.p.sap_restarts = p.sap_gmres_restarts;
+    a.p.sap_gmres_tol = (T)p.sap_gmres_tol; a.p.sap_tol = (T)p.sap_tol;
+    a.p.k_m = p.kcycle_m; a.p.k_restarts = p.kcycle_restarts; a.p.k_tol = (T)p.kcycle_tol;
+    a.p.c_m = p.coarse_m; a.p.c_restarts = p.coarse_restarts; a.p.c_tol = (T)p.coarse_tol;
+    std::vector<int> rb;
+    std::vector<int> rb_off(c->L, 0);
+    for (int l = 0; l < c->L; l++) {
+        rb_off[l] = (int)rb.size();
+        rb.insert(rb.end(), c->lv[l].red.begin(), c->lv[l].red.end());
+        rb.insert(rb.end(), c->lv[l].black.begin(), c->lv[l].black.end());
+    }
+    CKR(ps.red_black.alloc(std::max<size_t>(rb.size(), 1) * sizeof(int)));
+    if (!rb.empty())
+        CK(cudaMemcpyAsync(ps.red_black.p, rb.data(), rb.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    long long off = 0;
+    int sm = 0;
+    auto al = [](long long v) { return (v + 1) & ~1LL; };
+    for (int l = 1; l < c->L; l++) {
+        const LevelHost& h = c->lv[l];
+        EngLevel<T>& e = a.lv[l];
+        e.nx = h.nx; e.nt = h.nt; e.n = h.n; e.K = h.K; e.coarsest = h.coarsest;
+        e.bx = h.bx; e.bt = h.bt; e.xe = h.xe; e.te = h.te; e.ntest = h.ntest;
+        e.W = h.coarsest ? nullptr : ps.W[l].template as<cx<T>>();
+        e.links = ps.links[l].template as<cx<T>>();
+        e.sbx = h.sbx; e.sbt = h.sbt; e.sxe = h.sxe; e.ste = h.ste; e.ncol = h.ncol;
+        e.red = ps.red_black.template as<int>() + rb_off[l];
+        e.black = e.red + h.ncol;
+        // Level::gmres_l: GMRES(20, 20, 1e-10) below the coarsest level, the coarse knobs on it
+        e.gm_m = h.coarsest ? p.coarse_m : 20;
+        e.gm_restarts = h.coarsest ? p.coarse_restarts : 20;
+        e.gm_tol = h.coarsest ? (T)p.coarse_tol : (T)1e-10;
+        const long long nvec = (long long)h.n * h.K;
+        e.off_kfg = off; off += al((2LL * p.kcycle_m + 2) * nvec);
+        e.off_cg = off; off += al((long long)(e.gm_m + 2) * nvec);
+        e.sm_kfg = sm; sm += gm_state_bytes(1, p.kcycle_m, sizeof(T));
+        e.sm_cg = sm; sm += gm_state_bytes(1, e.gm_m, sizeof(T));
+        if (!h.coarsest) {
+            const LevelHost& hn = c->lv[l + 1];
+            const long long ncv = (long long)hn.n * hn.K;
+            e.off_cyc = off; off += al(nvec + 2 * ncv);
+            const long long segtot = (long long)h.ncol * h.sxe * h.ste * h.K;
+            e.off_sap = off; off += al(nvec + (long long)(p.sap_gmres_m + 4) * segtot);
+            e.sm_sap = sm; sm += gm_state_bytes(h.ncol, p.sap_gmres_m, sizeof(T));
+            if (h.ncol > kEngineThreads)
+                return fail(AMG_ERR_UNSUPPORTED, "level %d: %d SAP blocks per colour exceed %d", l, h.ncol, kEngineThreads);
+        }
+    }
+    a.smem_red = sm;
+    sm += 2 * (kEngineThreads / 32) * (int)sizeof(T) + 64;
+    if (sm > 200 * 1024) return fail(AMG_ERR_UNSUPPORTED, "engine scalar state needs %d bytes of shared memory", sm);
+    ps.eng_smem = sm;
+    a.slab = std::max<long long>(off, 2);
+    ps.eng_cap = std::max(nsrc, 1);
+    CKR(ps.eng_work.alloc((size_t)a.slab * ps.eng_cap * sizeof(cx<T>)));
+    CKR(ps.eng_status.alloc(sizeof(int) * (ps.eng_cap + 4)));
+    a.work = ps.eng_work.template as<cx<T>>();
+    a.status = ps.eng_status.template as<int>();
+    a.flags = a.status + ps.eng_cap;
+    CK(cudaMemsetAsync(a.flags, 0, sizeof(int), c->stream));
+    CKR(ps.eng_args.alloc(sizeof(EngArgs<T>)));
+    CK(cudaMemcpyAsync(ps.eng_args.p, &a, sizeof a, cudaMemcpyHostToDevice, c->stream));
+    return AMG_OK;
+}
+
+template <typename T>
+int run_engine(amg_context* c, PrecSet<T>& ps, int op, int level, int nu, const cx<T>* in, long long in_stride,
+               cx<T>* out, long long out_stride, int nsrc) {
+    if (nsrc > ps.eng_cap) return fail(AMG_ERR_INVALID, "engine capacity %d < %d sources", ps.eng_cap, nsrc);
+    CK(launch_engine_dev<T>(ps.eng_args.template as<EngArgs<T>>(), op, level, nu, in, in_stride, out, out_stride,
+                            nsrc, ps.eng_smem, c->stream));
+    return AMG_OK;
+}
+
+template <typename T>
+int alloc_fine(amg_context* c, PrecSet<T>& ps, int R) {
+    const LevelHost& h0 = c->lv[0];
+    const LevelHost& h1 = c->lv[1];
+    const long long len = vlen0(c);
+    CKR(ps.r0.alloc((size_t)R * len * sizeof(cx<T>)));
+    CKR(ps.sap_r.alloc((size_t)R * len * sizeof(cx<T>)));
+    CKR(ps.eta1.alloc((size_t)R * h1.n * h1.K * sizeof(cx<T>)));
+    CKR(ps.psi1.alloc((size_t)R * h1.n * h1.K * sizeof(cx<T>)));
+    const int nblk = h0.bx * h0.bt;
+    const int spb = h0.xe * h0.te;
+    int nchunk = std::max(1, std::min(std::max(1, spb / 256), (592 + nblk - 1) / nblk));
+    CKR(ps.rpart.alloc((size_t)R * nblk * nchunk * 2 * h0.ntest * sizeof(cx<T>)));
+    return AMG_OK;
+}
+
+template <typename T>
+int restrict_chunks(amg_context* c, int R) {
+    const LevelHost& h0 = c->lv[0];
+    const int nblk = h0.bx * h0.bt;
+    const int spb = h0.xe * h0.te;
+    (void)R;
+    return std::max(1, std::min(std::max(1, spb / 256), (592 + nblk - 1) / nblk));
+}
+
+template <typename T>
+void fine_restrict(amg_context* c, PrecSet<T>& ps, const cx<T>* v, cx<T>* out, int R) {
+    const LevelHost& h0 = c->lv[0];
+    const int nchunk = restrict_chunks<T>(c, R);
+    if (ps.w0_bf16)
+        launch_restrict0<float, __nv_bfloat162>(ps.W0.template as<__nv_bfloat162>(), (const cx<float>*)v,
+                                                 (cx<float>*)out, ps.rpart.template as<cx<float>>(), c->nx, c->nt,
+                                                 h0.bx, h0.bt, h0.ntest, R, nchunk, c->stream);
+    else
+        launch_restrict0<T, cx<T>>(ps.W0.template as<cx<T>>(), v, out, ps.rpart.template as<cx<T>>(), c->nx, c->nt,
+                                    h0.bx, h0.bt, h0.ntest, R, nchunk, c->stream);
+}
+
+template <typename T>
+void fine_prolong_add(amg_context* c, PrecSet<T>& ps, const cx<T>* vc, cx<T>* psi, int R) {
+    const LevelHost& h0 = c->lv[0];
+    if (ps.w0_bf16)
+        launch_prolong0_add<float, __nv_bfloat162>(ps.W0.template as<__nv_bfloat162>(), (const cx<float>*)vc,
+                                                    (cx<float>*)psi, c->nx, c->nt, h0.bx, h0.bt, h0.ntest, R,
+                                                    c->stream);
+    else
+        launch_prolong0_add<T, cx<T>>(ps.W0.template as<cx<T>>(), vc, psi, c->nx, c->nt, h0.bx, h0.bt, h0.ntest, R,
+                                       c->stream);
+}
+
+// ---------------------------------------------------------------------------------
+// SAP_C::SAP on the fine level (src/sap.cpp:64-174) for R sources, x in/out; v has stride
+// vstride (0: the same source for all).  Every block of a colour is solved in one launch.
+// Per-source early exit on ||v - D x|| < sap_tol ||v|| through device flags.  When
+// need_ret is 0 the residual after the last sweep is skipped: the reference computes it
+// only for the convergence test, whose result the cycles ignore.
+// ---------------------------------------------------------------------------------
+template <typename T>
+int fine_sap(amg_context* c, PrecSet<T>& ps, const cx<T>* v, long long vstride, cx<T>* x, int nu, int R,
+             int need_ret) {
+    const LevelHost& h = c->lv[0];
+    const amg_params& p = c->p;
+    const long long len = vlen0(c);
+    int* act = c->sap_flags.as<int>();
+    int* conv = act + c->Rcap;
+    double* vnorm2 = c->norms.as<double>();
+    double* norm2 = vnorm2 + c->Rcap;
+    double* partial = c->partial.as<double>();
+    cx<T>* r = ps.sap_r.template as<cx<T>>();
+    const cx<T>* U = ps.U.template as<cx<T>>();
+    const T m0 = (T)c->m0;
+    k_set_int<<<1, 256, 0, c->stream>>>(act, 1, R);
+    k_set_int<<<1, 256, 0, c->stream>>>(conv, 0, R);
+    launch_norm2<T>(v, len, vstride, R, partial, vnorm2, c->stream);
+    launch_residual<T>(U, v, vstride, x, r, c->nx, c->nt, R, m0, nullptr, nullptr, nullptr, c->stream);
+    const int S = h.sxe * h.ste;
+    const int use_smem = sap0_smem_bytes<T>(S, p.sap_gmres_m, 1) <= 200 * 1024;
+    if (!use_smem) CKR(ps.sap_scratch.alloc((size_t)h.ncol * R * (p.sap_gmres_m + 5) * 2 * S * sizeof(cx<T>)));
+    cx<T>* scratch = use_smem ? nullptr : ps.sap_scratch.template as<cx<T>>();
+    const int* d_red = ps.red_black.template as<int>();
+    const int* d_black = d_red + h.ncol;
+    for (int it = 0; it < nu; it++) {
+        for (int colour = 0; colour < 2; colour++) {
+            CK(launch_sap0<T>(U, r, x, colour == 0 ? d_red : d_black, h.ncol, R, c->nx, c->nt, h.sbt, h.sxe, h.ste,
+                              m0, p.sap_gmres_m, p.sap_gmres_restarts, (T)p.sap_gmres_tol, use_smem, scratch,
+                              nullptr, act, c->stream));
+            const bool last = (colour == 1) && (it == nu - 1);
+            if (last && !need_ret) break;
+            launch_residual<T>(U, v, vstride, x, r, c->nx, c->nt, R, m0, partial, colour == 1 ? norm2 : nullptr,
+                               act, c->stream);
+            if (colour == 1) k_sap_check<<<1, 256, 0, c->stream>>>(norm2, vnorm2, p.sap_tol, act, conv, R);
+        }
+    }
+    CKL();
+    return AMG_OK;
+}
+
+// ---------------------------------------------------------------------------------
+// AlgebraicMG::k_cycle / v_cycle from the fine level (src/amg.cpp:90-178) for R sources:
+// psi is added into.  psi_zero tells that psi is zero on entry (FGMRES_AMG zeroes it,
+// include/amg.h:135-139), so r = eta - D psi is eta exactly.
+// ---------------------------------------------------------------------------------
+template <typename T>
+int fine_cycle(amg_context* c, PrecSet<T>& ps, const cx<T>* eta, cx<T>* psi, int R, bool psi_zero) {
+    const amg_params& p = c->p;
+    const LevelHost& h1 = c->lv[1];
+    const long long len = vlen0(c);
+    const long long n1 = (long long)h1.n * h1.K;
+    if (p.nu1 > 0) {
+        CKR(fine_sap<T>(c, ps, eta, len, psi, p.nu1, R, 0));
+        psi_zero = false;
+    }
+    const cx<T>* r = eta;
+    if (!psi_zero) {
+        launch_residual<T>(ps.U.template as<cx<T>>(), eta, len, psi, ps.r0.template as<cx<T>>(), c->nx, c->nt, R,
+                           (T)c->m0, nullptr, nullptr, nullptr, c->stream);
+        r = ps.r0.template as<cx<T>>();
+    }
+    cx<T>* eta1 = ps.eta1.template as<cx<T>>();
+    cx<T>* psi1 = ps.psi1.template as<cx<T>>();
+    fine_restrict<T>(c, ps, r, eta1, R);
+    if (p.cycle == AMG_CYCLE_K) {
+        CKR(run_engine<T>(c, ps, ENG_KFGMRES, 1, 0, eta1, n1, psi1, n1, R));
+    } else {
+        CK(cudaMemsetAsync(psi1, 0, (size_t)R * n1 * sizeof(cx<T>), c->stream));
+        CKR(run_engine<T>(c, ps, ENG_VCYCLE, 1, 0, eta1, n1, psi1, n1, R));
+    }
+    fine_prolong_add<T>(c, ps, psi1, psi, R);
+    if (p.nu2 > 0) CKR(fine_sap<T>(c, ps, eta, len, psi, p.nu2, R, 0));
+    CKL();
+    return AMG_OK;
+}
+
+// FGMRES_AMG::preconditioner (include/amg.h:134-144): out = 0, then one cycle
+int precondition(amg_context* c, const double2* v, double2* z, int R) {
+    const long long len = vlen0(c);
+    if (c->p.precision == AMG_PREC_F64) {
+        CK(cudaMemsetAsync(z, 0, (size_t)R * len * sizeof(double2), c->stream));
+        return fine_cycle<double>(c, c->d, v, z, R, true);
+    }
+    float2* vf = c->vf.as<float2>();
+    float2* zf = c->zf.as<float2>();
+    launch_d2f(vf, v, R * len, c->stream);
+    CK(cudaMemsetAsync(zf, 0, (size_t)R * len * sizeof(float2), c->stream));
+    CKR(fine_cycle<float>(c, c->f, vf, zf, R, true));
+    launch_f2d(z, zf, R * len, c->stream);
+    CKL();
+    return AMG_OK;
+}
+
+// ---------------------------------------------------------------------------------
+// Outer FGMRES (FGMRES::fgmres, src/fgmres.cpp:5-115) with func = D_phi and the AMG
+// preconditioner, x0 = 0, for R sources with independent Krylov spaces.  Arnoldi uses
+// classical Gram-Schmidt with one re-orthogonalisation on the device; the Hessenberg
+// rotations, the triangular solve and every control decision run on the host in FP64,
+// per source exactly as the reference (maxIt carried over restart cycles).
+// ---------------------------------------------------------------------------------
+int outer_fgmres(amg_context* c, const double2* b, double2* x, int R, amg_solve_info* info) {
+    const amg_params& p = c->p;
+    const int m = p.outer_m;
+    const long long len = vlen0(c);
+    const long long vstride = (long long)R * len;
+    double2* V = c->V.as<double2>();
+    double2* Z = c->Z.as<double2>();
+    double2* w = c->w.as<double2>();
+    double* partial = c->partial.as<double>();
+    double2* dpart = c->partial.as<double2>();
+    double2* dots = c->dots.as<double2>();
+    double* scal = c->scal.as<double>();
+    int* act_d = c->masks.as<int>();
+    int* arn_d = act_d + c->Rcap;
+    int* wm_d = arn_d + c->Rcap;
+    int* nvr_d = wm_d + c->Rcap;
+    double2* eta_d = c->etab.as<double2>();
+    const double2* U = c->d.U.as<double2>();
+    const int np = std::min<long long>(592, (len + 255) / 256);
+
+    std::vector<cd> H((size_t)R * (m + 1) * m), g((size_t)R * (m + 1)), cn((size_t)R * m), sn((size_t)R * m),
+        eta((size_t)R * m);
+    std::vector<double> err(R), normb(R);
+    std::vector<int> maxit(R, m), act(R, 1), arn(R, 0), iters(R, p.outer_restarts * m);
+    std::vector<double> hbuf(2 * (size_t)R * (m + 2) * 3 + 2 * R);
+    c->history.clear();
+
+    // x = x0 = 0; r = b - D x into V0
+    CK(cudaMemsetAsync(x, 0, (size_t)R * len * sizeof(double2), c->stream));
+    double* n2 = c->norms.as<double>();
+    launch_residual<double>(U, b, len, x, V, c->nx, c->nt, R, c->m0, partial, n2, nullptr, c->stream);
+    launch_norm2<double>(b, len, len, R, partial, n2 + c->Rcap, c->stream);
+    std::vector<double> hn(2 * R);
+    CK(cudaMemcpyAsync(hn.data(), n2, R * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(hn.data() + R, n2 + c->Rcap, R * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (int r = 0; r < R; r++) { err[r] = std::sqrt(hn[r]); normb[r] = std::sqrt(hn[R + r]); }
+    std::vector<double> sc(R);
+    std::vector<int> hmask(4 * (size_t)R);
+
+    auto upload_masks = [&]() -> int {
+        for (int r = 0; r < R; r++) { hmask[r] = act[r]; hmask[R + r] = arn[r]; }
+        CK(cudaMemcpyAsync(act_d, hmask.data(), R * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(arn_d, hmask.data() + R, R * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+        return AMG_OK;
+    };
+
+    for (int k = 0; k < p.outer_restarts; k++) {
+        bool any = false;
+        for (int r = 0; r < R; r++) any |= act[r];
+        if (!any) break;
+        for (int r = 0; r < R; r++) {
+            arn[r] = act[r];
+            sc[r] = act[r] ? 1.0 / err[r] : 0.0;
+            if (act[r]) g[(size_t)r * (m + 1)] = cd(err[r], 0);
+        }
+        CKR(upload_masks());
+        CK(cudaMemcpyAsync(scal, sc.data(), R * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        launch_scale(V, V, len, scal, act_d, R, c->stream);
+        for (int j = 0; j < m; j++) {
+            bool anyarn = false;
+            for (int r = 0; r < R; r++) anyarn |= arn[r];
+            if (!anyarn) break;
+            double2* Vj = V + (long long)j * vstride;
+            double2* Zj = Z + (long long)j * vstride;
+            CKR(precondition(c, Vj, Zj, R));
+            launch_dirac<double>(U, Zj, w, c->nx, c->nt, R, c->m0, 0, c->stream);
+            const int nv = j + 1;
+            double2* d1 = dots;
+            double2* d2 = dots + (size_t)R * (nv + 1);
+            double2* d3 = d2 + (size_t)R * (nv + 1);
+            launch_multidot(w, V, len, vstride, nv, R, dpart, np, d1, c->stream);
+            launch_axpy_multidot(w, V, len, vstride, nv, d1, nv + 1, nv, arn_d, R, dpart, np, d2, c->stream);
+            launch_axpy_multidot(w, V, len, vstride, nv, d2, nv + 1, 0, arn_d, R, dpart, np, d3, c->stream);
+            k_inv_norm<<<1, 256, 0, c->stream>>>(d3, 1, 0, scal, arn_d, wm_d, R);
+            launch_scale(V + (long long)(j + 1) * vstride, w, len, scal, wm_d, R, c->stream);
+            std::vector<double2> hd((size_t)R * (2 * (nv + 1) + 1));
+            CK(cudaMemcpyAsync(hd.data(), dots, hd.size() * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+            CK(cudaStreamSynchronize(c->stream));
+            for (int r = 0; r < R; r++) {
+                if (!arn[r]) continue;
+                cd* Hr = &H[(size_t)r * (m + 1) * m];
+                cd* cnr = &cn[(size_t)r * m];
+                cd* snr = &sn[(size_t)r * m];
+                cd* gr = &g[(size_t)r * (m + 1)];
+                for (int i = 0; i <= j; i++) {
+                    const double2 a = hd[(size_t)r * (nv + 1) + i];
+                    const double2 bq = hd[(size_t)R * (nv + 1) + (size_t)r * (nv + 1) + i];
+                    Hr[i * m + j] = cd(a.x + bq.x, a.y + bq.y);
+                }
+                const double hn2 = hd[(size_t)2 * R * (nv + 1) + r].x;
+                Hr[(j + 1) * m + j] = cd(std::sqrt(hn2), 0);
+                // rotation(j) (src/fgmres.cpp:90-104)
+                for (int i = 0; i < j; i++) {
+                    cd temp = std::conj(cnr[i]) * Hr[i * m + j] + std::conj(snr[i]) * Hr[(i + 1) * m + j];
+                    Hr[(i + 1) * m + j] = -snr[i] * Hr[i * m + j] + cnr[i] * Hr[(i + 1) * m + j];
+                    Hr[i * m + j] = temp;
+                }
+                cd den = std::sqrt(std::conj(Hr[j * m + j]) * Hr[j * m + j] +
+                                   std::conj(Hr[(j + 1) * m + j]) * Hr[(j + 1) * m + j]);
+                snr[j] = Hr[(j + 1) * m + j] / den;
+                cnr[j] = Hr[j * m + j] / den;
+                Hr[j * m + j] = std::conj(cnr[j]) * Hr[j * m + j] + std::conj(snr[j]) * Hr[(j + 1) * m + j];
+                Hr[(j + 1) * m + j] = 0.0;
+                gr[j + 1] = -snr[j] * gr[j];
+                gr[j] = std::conj(cnr[j]) * gr[j];
+                if (r == 0) c->history.push_back(std::abs(gr[j + 1]));
+                if (std::abs(gr[j + 1]) < p.outer_tol * normb[r]) {
+                    maxit[r] = j + 1;
+                    arn[r] = 0;
+                }
+            }
+            CKR(upload_masks());
+        }
+        // solve_upper_triangular (src/fgmres.cpp:107-115) and x += sum eta_j Z_j
+        std::vector<double2> etah((size_t)R * m);
+        std::vector<int> nvr(R, 0);
+        for (int r = 0; r < R; r++) {
+            if (!act[r]) continue;
+            const cd* Hr = &H[(size_t)r * (m + 1) * m];
+            const cd* gr = &g[(size_t)r * (m + 1)];
+            cd* er = &eta[(size_t)r * m];
+            const int n = maxit[r];
+            for (int i = n - 1; i >= 0; i--) {
+                er[i] = gr[i];
+                for (int jj = i + 1; jj < n; jj++) er[i] -= Hr[i * m + jj] * er[jj];
+                er[i] /= Hr[i * m + i];
+            }
+            for (int i = 0; i < n; i++) etah[(size_t)r * m + i] = make_double2(er[i].real(), er[i].imag());
+            nvr[r] = n;
+        }
+        CK(cudaMemcpyAsync(eta_d, etah.data(), etah.size() * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(nvr_d, nvr.data(), R * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+        launch_multiaxpy_add(x, Z, len, vstride, m, eta_d, m, nvr_d, act_d, R, c->stream);
+        // true residual into V0
+        launch_residual<double>(U, b, len, x, V, c->nx, c->nt, R, c->m0, partial, n2, act_d, c->stream);
+        CK(cudaMemcpyAsync(hn.data(), n2, R * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        for (int r = 0; r < R; r++) {
+            if (!act[r]) continue;
+            err[r] = std::sqrt(hn[r]);
+            if (err[r] < p.outer_tol * normb[r]) {
+                iters[r] = k * m + maxit[r];
+                act[r] = 0;
+            }
+        }
+    }
+    CKL();
+    if (info)
+        for (int r = 0; r < R; r++) {
+            info[r].iterations = iters[r];
+            info[r].rel_residual = normb[r] > 0 ? err[r] / normb[r] : err[r];
+            info[r].converged = err[r] < p.outer_tol * normb[r];
+        }
+    for (int r = 0; r < R; r++)
+        if (act[r]) return AMG_NOT_CONVERGED;
+    return AMG_OK;
+}
+
+int ensure_capacity(amg_context* c, int R) {
+    if (R <= c->Rcap && c->V.p) return AMG_OK;
+    const int Rn = std::max(R, c->Rcap);
+    const long long len = vlen0(c);
+    const int m = c->p.outer_m;
+    CKR(c->V.alloc((size_t)(m + 1) * Rn * len * sizeof(double2)));
+    CKR(c->Z.alloc((size_t)m * Rn * len * sizeof(double2)));
+    CKR(c->w.alloc((size_t)Rn * len * sizeof(double2)));
+    CKR(c->x.alloc((size_t)Rn * len * sizeof(double2)));
+    CKR(c->b.alloc((size_t)Rn * len * sizeof(double2)));
+    const size_t np = 592;
+    CKR(c->partial.alloc(np * Rn * 24 * sizeof(double2)));
+    CKR(c->dots.alloc((size_t)Rn * 3 * 24 * sizeof(double2)));
+    CKR(c->scal.alloc((size_t)Rn * sizeof(double)));
+    CKR(c->masks.alloc((size_t)4 * Rn * sizeof(int)));
+    CKR(c->etab.alloc((size_t)Rn * m * sizeof(double2)));
+    CKR(c->sap_flags.alloc((size_t)2 * Rn * sizeof(int)));
+    CKR(c->norms.alloc((size_t)2 * Rn * sizeof(double)));
+    c->Rcap = Rn;
+    CKR(alloc_fine<double>(c, c->d, Rn));
+    if (c->p.precision == AMG_PREC_MIXED) {
+        CKR(c->vf.alloc((size_t)Rn * len * sizeof(float2)));
+        CKR(c->zf.alloc((size_t)Rn * len * sizeof(float2)));
+        CKR(alloc_fine<float>(c, c->f, Rn));
+    }
+    return AMG_OK;
+}
+
+// ---------------------------------------------------------------------------------
+// set-up (AlgebraicMG::setUpPhase, src/amg.cpp:3-88)
+// ---------------------------------------------------------------------------------
+struct Draw {
+    // The reference draws `distribution(randomInt) + I_number * distribution(randomInt)` with
+    // std::mt19937(50) and uniform(-1, 1) (src/amg.cpp:8-16); g++ evaluates the imaginary
+    // operand first, which this generator reproduces.  A non-zero seed selects a 64-bit
+    // Mersenne twister instead.
+    std::mt19937 g32;
+    std::mt19937_64 g64;
+    bool use64;
+    std::uniform_real_distribution<double> dist{-1.0, 1.0};
+    explicit Draw(unsigned long long seed) : g32(50), g64(seed), use64(seed != 0) {}
+    double next() { return use64 ? dist(g64) : dist(g32); }
+    void fill(std::vector<double2>& v) {
+        for (auto& z : v) {
+            const double im = next();
+            const double re = next();
+            z = make_double2(re, im);
+        }
+    }
+};
+
+int coarse_links(amg_context* c, int l) {
+    const LevelHost& h = c->lv[l];
+    const int nblk = h.bx * h.bt, spb = h.xe * h.te;
+    const int nchunk = std::max(1, std::min(std::max(1, spb / 64), (592 + nblk - 1) / nblk));
+    const int Kc = 2 * h.ntest;
+    CKR(c->linkpart.alloc((size_t)nblk * nchunk * 5 * Kc * Kc * sizeof(double2)));
+    const double2* hops = l == 0 ? c->hops0.as<double2>() : c->d.links[l].as<double2>();
+    const double2* W = l == 0 ? c->d.W0.as<double2>() : c->d.W[l].as<double2>();
+    launch_coarse_links<double>(W, hops, c->d.links[l + 1].as<double2>(), h.nx, h.nt, h.K, h.bx, h.bt, h.ntest,
+                                c->linkpart.as<double2>(), nchunk, c->stream);
+    CKL();
+    return AMG_OK;
+}
+
+int orthonormalize(amg_context* c, int l) {
+    const LevelHost& h = c->lv[l];
+    double2* W = l == 0 ? c->d.W0.as<double2>() : c->d.W[l].as<double2>();
+    launch_orthonormalize<double>(W, h.nx, h.nt, h.K, h.bx, h.bt, h.ntest, c->stream);
+    CKL();
+    return AMG_OK;
+}
+
+int build_mixed(amg_context* c) {
+    PrecSet<float>& f = c->f;
+    const long long len = vlen0(c);
+    CKR(f.U.alloc((size_t)len * sizeof(float2)));
+    launch_d2f(f.U.as<float2>(), c->d.U.as<double2>(), len, c->stream);
+    const LevelHost& h0 = c->lv[0];
+    CKR(f.W0.alloc((size_t)h0.ntest * len * sizeof(__nv_bfloat162)));
+    launch_d2bf(f.W0.as<__nv_bfloat162>(), c->d.W0.as<double2>(), h0.ntest * len, c->stream);
+    f.w0_bf16 = 1;
+    f.W.resize(c->L);
+    f.links.resize(c->L);
+    for (int l = 1; l < c->L; l++) {
+        const LevelHost& h = c->lv[l];
+        const long long nl = (long long)h.n * 5 * h.K * h.K;
+        CKR(f.links[l].alloc((size_t)nl * sizeof(float2)));
+        launch_d2f(f.links[l].as<float2>(), c->d.links[l].as<double2>(), nl, c->stream);
+        if (!h.coarsest) {
+            const long long nw = (long long)h.ntest * h.n * h.K;
+            CKR(f.W[l].alloc((size_t)nw * sizeof(float2)));
+            launch_d2f(f.W[l].as<float2>(), c->d.W[l].as<double2>(), nw, c->stream);
+        }
+    }
+    CKR(build_engine<float>(c, f, c->d.eng_cap));
+    CKR(alloc_fine<float>(c, f, c->Rcap));
+    CKR(c->vf.alloc((size_t)c->Rcap * len * sizeof(float2)));
+    CKR(c->zf.alloc((size_t)c->Rcap * len * sizeof(float2)));
+    f.ready = 1;
+    CKL();
+    return AMG_OK;
+}
+
+int do_setup(amg_context* c) {
+    if (!c->gauge_set) return fail(AMG_ERR_STATE, "set the gauge field before the set-up");
+    const amg_params& p = c->p;
+    const int L = c->L;
+    int cap = c->Rcap;
+    for (int l = 0; l < L - 1; l++) cap = std::max(cap, c->lv[l].ntest);
+    CKR(ensure_capacity(c, cap));
+    CKR(build_engine<double>(c, c->d, cap));
+    const long long len = vlen0(c);
+    long long zlen = len;
+    for (int l = 1; l < L; l++) zlen = std::max<long long>(zlen, (long long)c->lv[l].n * c->lv[l].K);
+    CKR(c->zero.alloc((size_t)zlen * sizeof(double2)));
+    CK(cudaMemsetAsync(c->zero.p, 0, (size_t)zlen * sizeof(double2), c->stream));
+
+    // initial test vectors (src/amg.cpp:8-35)
+    Draw rng(p.tv_seed);
+    const LevelHost& h0 = c->lv[0];
+    if (!c->have_init[0]) {
+        std::vector<double2> host((size_t)h0.ntest * len);
+        rng.fill(host);
+        CK(cudaMemcpyAsync(c->d.W0.p, host.data(), host.size() * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    for (int l = 1; l < L - 1; l++) {
+        if (c->have_init[l]) continue;
+        const LevelHost& h = c->lv[l];
+        const LevelHost& hp = c->lv[l - 1];
+        const long long nv = (long long)h.n * h.K;
+        double2* W = c->d.W[l].as<double2>();
+        for (int i = 0; i < h.ntest; i++) {
+            if (i < hp.ntest) {
+                if (l == 1) {
+                    fine_restrict<double>(c, c->d, c->d.W0.as<double2>() + (long long)i * len, W + i * nv, 1);
+                } else {
+                    const long long nvp = (long long)hp.n * hp.K;
+                    CKR(run_engine<double>(c, c->d, ENG_RESTRICT, l - 1, 0, c->d.W[l - 1].as<double2>() + i * nvp, 0,
+                                           W + i * nv, 0, 1));
+                }
+            } else {
+                std::vector<double2> host((size_t)nv);
+                rng.fill(host);
+                CK(cudaMemcpyAsync(W + i * nv, host.data(), nv * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+                CK(cudaStreamSynchronize(c->stream));
+            }
+        }
+    }
+    CKR(c->hops0.alloc((size_t)c->N * 20 * sizeof(double2)));
+    launch_fine_hops<double>(c->d.U.as<double2>(), c->hops0.as<double2>(), c->nx, c->nt, c->stream);
+    // smoothing, orthonormalisation and coarse links, level by level
+    for (int l = 0; l < L - 1; l++) {
+        const LevelHost& h = c->lv[l];
+        if (p.sap_tv_iters > 0) {
+            if (l == 0) {
+                CKR(fine_sap<double>(c, c->d, c->zero.as<double2>(), 0, c->d.W0.as<double2>(), p.sap_tv_iters,
+                                     h.ntest, 0));
+            } else {
+                const long long nv = (long long)h.n * h.K;
+                CKR(run_engine<double>(c, c->d, ENG_SAP, l, p.sap_tv_iters, c->zero.as<double2>(), 0,
+                                       c->d.W[l].as<double2>(), nv, h.ntest));
+            }
+        }
+        CKR(orthonormalize(c, l));
+        CKR(coarse_links(c, l));
+    }
+    // bootstrap passes (src/amg.cpp:52-84)
+    for (int it = 0; it < p.nit; it++) {
+        for (int l = 0; l < L - 1; l++) {
+            const LevelHost& h = c->lv[l];
+            const long long nv = (long long)h.n * h.K;
+            const long long tot = nv * h.ntest;
+            CKR(c->boot_a.alloc((size_t)tot * sizeof(double2)));
+            CKR(c->boot_b.alloc((size_t)tot * sizeof(double2)));
+            double2* rhs = c->boot_a.as<double2>();
+            double2* z = c->boot_b.as<double2>();
+            double2* W = l == 0 ? c->d.W0.as<double2>() : c->d.W[l].as<double2>();
+            if (l == 0) {
+                launch_dirac<double>(c->d.U.as<double2>(), W, rhs, c->nx, c->nt, h.ntest, c->m0, 0, c->stream);
+            } else {
+                CKR(run_engine<double>(c, c->d, ENG_APPLY, l, 0, W, nv, rhs, nv, h.ntest));
+            }
+            k_sub_d<<<592, 256, 0, c->stream>>>(rhs, W, rhs, tot);
+            CK(cudaMemsetAsync(z, 0, (size_t)tot * sizeof(double2), c->stream));
+            if (l == 0) {
+                CKR(fine_cycle<double>(c, c->d, rhs, z, h.ntest, true));
+            } else {
+                CKR(run_engine<double>(c, c->d, p.cycle == AMG_CYCLE_K ? ENG_KCYCLE : ENG_VCYCLE, l, 0, rhs, nv, z,
+                                       nv, h.ntest));
+            }
+            k_add_d<<<592, 256, 0, c->stream>>>(W, z, tot);
+            CKR(orthonormalize(c, l));
+            CKR(coarse_links(c, l));
+        }
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    int flags = 0;
+    CK(cudaMemcpy(&flags, c->d.eh.flags, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flags) return fail(AMG_ERR_UNSUPPORTED, "engine reported flags %d", flags);
+    c->f.ready = 0;
+    if (p.precision == AMG_PREC_MIXED) CKR(build_mixed(c));
+    c->setup_done = 1;
+    CK(cudaStreamSynchronize(c->stream));
+    return AMG_OK;
+}
+
+// copy helpers for the single-source probes
+int to_dev(DevBuf& b, const double* h, long long ncplx, cudaStream_t s) {
+    CKR(b.alloc((size_t)ncplx * sizeof(double2)));
+    if (h) CK(cudaMemcpyAsync(b.p, h, (size_t)ncplx * sizeof(double2), cudaMemcpyHostToDevice, s));
+    return AMG_OK;
+}
+int to_host(double* h, const DevBuf& b, long long ncplx, cudaStream_t s) {
+    CK(cudaMemcpyAsync(h, b.p, (size_t)ncplx * sizeof(double2), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return AMG_OK;
+}
+
+int check_ready(amg_ctx c, int level, bool need_setup) {
+    if (!c) return fail(AMG_ERR_INVALID, "null context");
+    if (level < 0 || level >= c->L) return fail(AMG_ERR_INVALID, "level %d out of range", level);
+    if (need_setup && !c->setup_done) return fail(AMG_ERR_STATE, "set-up not done");
+    if (!c->gauge_set) return fail(AMG_ERR_STATE, "gauge field not set");
+    return AMG_OK;
+}
+
+int select_device(amg_ctx c) {
+    CK(cudaSetDevice(c->device));
+    return AMG_OK;
+}
+
+}  // namespace
+
+// =================================================================================
+// C ABI
+// =================================================================================
+extern "C" {
+
+const char* amg_status_string(int s) {
+    switch (s) {
+        case AMG_OK: return "ok";
+        case AMG_NOT_CONVERGED: return "not converged";
+        case AMG_ERR_INVALID: return "invalid argument";
+        case AMG_ERR_CUDA: return "CUDA error";
+        case AMG_ERR_STATE: return "wrong call order";
+        case AMG_ERR_NOMEM: return "out of device memory";
+        case AMG_ERR_DEVICE_WAIT: return "device-side wait gave up";
+        case AMG_ERR_UNSUPPORTED: return "unsupported configuration";
+        default: return "unknown status";
+    }
+}
+const char* amg_last_error(void) { return g_last_error.c_str(); }
+int amg_version(void) { return 100; }
+
+void amg_params_default(amg_params* p) {
+    if (!p) return;
+    memset(p, 0, sizeof *p);
+    p->cycle = AMG_CYCLE_K;
+    p->nu1 = 0;
+    p->nu2 = 2;
+    p->nit = 0;
+    p->sap_tv_iters = 4;
+    p->sap_gmres_m = 5;
+    p->sap_gmres_restarts = 5;
+    p->sap_gmres_tol = 1e-3;
+    p->sap_tol = 1e-10;
+    p->kcycle_m = 5;
+    p->kcycle_restarts = 2;
+    p->kcycle_tol = 0.1;
+    p->coarse_m = 20;
+    p->coarse_restarts = 20;
+    p->coarse_tol = 0.1;
+    p->outer_m = 20;
+    p->outer_restarts = 50;
+    p->outer_tol = 1e-10;
+    p->precision = AMG_PREC_F64;
+    p->max_rhs = 1;
+    p->tv_seed = 0;
+}
+
+int amg_read_parameters(const char* path, int* rows, int max_rows, int* nrows) {
+    if (!path || !rows || !nrows) return fail(AMG_ERR_INVALID, "null argument");
+    std::ifstream f(path);
+    if (!f) return fail(AMG_ERR_INVALID, "parameters file %s not found", path);
+    int v[6], n = 0;
+    while (f >> v[0] >> v[1] >> v[2] >> v[3] >> v[4] >> v[5]) {
+        if (n >= max_rows) return fail(AMG_ERR_INVALID, "more than %d parameter rows", max_rows);
+        for (int k = 0; k < 6; k++) rows[6 * n + k] = v[k];
+        n++;
+    }
+    if (!f.eof()) return fail(AMG_ERR_INVALID, "malformed parameters file %s (6 integers per row)", path);
+    *nrows = n;
+    return AMG_OK;
+}
+
+int amg_create(amg_ctx* out, int nx, int nt, int levels, const int* rows, double m0, const amg_params* params,
+               int device) {
+    if (!out) return fail(AMG_ERR_INVALID, "null context pointer");
+    *out = nullptr;
+    amg_params p;
+    if (params) p = *params; else amg_params_default(&p);
+    if (p.sap_gmres_m < 1 || p.kcycle_m < 1 || p.coarse_m < 1 || p.outer_m < 1 || p.outer_m > 22)
+        return fail(AMG_ERR_INVALID, "restart lengths must be >= 1 (outer <= 22)");
+    if (p.sap_gmres_restarts < 1 || p.kcycle_restarts < 1 || p.coarse_restarts < 1 || p.outer_restarts < 1)
+        return fail(AMG_ERR_INVALID, "restart counts must be >= 1");
+    if (p.precision != AMG_PREC_F64 && p.precision != AMG_PREC_MIXED) return fail(AMG_ERR_INVALID, "precision");
+    if (p.cycle != AMG_CYCLE_K && p.cycle != AMG_CYCLE_V) return fail(AMG_ERR_INVALID, "cycle");
+    if (p.max_rhs < 1) p.max_rhs = 1;
+    std::vector<LevelHost> lv;
+    CKR(build_levels(nx, nt, levels, rows, lv));
+    int ndev = 0;
+    CK(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) return fail(AMG_ERR_INVALID, "device %d of %d", device, ndev);
+    CK(cudaSetDevice(device));
+    amg_context* c = new amg_context();
+    c->device = device;
+    c->p = p;
+    c->m0 = m0;
+    c->nx = nx; c->nt = nt; c->N = nx * nt; c->L = levels;
+    c->lv = lv;
+    c->have_init.assign(levels, 0);
+    int rc = AMG_OK;
+    auto bail = [&](int r) { delete c; return r; };
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess)
+        return bail(fail(AMG_ERR_CUDA, "stream/event creation failed"));
+    const long long len = vlen0(c);
+    if ((rc = c->d.U.alloc((size_t)len * sizeof(double2))) < 0) return bail(rc);
+    if ((rc = c->d.W0.alloc((size_t)lv[0].ntest * len * sizeof(double2))) < 0) return bail(rc);
+    c->d.W.resize(levels);
+    c->d.links.resize(levels);
+    for (int l = 1; l < levels; l++) {
+        const LevelHost& h = lv[l];
+        if ((rc = c->d.links[l].alloc((size_t)h.n * 5 * h.K * h.K * sizeof(double2))) < 0) return bail(rc);
+        if (!h.coarsest && (rc = c->d.W[l].alloc((size_t)h.ntest * h.n * h.K * sizeof(double2))) < 0) return bail(rc);
+    }
+    if ((rc = ensure_capacity(c, p.max_rhs)) < 0) return bail(rc);
+    *out = c;
+    return AMG_OK;
+}
+
+int amg_destroy(amg_ctx c) {
+    if (!c) return AMG_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    cudaStream_t s = c->stream;
+    delete c;
+    if (s) cudaStreamDestroy(s);
+    return AMG_OK;
+}
+
+int amg_get_params(amg_ctx c, amg_params* out) {
+    if (!c || !out) return fail(AMG_ERR_INVALID, "null argument");
+    *out = c->p;
+    return AMG_OK;
+}
+
+int amg_set_mass(amg_ctx c, double m0) {
+    if (!c) return fail(AMG_ERR_INVALID, "null context");
+    c->m0 = m0;
+    c->setup_done = 0;
+    return AMG_OK;
+}
+
+int amg_level_info(amg_ctx c, int level, int* o) {
+    if (!c || !o) return fail(AMG_ERR_INVALID, "null argument");
+    if (level < 0 || level >= c->L) return fail(AMG_ERR_INVALID, "level %d out of range", level);
+    const LevelHost& h = c->lv[level];
+    o[0] = h.n; o[1] = h.nx; o[2] = h.nt; o[3] = h.K; o[4] = h.colors; o[5] = h.coarsest ? 0 : h.ntest;
+    return AMG_OK;
+}
+
+int amg_set_gauge(amg_ctx c, const double* U) {
+    if (!c || !U) return fail(AMG_ERR_INVALID, "null argument");
+    CKR(select_device(c));
+    CK(cudaMemcpyAsync(c->d.U.p, U, (size_t)vlen0(c) * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->gauge_set = 1;
+    c->setup_done = 0;
+    return AMG_OK;
+}
+
+int amg_dirac_apply_dev(amg_ctx c, const void* in, void* out, int nrhs, int dagger) {
+    if (!c || !in || !out || nrhs < 1) return fail(AMG_ERR_INVALID, "bad argument");
+    if (!c->gauge_set) return fail(AMG_ERR_STATE, "gauge field not set");
+    CKR(select_device(c));
+    launch_dirac<double>(c->d.U.as<double2>(), (const double2*)in, (double2*)out, c->nx, c->nt, nrhs, c->m0,
+                         dagger ? 1 : 0, c->stream);
+    CKL();
+    CK(cudaStreamSynchronize(c->stream));
+    return AMG_OK;
+}
+
+int amg_dirac_apply(amg_ctx c, const double* in, double* out, int nrhs, int dagger) {
+    if (!c || !in || !out || nrhs < 1) return fail(AMG_ERR_INVALID, "bad argument");
+    if (!c->gauge_set) return fail(AMG_ERR_STATE, "gauge field not set");
+    CKR(select_device(c));
+    DevBuf a, b;
+    const long long n = (long long)nrhs * vlen0(c);
+    CKR(to_dev(a, in, n, c->stream));
+    CKR(to_dev(b, nullptr, n, c->stream));
+    launch_dirac<double>(c->d.U.as<double2>(), a.as<double2>(), b.as<double2>(), c->nx, c->nt, nrhs, c->m0,
+                         dagger ? 1 : 0, c->stream);
+    CKL();
+    return to_host(out, b, n, c->stream);
+}
+
+int amg_dirac_apply_raw(const void* U_dev, const void* in_dev, void* out_dev, int nx, int nt, int nrhs, double m0,
+                        int dagger, void* stream) {
+    if (!U_dev || !in_dev || !out_dev || nx < 2 || nt < 2 || nrhs < 1) return fail(AMG_ERR_INVALID, "bad argument");
+    launch_dirac<double>((const double2*)U_dev, (const double2*)in_dev, (double2*)out_dev, nx, nt, nrhs, m0,
+                         dagger ? 1 : 0, (cudaStream_t)stream);
+    CKL();
+    return AMG_OK;
+}
+
+int amg_set_initial_test_vectors(amg_ctx c, int level, const double* W) {
+    if (!c || !W) return fail(AMG_ERR_INVALID, "null argument");
+    if (level < 0 || level >= c->L - 1) return fail(AMG_ERR_INVALID, "level %d has no test vectors", level);
+    CKR(select_device(c));
+    const LevelHost& h = c->lv[level];
+    const size_t bytes = (size_t)h.ntest * h.n * h.K * sizeof(double2);
+    void* dst = level == 0 ? c->d.W0.p : c->d.W[level].p;
+    CK(cudaMemcpyAsync(dst, W, bytes, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->have_init[level] = 1;
+    c->setup_done = 0;
+    return AMG_OK;
+}
+
+int amg_setup(amg_ctx c) {
+    if (!c) return fail(AMG_ERR_INVALID, "null context");
+    CKR(select_device(c));
+    CK(cudaEventRecord(c->ev0, c->stream));
+    int rc = do_setup(c);
+    if (rc < 0) return rc;
+    CK(cudaEventRecord(c->ev1, c->stream));
+    CK(cudaEventSynchronize(c->ev1));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    c->last_setup_ms = ms;
+    // imported initial vectors are consumed by one set-up
+    std::fill(c->have_init.begin(), c->have_init.end(), 0);
+    return AMG_OK;
+}
+
+int amg_get_test_vectors(amg_ctx c, int level, double* W) {
+    CKR(check_ready(c, level, true));
+    if (level >= c->L - 1) return fail(AMG_ERR_INVALID, "level %d has no test vectors", level);
+    const LevelHost& h = c->lv[level];
+    const void* src = level == 0 ? c->d.W0.p : c->d.W[level].p;
+    CK(cudaMemcpyAsync(W, src, (size_t)h.ntest * h.n * h.K * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return AMG_OK;
+}
+
+int amg_get_coarse_links(amg_ctx c, int level, double* G1, double* G2, double* G3) {
+    CKR(check_ready(c, level, true));
+    if (level < 1) return fail(AMG_ERR_INVALID, "coarse links exist for levels >= 1");
+    const LevelHost& h = c->lv[level];
+    const int K = h.K, col = h.colors;
+    std::vector<double2> lk((size_t)h.n * 5 * K * K);
+    CK(cudaMemcpyAsync(lk.data(), c->d.links[level].p, lk.size() * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    // links[x][h][j = 2b+bet][i = 2c+alf] -> G1[x][alf][bet][c][b], G2/G3[x][alf][bet][c][b][mu]
+    for (int x = 0; x < h.n; x++)
+        for (int alf = 0; alf < 2; alf++)
+            for (int bet = 0; bet < 2; bet++)
+                for (int cc = 0; cc < col; cc++)
+                    for (int bb = 0; bb < col; bb++) {
+                        const int i = 2 * cc + alf, j = 2 * bb + bet;
+                        auto at = [&](int hop) { return lk[(((size_t)x * 5 + hop) * K + j) * K + i]; };
+                        const size_t g1 = (((((size_t)x * 2 + alf) * 2 + bet) * col + cc) * col + bb);
+                        if (G1) { G1[2 * g1] = at(0).x; G1[2 * g1 + 1] = at(0).y; }
+                        for (int mu = 0; mu < 2; mu++) {
+                            const size_t g2 = g1 * 2 + mu;
+                            if (G2) { G2[2 * g2] = at(1 + mu).x; G2[2 * g2 + 1] = at(1 + mu).y; }
+                            if (G3) { G3[2 * g2] = at(3 + mu).x; G3[2 * g2 + 1] = at(3 + mu).y; }
+                        }
+                    }
+    return AMG_OK;
+}
+
+int amg_level_apply(amg_ctx c, int level, const double* in, double* out) {
+    CKR(check_ready(c, level, level > 0));
+    CKR(select_device(c));
+    const LevelHost& h = c->lv[level];
+    const long long nv = (long long)h.n * h.K;
+    DevBuf a, b;
+    CKR(to_dev(a, in, nv, c->stream));
+    CKR(to_dev(b, nullptr, nv, c->stream));
+    if (level == 0)
+        launch_dirac<double>(c->d.U.as<double2>(), a.as<double2>(), b.as<double2>(), c->nx, c->nt, 1, c->m0, 0,
+                             c->stream);
+    else
+        CKR(run_engine<double>(c, c->d, ENG_APPLY, level, 0, a.as<double2>(), 0, b.as<double2>(), 0, 1));
+    CKL();
+    return to_host(out, b, nv, c->stream);
+}
+
+int amg_restrict(amg_ctx c, int level, const double* in, double* out) {
+    CKR(check_ready(c, level, true));
+    if (level >= c->L - 1) return fail(AMG_ERR_INVALID, "no coarser level below %d", level);
+    CKR(select_device(c));
+    const LevelHost& h = c->lv[level];
+    const LevelHost& hn = c->lv[level + 1];
+    DevBuf a, b;
+    CKR(to_dev(a, in, (long long)h.n * h.K, c->stream));
+    CKR(to_dev(b, nullptr, (long long)hn.n * hn.K, c->stream));
+    if (level == 0) fine_restrict<double>(c, c->d, a.as<double2>(), b.as<double2>(), 1);
+    else CKR(run_engine<double>(c, c->d, ENG_RESTRICT, level, 0, a.as<double2>(), 0, b.as<double2>(), 0, 1));
+    CKL();
+    return to_host(out, b, (long long)hn.n * hn.K, c->stream);
+}
+
+int amg_prolong(amg_ctx c, int level, const double* in, double* out) {
+    CKR(check_ready(c, level, true));
+    if (level >= c->L - 1) return fail(AMG_ERR_INVALID, "no coarser level below %d", level);
+    CKR(select_device(c));
+    const LevelHost& h = c->lv[level];
+    const LevelHost& hn = c->lv[level + 1];
+    DevBuf a, b;
+    CKR(to_dev(a, in, (long long)hn.n * hn.K, c->stream));
+    CKR(to_dev(b, nullptr, (long long)h.n * h.K, c->stream));
+    if (level == 0) {
+        CK(cudaMemsetAsync(b.p, 0, (size_t)h.n * h.K * sizeof(double2), c->stream));
+        fine_prolong_add<double>(c, c->d, a.as<double2>(), b.as<double2>(), 1);
+    } else {
+        CKR(run_engine<double>(c, c->d, ENG_PROLONG, level, 0, a.as<double2>(), 0, b.as<double2>(), 0, 1));
+    }
+    CKL();
+    return to_host(out, b, (long long)h.n * h.K, c->stream);
+}
+
+int amg_sap(amg_ctx c, int level, const double* v, double* x, int nu) {
+    CKR(check_ready(c, level, level > 0));
+    if (level >= c->L - 1) return fail(AMG_ERR_INVALID, "no SAP on the coarsest level");
+    if (nu < 0) return fail(AMG_ERR_INVALID, "nu < 0");
+    CKR(select_device(c));
+    const LevelHost& h = c->lv[level];
+    const long long nv = (long long)h.n * h.K;
+    DevBuf a, b;
+    CKR(to_dev(a, v, nv, c->stream));
+    CKR(to_dev(b, x, nv, c->stream));
+    int conv = 0;
+    if (level == 0) {
+        if (!c->d.eng_args.p) CKR(build_engine<double>(c, c->d, c->Rcap));
+        CKR(fine_sap<double>(c, c->d, a.as<double2>(), nv, b.as<double2>(), nu, 1, 1));
+        CK(cudaMemcpyAsync(&conv, c->sap_flags.as<int>() + c->Rcap, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    } else {
+        CKR(run_engine<double>(c, c->d, ENG_SAP, level, nu, a.as<double2>(), 0, b.as<double2>(), 0, 1));
+        CK(cudaMemcpyAsync(&conv, c->d.eh.status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    }
+    CKR(to_host(x, b, nv, c->stream));
+    return conv ? AMG_OK : AMG_NOT_CONVERGED;
+}
+
+int amg_level_gmres(amg_ctx c, int level, const double* bh, double* xh, int* iterations) {
+    CKR(check_ready(c, level, true));
+    if (level < 1) return fail(AMG_ERR_UNSUPPORTED, "level GMRES is provided for levels >= 1");
+    CKR(select_device(c));
+    const LevelHost& h = c->lv[level];
+    const long long nv = (long long)h.n * h.K;
+    DevBuf a, b;
+    CKR(to_dev(a, bh, nv, c->stream));
+    CKR(to_dev(b, nullptr, nv, c->stream));
+    CKR(run_engine<double>(c, c->d, ENG_GMRES, level, 0, a.as<double2>(), 0, b.as<double2>(), 0, 1));
+    int it = 0;
+    CK(cudaMemcpyAsync(&it, c->d.eh.status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CKR(to_host(xh, b, nv, c->stream));
+    if (iterations) *iterations = it;
+    return AMG_OK;
+}
+
+int amg_cycle(amg_ctx c, int level, const double* eta, double* psi) {
+    CKR(check_ready(c, level, true));
+    CKR(select_device(c));
+    const LevelHost& h = c->lv[level];
+    const long long nv = (long long)h.n * h.K;
+    DevBuf a, b;
+    CKR(to_dev(a, eta, nv, c->stream));
+    CKR(to_dev(b, psi, nv, c->stream));
+    if (level == 0) {
+        CKR(fine_cycle<double>(c, c->d, a.as<double2>(), b.as<double2>(), 1, false));
+    } else {
+        CKR(run_engine<double>(c, c->d, c->p.cycle == AMG_CYCLE_K ? ENG_KCYCLE : ENG_VCYCLE, level, 0,
+                               a.as<double2>(), 0, b.as<double2>(), 0, 1));
+    }
+    CKL();
+    return to_host(psi, b, nv, c->stream);
+}
+
+int amg_kcycle_fgmres(amg_ctx c, int level, const double* bh, double* xh, int* iterations) {
+    CKR(check_ready(c, level, true));
+    if (level < 1) return fail(AMG_ERR_INVALID, "the K-cycle FGMRES exists for levels >= 1");
+    CKR(select_device(c));
+    const LevelHost& h = c->lv[level];
+    const long long nv = (long long)h.n * h.K;
+    DevBuf a, b;
+    CKR(to_dev(a, bh, nv, c->stream));
+    CKR(to_dev(b, nullptr, nv, c->stream));
+    CKR(run_engine<double>(c, c->d, ENG_KFGMRES, level, 0, a.as<double2>(), 0, b.as<double2>(), 0, 1));
+    int it = 0;
+    CK(cudaMemcpyAsync(&it, c->d.eh.status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CKR(to_host(xh, b, nv, c->stream));
+    if (iterations) *iterations = it;
+    return AMG_OK;
+}
+
+int amg_solve_dev(amg_ctx c, const void* b_dev, void* x_dev, int nrhs, amg_solve_info* info) {
+    CKR(check_ready(c, 0, true));
+    if (!b_dev || !x_dev || nrhs < 1) return fail(AMG_ERR_INVALID, "bad argument");
+    CKR(select_device(c));
+    if (nrhs > c->Rcap) {
+        CKR(ensure_capacity(c, nrhs));
+        CKR(build_engine<double>(c, c->d, std::max(c->d.eng_cap, nrhs)));
+        if (c->p.precision == AMG_PREC_MIXED) CKR(build_engine<float>(c, c->f, std::max(c->f.eng_cap, nrhs)));
+    }
+    CK(cudaEventRecord(c->ev0, c->stream));
+    int rc = outer_fgmres(c, (const double2*)b_dev, (double2*)x_dev, nrhs, info);
+    if (rc < 0) return rc;
+    CK(cudaEventRecord(c->ev1, c->stream));
+    CK(cudaEventSynchronize(c->ev1));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    c->last_solve_ms = ms;
+    int flags = 0;
+    CK(cudaMemcpy(&flags, c->d.eh.flags, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flags) return fail(AMG_ERR_UNSUPPORTED, "engine reported flags %d", flags);
+    return rc;
+}
+
+int amg_solve(amg_ctx c, const double* b, double* x, int nrhs, amg_solve_info* info) {
+    CKR(check_ready(c, 0, true));
+    if (!b || !x || nrhs < 1) return fail(AMG_ERR_INVALID, "bad argument");
+    CKR(select_device(c));
+    if (nrhs > c->Rcap) {
+        CKR(ensure_capacity(c, nrhs));
+        CKR(build_engine<double>(c, c->d, std::max(c->d.eng_cap, nrhs)));
+        if (c->p.precision == AMG_PREC_MIXED) CKR(build_engine<float>(c, c->f, std::max(c->f.eng_cap, nrhs)));
+    }
+    const long long n = (long long)nrhs * vlen0(c);
+    CK(cudaMemcpyAsync(c->b.p, b, (size_t)n * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+    int rc = amg_solve_dev(c, c->b.p, c->x.p, nrhs, info);
+    if (rc < 0) return rc;
+    CK(cudaMemcpyAsync(x, c->x.p, (size_t)n * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return rc;
+}
+
+int amg_residual_history(amg_ctx c, double* out, int max_len, int* len) {
+    if (!c || !len) return fail(AMG_ERR_INVALID, "null argument");
+    const int n = (int)c->history.size();
+    *len = n;
+    if (out)
+        for (int i = 0; i < std::min(n, max_len); i++) out[i] = c->history[i];
+    return AMG_OK;
+}
+
+int amg_solve_adjoint(amg_ctx c, const double* g, double* lambda, int nrhs, amg_solve_info* info) {
+    (void)c; (void)g; (void)lambda; (void)nrhs; (void)info;
+    return fail(AMG_ERR_UNSUPPORTED, "adjoint solve not built yet");
+}
+int amg_solve_adjoint_dev(amg_ctx c, const void* g, void* lambda, int nrhs, amg_solve_info* info) {
+    (void)c; (void)g; (void)lambda; (void)nrhs; (void)info;
+    return fail(AMG_ERR_UNSUPPORTED, "adjoint solve not built yet");
+}
+int amg_force(amg_ctx c, const double* lambda, const double* x, int nrhs, double* F) {
+    (void)c; (void)lambda; (void)x; (void)nrhs; (void)F;
+    return fail(AMG_ERR_UNSUPPORTED, "force not built yet");
+}
+int amg_force_dev(amg_ctx c, const void* lambda, const void* x, int nrhs, void* F) {
+    (void)c; (void)lambda; (void)x; (void)nrhs; (void)F;
+    return fail(AMG_ERR_UNSUPPORTED, "force not built yet");
+}
+
+int amg_last_timings(amg_ctx c, double* setup_ms, double* solve_ms) {
+    if (!c) return fail(AMG_ERR_INVALID, "null context");
+    if (setup_ms) *setup_ms = c->last_setup_ms;
+    if (solve_ms) *solve_ms = c->last_solve_ms;
+    return AMG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,582 @@
+// Fine-lattice (level 0) kernels: the U(1) Wilson-Dirac stencil, the fused residual,
+// restriction / prolongation between level 0 and level 1, the SAP block solver and the
+// BLAS-1 kernels of the outer FGMRES.
+//
+// Layout: psi[rhs][n][spin] complex (double2 or float2), n = x*Nt + t; U[n][mu].
+#include "kernels.h"
+
+namespace amgb {
+
+// ---------------------------------------------------------------------------------
+// D_phi / D_dagger_phi (src/dirac_operator.cpp:3-54) for one site.  With forward
+// neighbours (a,b) = psi(n+t), (c,d) = psi(n+x) and backward (e,f) = psi(n-t),
+// (g,h) = psi(n-x):
+//   D:   t0 = sR U0 (a-b), t1 = U1 (c+id), t2 = sL U0*(n-t) (e+f), t3 = U1*(n-x) (g-ih)
+//        out0 = (m0+2) p0 - (t0+t1+t2+t3)/2,  out1 = (m0+2) p1 - (-t0 - i t1 + t2 + i t3)/2
+//   D^+: the (1 -/+ sigma) projectors swap between forward and backward hops.
+// ---------------------------------------------------------------------------------
+template <typename T, bool DAG>
+__device__ __forceinline__ void dirac_site(const cx<T>* __restrict__ U, const cx<T>* __restrict__ psi,
+                                           int n, int nx, int nt, T mass, cx<T>& o0, cx<T>& o1) {
+    const int x = n / nt, t = n - x * nt;
+    const int r0 = x * nt + ((t + 1 == nt) ? 0 : t + 1);
+    const int r1 = ((x + 1 == nx) ? 0 : x + 1) * nt + t;
+    const int l0 = x * nt + ((t == 0) ? nt - 1 : t - 1);
+    const int l1 = ((x == 0) ? nx - 1 : x - 1) * nt + t;
+    const cx<T> u0 = U[2 * n], u1 = U[2 * n + 1];
+    const cx<T> ul0 = cconj(U[2 * l0]), ul1 = cconj(U[2 * l1 + 1]);
+    const cx<T> a = psi[2 * r0], b = psi[2 * r0 + 1];
+    const cx<T> c = psi[2 * r1], d = psi[2 * r1 + 1];
+    const cx<T> e = psi[2 * l0], f = psi[2 * l0 + 1];
+    const cx<T> g = psi[2 * l1], h = psi[2 * l1 + 1];
+    const cx<T> p0 = psi[2 * n], p1 = psi[2 * n + 1];
+    const T sR = (t == nt - 1) ? T(-1) : T(1);
+    const T sL = (t == 0) ? T(-1) : T(1);
+    cx<T> t0, t1, t2, t3;
+    if (!DAG) {
+        t0 = sR * cmul(u0, a - b);
+        t1 = cmul(u1, c + cmuli(d));
+        t2 = sL * cmul(ul0, e + f);
+        t3 = cmul(ul1, g - cmuli(h));
+        o0 = mass * p0 - T(0.5) * (t0 + t1 + t2 + t3);
+        o1 = mass * p1 - T(0.5) * ((t2 - t0) + cmuli(t3 - t1));
+    } else {
+        t0 = sL * cmul(ul0, e - f);
+        t1 = cmul(ul1, g + cmuli(h));
+        t2 = sR * cmul(u0, a + b);
+        t3 = cmul(u1, c - cmuli(d));
+        o0 = mass * p0 - T(0.5) * (t0 + t1 + t2 + t3);
+        o1 = mass * p1 - T(0.5) * ((t2 - t0) + cmuli(t3 - t1));
+    }
+}
+
+template <typename T, bool DAG>
+__global__ void __launch_bounds__(256) k_dirac(const cx<T>* __restrict__ U, const cx<T>* __restrict__ in,
+                                               cx<T>* __restrict__ out, int nx, int nt, T m0) {
+    const int N = nx * nt;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    const long long off = (long long)blockIdx.y * N * 2;
+    cx<T> o0, o1;
+    dirac_site<T, DAG>(U, in + off, n, nx, nt, m0 + T(2), o0, o1);
+    out[off + 2 * n] = o0;
+    out[off + 2 * n + 1] = o1;
+}
+
+// r = b - D x, and per-CTA partial sums of |r|^2 (deterministic second stage)
+template <typename T>
+__global__ void __launch_bounds__(256) k_residual(const cx<T>* __restrict__ U, const cx<T>* __restrict__ b,
+                                                  long long bstride, const cx<T>* __restrict__ x,
+                                                  cx<T>* __restrict__ r, int nx, int nt, T m0,
+                                                  double* __restrict__ partial, const int* __restrict__ act) {
+    __shared__ double red[8];
+    if (act && !act[blockIdx.y]) return;
+    const int N = nx * nt;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    const long long off = (long long)blockIdx.y * N * 2;
+    const cx<T>* bb = b + (long long)blockIdx.y * bstride;
+    double nrm = 0;
+    if (n < N) {
+        cx<T> o0, o1;
+        dirac_site<T, false>(U, x + off, n, nx, nt, m0 + T(2), o0, o1);
+        cx<T> r0 = bb[2 * n] - o0, r1 = bb[2 * n + 1] - o1;
+        r[off + 2 * n] = r0;
+        r[off + 2 * n + 1] = r1;
+        nrm = (double)cnorm2(r0) + (double)cnorm2(r1);
+    }
+    nrm = cta_sum(nrm, red);
+    if (partial && threadIdx.x == 0) partial[(long long)blockIdx.y * gridDim.x + blockIdx.x] = nrm;
+}
+
+// out[rhs] = sum_k partial[rhs][k] in a fixed order
+__global__ void k_sum_partials(const double* __restrict__ partial, int nparts, double* __restrict__ out) {
+    __shared__ double red[32];
+    double s = 0;
+    for (int k = threadIdx.x; k < nparts; k += blockDim.x) s += partial[(long long)blockIdx.x * nparts + k];
+    s = cta_sum(s, red);
+    if (threadIdx.x == 0) out[blockIdx.x] = s;
+}
+
+// ---------------------------------------------------------------------------------
+// Level::Pt_v at level 0 (src/level.cpp:212-237, colors = 1):
+//   out[rhs][nc][2cc+s] = sum_{n in block nc} conj(W[cc][n][s]) v[rhs][n][s]
+// Grid (chunk, block, rhs); per-chunk partials reduced by k_restrict0_sum in chunk order.
+// ---------------------------------------------------------------------------------
+template <typename T, typename TW, int NV>
+__global__ void __launch_bounds__(256) k_restrict0(const TW* __restrict__ W, const cx<T>* __restrict__ v,
+                                                   cx<T>* __restrict__ partial, int nx, int nt, int bt, int xe,
+                                                   int te, int nchunk, int ntest) {
+    extern __shared__ __align__(16) unsigned char smraw_r[];
+    T* red = reinterpret_cast<T*>(smraw_r);
+    const int N = nx * nt;
+    const int chunk = blockIdx.x, nc = blockIdx.y, rhs = blockIdx.z;
+    const int bxi = nc / bt, bti = nc - bxi * bt;
+    const int spb = xe * te;
+    const int per = (spb + nchunk - 1) / nchunk;
+    const int q0 = chunk * per, q1 = min(spb, q0 + per);
+    const cx<T>* vv = v + (long long)rhs * N * 2;
+    cx<T> acc[NV][2];
+#pragma unroll
+    for (int k = 0; k < NV; k++) { acc[k][0] = czero<T>(); acc[k][1] = czero<T>(); }
+    for (int q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
+        const int mx = q / te, mt = q - mx * te;
+        const long long n = (long long)(bxi * xe + mx) * nt + (bti * te + mt);
+        const cx<T> p0 = vv[2 * n], p1 = vv[2 * n + 1];
+#pragma unroll
+        for (int k = 0; k < NV; k++) {
+            if (k < ntest) {
+                cx<T> w0 = ccast<T>(load_cx(W + ((long long)k * N + n) * 2));
+                cx<T> w1 = ccast<T>(load_cx(W + ((long long)k * N + n) * 2 + 1));
+                cfmac(acc[k][0], w0, p0);
+                cfmac(acc[k][1], w1, p1);
+            }
+        }
+    }
+    // CTA reduction of 4*NV reals: warp shuffles, then one value per warp in smem
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+        if (k >= ntest) break;
+#pragma unroll
+        for (int s = 0; s < 2; s++) {
+            T xr = warp_sum(acc[k][s].x), xi = warp_sum(acc[k][s].y);
+            if (lane == 0) { red[((k * 2 + s) * nw + wid) * 2] = xr; red[((k * 2 + s) * nw + wid) * 2 + 1] = xi; }
+        }
+    }
+    __syncthreads();
+    for (int o = threadIdx.x; o < ntest * 2; o += blockDim.x) {
+        T sr = 0, si = 0;
+        for (int w = 0; w < nw; w++) { sr += red[(o * nw + w) * 2]; si += red[(o * nw + w) * 2 + 1]; }
+        // o = k*2 + s  ->  coarse dof 2k + s
+        partial[(((long long)rhs * gridDim.y + nc) * nchunk + chunk) * (2 * ntest) + o] = mk<T>(sr, si);
+    }
+}
+
+template <typename T>
+__global__ void k_restrict0_sum(const cx<T>* __restrict__ partial, cx<T>* __restrict__ out, int nblk, int nchunk,
+                                int K1) {
+    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    const int rhs = blockIdx.y;
+    if (o >= nblk * K1) return;
+    const int nc = o / K1, d = o - nc * K1;
+    const cx<T>* p = partial + (((long long)rhs * nblk + nc) * nchunk) * K1 + d;
+    cx<T> s = czero<T>();
+    for (int c = 0; c < nchunk; c++) s += p[(long long)c * K1];
+    out[(long long)rhs * nblk * K1 + o] = s;
+}
+
+// Level::P_v at level 0 (src/level.cpp:182-209) added into psi:
+//   psi[rhs][n][s] += sum_cc W[cc][n][s] vc[rhs][nc(n)][2cc+s]
+template <typename T, typename TW>
+__global__ void __launch_bounds__(256) k_prolong0_add(const TW* __restrict__ W, const cx<T>* __restrict__ vc,
+                                                      cx<T>* __restrict__ psi, int nx, int nt, int bt, int xe,
+                                                      int te, int ntest, int nblk, int nrhs) {
+    const int N = nx * nt;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    const int x = n / nt, t = n - x * nt;
+    const int nc = (x / xe) * bt + (t / te);
+    for (int rhs = 0; rhs < nrhs; rhs++) {
+        const cx<T>* pv = vc + ((long long)rhs * nblk + nc) * 2 * ntest;
+        cx<T> a0 = czero<T>(), a1 = czero<T>();
+        for (int k = 0; k < ntest; k++) {
+            cx<T> w0 = ccast<T>(load_cx(W + ((long long)k * N + n) * 2));
+            cx<T> w1 = ccast<T>(load_cx(W + ((long long)k * N + n) * 2 + 1));
+            cfma(a0, w0, pv[2 * k]);
+            cfma(a1, w1, pv[2 * k + 1]);
+        }
+        cx<T>* o = psi + (long long)rhs * N * 2 + 2 * n;
+        o[0] += a0;
+        o[1] += a1;
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// SAP block solve at level 0 (src/sap.cpp:44-62 with the block operator of
+// src/level.cpp:304-368 at colors = 1): one CTA per (block of the colour, source).
+// rhs b = r restricted to the block, GMRES(m, restarts, tol) with x0 = b, then
+// x[block] += solution.  Vectors live in shared memory when they fit, otherwise in a
+// global scratch slab per CTA.
+// ---------------------------------------------------------------------------------
+template <typename T>
+struct FineBlock {
+    int nx, nt, sbt, sxe, ste, x0, t0;   // block origin
+    T mass;
+    const cx<T>* u;                      // block links [S][2] (staged)
+};
+
+// out = D_B in on the block (neighbours outside the block dropped, fermionic sign kept)
+template <typename T>
+__device__ void fine_block_apply(const FineBlock<T>& B, const cx<T>* in, cx<T>* out) {
+    const int S = B.sxe * B.ste;
+    for (int m = threadIdx.x; m < S; m += blockDim.x) {
+        const int mx = m / B.ste, mt = m - mx * B.ste;
+        const int t = B.t0 + mt;
+        const T sR = (t == B.nt - 1) ? T(-1) : T(1);
+        const T sL = (t == 0) ? T(-1) : T(1);
+        // neighbour local indices (or -1 when outside the block); periodic wrap stays
+        // inside only when the block spans the whole direction
+        int mr0 = -1, mr1 = -1, ml0 = -1, ml1 = -1;
+        if (mt + 1 < B.ste) mr0 = m + 1; else if (B.ste == B.nt) mr0 = mx * B.ste;
+        if (mt > 0) ml0 = m - 1; else if (B.ste == B.nt) ml0 = mx * B.ste + B.ste - 1;
+        if (mx + 1 < B.sxe) mr1 = m + B.ste; else if (B.sxe == B.nx) mr1 = mt;
+        if (mx > 0) ml1 = m - B.ste; else if (B.sxe == B.nx) ml1 = (B.sxe - 1) * B.ste + mt;
+        const cx<T> p0 = in[2 * m], p1 = in[2 * m + 1];
+        cx<T> t0 = czero<T>(), t1 = czero<T>(), t2 = czero<T>(), t3 = czero<T>();
+        if (mr0 >= 0) t0 = sR * cmul(B.u[2 * m], in[2 * mr0] - in[2 * mr0 + 1]);
+        if (mr1 >= 0) t1 = cmul(B.u[2 * m + 1], in[2 * mr1] + cmuli(in[2 * mr1 + 1]));
+        if (ml0 >= 0) t2 = sL * cmul(cconj(B.u[2 * ml0]), in[2 * ml0] + in[2 * ml0 + 1]);
+        if (ml1 >= 0) t3 = cmul(cconj(B.u[2 * ml1 + 1]), in[2 * ml1] - cmuli(in[2 * ml1 + 1]));
+        out[2 * m] = B.mass * p0 - T(0.5) * (t0 + t1 + t2 + t3);
+        out[2 * m + 1] = B.mass * p1 - T(0.5) * ((t2 - t0) + cmuli(t3 - t1));
+    }
+    __syncthreads();
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_sap0_blocks(const cx<T>* __restrict__ U, const cx<T>* __restrict__ r,
+                                                     cx<T>* __restrict__ x, const int* __restrict__ blocks, int ncol,
+                                                     int nx, int nt, int sbt, int sxe, int ste, T m0, int m,
+                                                     int restarts, T tol, int use_smem, cx<T>* gscratch,
+                                                     int* __restrict__ iters_out, const int* __restrict__ act) {
+    extern __shared__ __align__(16) unsigned char smraw_s[];
+    const int seg = blockIdx.x, rhs = blockIdx.y;
+    if (act && !act[rhs]) return;
+    const int block = blocks[seg];
+    const int S = sxe * ste, len = 2 * S;
+    const int N = nx * nt;
+    const int bxi = block / sbt, bti = block - bxi * sbt;
+    FineBlock<T> B;
+    B.nx = nx; B.nt = nt; B.sbt = sbt; B.sxe = sxe; B.ste = ste;
+    B.x0 = bxi * sxe; B.t0 = bti * ste; B.mass = m0 + T(2);
+    // carve: red | state | u | b | x | w | V[m+1]
+    char* p = reinterpret_cast<char*>(smraw_s);
+    T* red = reinterpret_cast<T*>(p); p += 2 * 32 * sizeof(T);
+    GmState<T> st = gm_state_at<T>(p, 1, m); p += gm_state_bytes(1, m, sizeof(T));
+    cx<T>* vec;
+    if (use_smem) vec = reinterpret_cast<cx<T>*>(p);
+    else vec = gscratch + ((long long)rhs * gridDim.x + seg) * (long long)(m + 5) * len;
+    cx<T>* u = vec;
+    cx<T>* b = u + len;
+    cx<T>* xs = b + len;
+    cx<T>* w = xs + len;
+    cx<T>* V = w + len;
+    const cx<T>* rr = r + (long long)rhs * N * 2;
+    for (int q = threadIdx.x; q < S; q += blockDim.x) {
+        const int mx = q / ste, mt = q - mx * ste;
+        const long long n = (long long)(B.x0 + mx) * nt + (B.t0 + mt);
+        u[2 * q] = U[2 * n]; u[2 * q + 1] = U[2 * n + 1];
+        b[2 * q] = rr[2 * n]; b[2 * q + 1] = rr[2 * n + 1];
+    }
+    __syncthreads();
+    B.u = u;
+    Seg<T> sp = make_seg<T>(1, len, red);
+    auto op = [&](const cx<T>* in, cx<T>* out) { fine_block_apply(B, in, out); };
+    auto ident = [](int, const cx<T>*, cx<T>*, const int*) {};
+    seg_fgmres(sp, op, ident, b, xs, V, V, w, st, m, restarts, tol);
+    cx<T>* xx = x + (long long)rhs * N * 2;
+    for (int q = threadIdx.x; q < S; q += blockDim.x) {
+        const int mx = q / ste, mt = q - mx * ste;
+        const long long n = (long long)(B.x0 + mx) * nt + (B.t0 + mt);
+        xx[2 * n] += xs[2 * q];
+        xx[2 * n + 1] += xs[2 * q + 1];
+    }
+    if (iters_out && threadIdx.x == 0) iters_out[rhs * gridDim.x + seg] = st.iters[0];
+}
+
+// ---------------------------------------------------------------------------------
+// BLAS-1 for the outer FGMRES (FP64).  Vectors are [rhs][len]; V bases [j][rhs][len].
+// ---------------------------------------------------------------------------------
+// partial[rhs][k][blk] = sum_e w[e] * conj(V_k[e]) for k < nv, and |w|^2 at k = nv
+__global__ void __launch_bounds__(256) k_multidot(const double2* __restrict__ w, const double2* __restrict__ V,
+                                                  long long len, long long vstride, int nv, int nrhs,
+                                                  double2* __restrict__ partial) {
+    __shared__ double red[2 * 8 * 24];
+    const int rhs = blockIdx.y;
+    const double2* ww = w + (long long)rhs * len;
+    double ax[24], ay[24];
+    for (int k = 0; k <= nv; k++) { ax[k] = 0; ay[k] = 0; }
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (long long)gridDim.x * blockDim.x) {
+        const double2 a = ww[e];
+#pragma unroll 4
+        for (int k = 0; k < nv; k++) {
+            const double2 b = V[(long long)k * vstride + (long long)rhs * len + e];
+            ax[k] += a.x * b.x + a.y * b.y;
+            ay[k] += a.y * b.x - a.x * b.y;
+        }
+        ax[nv] += a.x * a.x + a.y * a.y;
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int k = 0; k <= nv; k++) {
+        double sx = warp_sum(ax[k]), sy = warp_sum(ay[k]);
+        if (lane == 0) { red[(k * 8 + wid) * 2] = sx; red[(k * 8 + wid) * 2 + 1] = sy; }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k <= nv; k += blockDim.x) {
+        double sx = 0, sy = 0;
+        for (int q = 0; q < 8; q++) { sx += red[(k * 8 + q) * 2]; sy += red[(k * 8 + q) * 2 + 1]; }
+        partial[((long long)rhs * (nv + 1) + k) * gridDim.x + blockIdx.x] = make_double2(sx, sy);
+    }
+}
+
+__global__ void k_multidot_sum(const double2* __restrict__ partial, int nparts, double2* __restrict__ out) {
+    __shared__ double red[64];
+    const int o = blockIdx.x;   // (rhs, k) flattened
+    double sx = 0, sy = 0;
+    for (int q = threadIdx.x; q < nparts; q += blockDim.x) {
+        double2 v = partial[(long long)o * nparts + q];
+        sx += v.x; sy += v.y;
+    }
+    sx = cta_sum(sx, red);
+    sy = cta_sum(sy, red + 32);
+    if (threadIdx.x == 0) out[o] = make_double2(sx, sy);
+}
+
+// w[rhs] -= sum_k h[rhs][k] V_k[rhs]   (masked by act[rhs])
+__global__ void __launch_bounds__(256) k_multiaxpy(double2* __restrict__ w, const double2* __restrict__ V,
+                                                   long long len, long long vstride, int nv,
+                                                   const double2* __restrict__ h, int hstride,
+                                                   const int* __restrict__ act) {
+    const int rhs = blockIdx.y;
+    if (act && !act[rhs]) return;
+    double2* ww = w + (long long)rhs * len;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (long long)gridDim.x * blockDim.x) {
+        double2 a = ww[e];
+        for (int k = 0; k < nv; k++) {
+            const double2 hk = h[(long long)rhs * hstride + k];
+            const double2 b = V[(long long)k * vstride + (long long)rhs * len + e];
+            a.x -= hk.x * b.x - hk.y * b.y;
+            a.y -= hk.x * b.y + hk.y * b.x;
+        }
+        ww[e] = a;
+    }
+}
+
+// w[rhs] -= sum_k h[rhs][k] V_k[rhs], then partial[rhs][k][blk] = sum_e w[e] conj(V_k[e]) for
+// k < nd and |w|^2 at k = nd, all from one pass over w and the basis (classical Gram-Schmidt
+// with re-orthogonalisation needs both halves back to back).
+__global__ void __launch_bounds__(256) k_axpy_multidot(double2* __restrict__ w, const double2* __restrict__ V,
+                                                       long long len, long long vstride, int nv,
+                                                       const double2* __restrict__ h, int hstride, int nd,
+                                                       const int* __restrict__ act, double2* __restrict__ partial) {
+    __shared__ double red[2 * 8 * 24];
+    const int rhs = blockIdx.y;
+    const bool on = !act || act[rhs];
+    double2* ww = w + (long long)rhs * len;
+    double ax[24], ay[24];
+    for (int k = 0; k <= nd; k++) { ax[k] = 0; ay[k] = 0; }
+    double2 hk[24];
+    for (int k = 0; k < nv; k++) hk[k] = h[(long long)rhs * hstride + k];
+    if (on) {
+        for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (long long)gridDim.x * blockDim.x) {
+            double2 a = ww[e];
+            for (int k = 0; k < nv; k++) {
+                const double2 b = V[(long long)k * vstride + (long long)rhs * len + e];
+                a.x -= hk[k].x * b.x - hk[k].y * b.y;
+                a.y -= hk[k].x * b.y + hk[k].y * b.x;
+            }
+            ww[e] = a;
+            for (int k = 0; k < nd; k++) {
+                const double2 b = V[(long long)k * vstride + (long long)rhs * len + e];
+                ax[k] += a.x * b.x + a.y * b.y;
+                ay[k] += a.y * b.x - a.x * b.y;
+            }
+            ax[nd] += a.x * a.x + a.y * a.y;
+        }
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int k = 0; k <= nd; k++) {
+        double sx = warp_sum(ax[k]), sy = warp_sum(ay[k]);
+        if (lane == 0) { red[(k * 8 + wid) * 2] = sx; red[(k * 8 + wid) * 2 + 1] = sy; }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k <= nd; k += blockDim.x) {
+        double sx = 0, sy = 0;
+        for (int q = 0; q < 8; q++) { sx += red[(k * 8 + q) * 2]; sy += red[(k * 8 + q) * 2 + 1]; }
+        partial[((long long)rhs * (nd + 1) + k) * gridDim.x + blockIdx.x] = make_double2(sx, sy);
+    }
+}
+
+// x[rhs] += sum_k c[rhs][k] Z_k[rhs]  (masked)
+__global__ void __launch_bounds__(256) k_multiaxpy_add(double2* __restrict__ x, const double2* __restrict__ Z,
+                                                       long long len, long long vstride, int nv,
+                                                       const double2* __restrict__ c, int cstride,
+                                                       const int* __restrict__ nvr, const int* __restrict__ act) {
+    const int rhs = blockIdx.y;
+    if (act && !act[rhs]) return;
+    const int n = nvr ? nvr[rhs] : nv;
+    double2* xx = x + (long long)rhs * len;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (long long)gridDim.x * blockDim.x) {
+        double2 a = xx[e];
+        for (int k = 0; k < n; k++) {
+            const double2 ck = c[(long long)rhs * cstride + k];
+            const double2 b = Z[(long long)k * vstride + (long long)rhs * len + e];
+            a.x += ck.x * b.x - ck.y * b.y;
+            a.y += ck.x * b.y + ck.y * b.x;
+        }
+        xx[e] = a;
+    }
+}
+
+// y[rhs] = s[rhs] * x[rhs]  (masked; s real)
+__global__ void k_scale(double2* __restrict__ y, const double2* __restrict__ x, long long len,
+                        const double* __restrict__ s, const int* __restrict__ act) {
+    const int rhs = blockIdx.y;
+    if (act && !act[rhs]) return;
+    const double f = s[rhs];
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (long long)gridDim.x * blockDim.x)
+        y[(long long)rhs * len + e] = f * x[(long long)rhs * len + e];
+}
+
+// precision conversions between the FP64 outer vectors and the FP32 cycle
+__global__ void k_d2f(float2* __restrict__ y, const double2* __restrict__ x, long long n) {
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+        y[e] = make_float2((float)x[e].x, (float)x[e].y);
+}
+__global__ void k_f2d(double2* __restrict__ y, const float2* __restrict__ x, long long n) {
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+        y[e] = make_double2((double)x[e].x, (double)x[e].y);
+}
+__global__ void k_d2bf(__nv_bfloat162* __restrict__ y, const double2* __restrict__ x, long long n) {
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+        y[e] = __floats2bfloat162_rn((float)x[e].x, (float)x[e].y);
+}
+
+// ---------------------------------------------------------------------------------
+// host launchers
+// ---------------------------------------------------------------------------------
+template <typename T>
+void launch_dirac(const cx<T>* U, const cx<T>* in, cx<T>* out, int nx, int nt, int nrhs, T m0, int dagger,
+                  cudaStream_t s) {
+    dim3 grid((nx * nt + 255) / 256, nrhs);
+    if (dagger) k_dirac<T, true><<<grid, 256, 0, s>>>(U, in, out, nx, nt, m0);
+    else k_dirac<T, false><<<grid, 256, 0, s>>>(U, in, out, nx, nt, m0);
+}
+
+template <typename T>
+void launch_residual(const cx<T>* U, const cx<T>* b, long long bstride, const cx<T>* x, cx<T>* r, int nx, int nt,
+                     int nrhs, T m0, double* partial, double* norm2_out, const int* act, cudaStream_t s) {
+    const int nblk = (nx * nt + 255) / 256;
+    dim3 grid(nblk, nrhs);
+    k_residual<T><<<grid, 256, 0, s>>>(U, b, bstride, x, r, nx, nt, m0, norm2_out ? partial : nullptr, act);
+    if (norm2_out) k_sum_partials<<<nrhs, 256, 0, s>>>(partial, nblk, norm2_out);
+}
+
+// |v[rhs]|^2 for [nrhs][len] vectors, deterministic
+template <typename T>
+__global__ void __launch_bounds__(256) k_norm2(const cx<T>* __restrict__ v, long long len, long long stride,
+                                               double* __restrict__ partial) {
+    __shared__ double red[8];
+    const cx<T>* vv = v + (long long)blockIdx.y * stride;
+    double s = 0;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (long long)gridDim.x * blockDim.x)
+        s += (double)cnorm2(vv[e]);
+    s = cta_sum(s, red);
+    if (threadIdx.x == 0) partial[(long long)blockIdx.y * gridDim.x + blockIdx.x] = s;
+}
+template <typename T>
+void launch_norm2(const cx<T>* v, long long len, long long stride, int nrhs, double* partial, double* out,
+                  cudaStream_t s) {
+    const int np = 296;
+    dim3 grid(np, nrhs);
+    k_norm2<T><<<grid, 256, 0, s>>>(v, len, stride, partial);
+    k_sum_partials<<<nrhs, 256, 0, s>>>(partial, np, out);
+}
+int residual_partials(int nx, int nt) { return (nx * nt + 255) / 256; }
+
+template <typename T, typename TW>
+void launch_restrict0(const TW* W, const cx<T>* v, cx<T>* out, cx<T>* partial, int nx, int nt, int bx, int bt,
+                      int ntest, int nrhs, int nchunk, cudaStream_t s) {
+    const int xe = nx / bx, te = nt / bt, nblk = bx * bt;
+    dim3 grid(nchunk, nblk, nrhs);
+    const int smem = 4 * ntest * 8 * sizeof(T) * 2;
+    if (ntest <= 8) k_restrict0<T, TW, 8><<<grid, 256, smem, s>>>(W, v, partial, nx, nt, bt, xe, te, nchunk, ntest);
+    else if (ntest <= 16) k_restrict0<T, TW, 16><<<grid, 256, smem, s>>>(W, v, partial, nx, nt, bt, xe, te, nchunk, ntest);
+    else k_restrict0<T, TW, 32><<<grid, 256, smem, s>>>(W, v, partial, nx, nt, bt, xe, te, nchunk, ntest);
+    dim3 g2((nblk * 2 * ntest + 127) / 128, nrhs);
+    k_restrict0_sum<T><<<g2, 128, 0, s>>>(partial, out, nblk, nchunk, 2 * ntest);
+}
+
+template <typename T, typename TW>
+void launch_prolong0_add(const TW* W, const cx<T>* vc, cx<T>* psi, int nx, int nt, int bx, int bt, int ntest,
+                         int nrhs, cudaStream_t s) {
+    const int xe = nx / bx, te = nt / bt;
+    k_prolong0_add<T, TW><<<(nx * nt + 255) / 256, 256, 0, s>>>(W, vc, psi, nx, nt, bt, xe, te, ntest, bx * bt, nrhs);
+}
+
+template <typename T>
+int sap0_smem_bytes(int S, int m, int use_smem) {
+    int b = 2 * 32 * (int)sizeof(T) + gm_state_bytes(1, m, sizeof(T));
+    if (use_smem) b += (m + 5) * 2 * S * (int)sizeof(cx<T>);
+    return b;
+}
+
+template <typename T>
+cudaError_t launch_sap0(const cx<T>* U, const cx<T>* r, cx<T>* x, const int* blocks, int ncol, int nrhs, int nx,
+                        int nt, int sbt, int sxe, int ste, T m0, int m, int restarts, T tol, int use_smem,
+                        cx<T>* gscratch, int* iters, const int* act, cudaStream_t s) {
+    const int bytes = sap0_smem_bytes<T>(sxe * ste, m, use_smem);
+    cudaError_t e = cudaFuncSetAttribute(k_sap0_blocks<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+    dim3 grid(ncol, nrhs);
+    k_sap0_blocks<T><<<grid, 256, bytes, s>>>(U, r, x, blocks, ncol, nx, nt, sbt, sxe, ste, m0, m, restarts, tol,
+                                               use_smem, gscratch, iters, act);
+    return cudaGetLastError();
+}
+
+void launch_multidot(const double2* w, const double2* V, long long len, long long vstride, int nv, int nrhs,
+                     double2* partial, int nparts, double2* out, cudaStream_t s) {
+    dim3 grid(nparts, nrhs);
+    k_multidot<<<grid, 256, 0, s>>>(w, V, len, vstride, nv, nrhs, partial);
+    k_multidot_sum<<<nrhs * (nv + 1), 256, 0, s>>>(partial, nparts, out);
+}
+void launch_axpy_multidot(double2* w, const double2* V, long long len, long long vstride, int nv, const double2* h,
+                          int hstride, int nd, const int* act, int nrhs, double2* partial, int nparts, double2* out,
+                          cudaStream_t s) {
+    dim3 grid(nparts, nrhs);
+    k_axpy_multidot<<<grid, 256, 0, s>>>(w, V, len, vstride, nv, h, hstride, nd, act, partial);
+    k_multidot_sum<<<nrhs * (nd + 1), 256, 0, s>>>(partial, nparts, out);
+}
+void launch_multiaxpy(double2* w, const double2* V, long long len, long long vstride, int nv, const double2* h,
+                      int hstride, const int* act, int nrhs, cudaStream_t s) {
+    dim3 grid(592, nrhs);
+    k_multiaxpy<<<grid, 256, 0, s>>>(w, V, len, vstride, nv, h, hstride, act);
+}
+void launch_multiaxpy_add(double2* x, const double2* Z, long long len, long long vstride, int nv, const double2* c,
+                          int cstride, const int* nvr, const int* act, int nrhs, cudaStream_t s) {
+    dim3 grid(592, nrhs);
+    k_multiaxpy_add<<<grid, 256, 0, s>>>(x, Z, len, vstride, nv, c, cstride, nvr, act);
+}
+void launch_scale(double2* y, const double2* x, long long len, const double* sc, const int* act, int nrhs,
+                  cudaStream_t s) {
+    dim3 grid(592, nrhs);
+    k_scale<<<grid, 256, 0, s>>>(y, x, len, sc, act);
+}
+void launch_d2f(float2* y, const double2* x, long long n, cudaStream_t s) { k_d2f<<<592, 256, 0, s>>>(y, x, n); }
+void launch_f2d(double2* y, const float2* x, long long n, cudaStream_t s) { k_f2d<<<592, 256, 0, s>>>(y, x, n); }
+void launch_d2bf(__nv_bfloat162* y, const double2* x, long long n, cudaStream_t s) { k_d2bf<<<592, 256, 0, s>>>(y, x, n); }
+
+#define INST(T)                                                                                                 \
+    template void launch_dirac<T>(const cx<T>*, const cx<T>*, cx<T>*, int, int, int, T, int, cudaStream_t);     \
+    template void launch_residual<T>(const cx<T>*, const cx<T>*, long long, const cx<T>*, cx<T>*, int, int, int, T,\
+                                     double*, double*, const int*, cudaStream_t);                                \
+    template void launch_norm2<T>(const cx<T>*, long long, long long, int, double*, double*, cudaStream_t);      \
+    template int sap0_smem_bytes<T>(int, int, int);                                                              \
+    template cudaError_t launch_sap0<T>(const cx<T>*, const cx<T>*, cx<T>*, const int*, int, int, int, int, int, \
+                                        int, int, T, int, int, T, int, cx<T>*, int*, const int*, cudaStream_t);
+INST(double)
+INST(float)
+template void launch_restrict0<double, double2>(const double2*, const cx<double>*, cx<double>*, cx<double>*, int,
+                                                 int, int, int, int, int, int, cudaStream_t);
+template void launch_restrict0<float, float2>(const float2*, const cx<float>*, cx<float>*, cx<float>*, int, int,
+                                               int, int, int, int, int, cudaStream_t);
+template void launch_restrict0<float, __nv_bfloat162>(const __nv_bfloat162*, const cx<float>*, cx<float>*,
+                                                       cx<float>*, int, int, int, int, int, int, int, cudaStream_t);
+template void launch_prolong0_add<double, double2>(const double2*, const cx<double>*, cx<double>*, int, int, int,
+                                                    int, int, int, cudaStream_t);
+template void launch_prolong0_add<float, float2>(const float2*, const cx<float>*, cx<float>*, int, int, int, int,
+                                                  int, int, cudaStream_t);
+template void launch_prolong0_add<float, __nv_bfloat162>(const __nv_bfloat162*, const cx<float>*, cx<float>*, int,
+                                                          int, int, int, int, int, cudaStream_t);
+
+}  // namespace amgb

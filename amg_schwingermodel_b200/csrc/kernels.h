@@ -1,0 +1,73 @@
+// Launchers of the CUDA kernels (host side).  All take a stream; none synchronises.
+#pragma once
+#include "common.cuh"
+#include "engine.cuh"
+
+namespace amgb {
+
+void set_last_error(const char* msg, const char* file, int line);
+
+// ---- fine lattice (fine.cu) ----
+template <typename T>
+void launch_dirac(const cx<T>* U, const cx<T>* in, cx<T>* out, int nx, int nt, int nrhs, T m0, int dagger,
+                  cudaStream_t s);
+template <typename T>
+void launch_residual(const cx<T>* U, const cx<T>* b, long long bstride, const cx<T>* x, cx<T>* r, int nx, int nt,
+                     int nrhs, T m0, double* partial, double* norm2_out, const int* act, cudaStream_t s);
+template <typename T>
+void launch_norm2(const cx<T>* v, long long len, long long stride, int nrhs, double* partial, double* out,
+                  cudaStream_t s);
+int residual_partials(int nx, int nt);
+template <typename T, typename TW>
+void launch_restrict0(const TW* W, const cx<T>* v, cx<T>* out, cx<T>* partial, int nx, int nt, int bx, int bt,
+                      int ntest, int nrhs, int nchunk, cudaStream_t s);
+template <typename T, typename TW>
+void launch_prolong0_add(const TW* W, const cx<T>* vc, cx<T>* psi, int nx, int nt, int bx, int bt, int ntest,
+                         int nrhs, cudaStream_t s);
+template <typename T>
+int sap0_smem_bytes(int S, int m, int use_smem);
+template <typename T>
+cudaError_t launch_sap0(const cx<T>* U, const cx<T>* r, cx<T>* x, const int* blocks, int ncol, int nrhs, int nx,
+                        int nt, int sbt, int sxe, int ste, T m0, int m, int restarts, T tol, int use_smem,
+                        cx<T>* gscratch, int* iters, const int* act, cudaStream_t s);
+void launch_multidot(const double2* w, const double2* V, long long len, long long vstride, int nv, int nrhs,
+                     double2* partial, int nparts, double2* out, cudaStream_t s);
+void launch_axpy_multidot(double2* w, const double2* V, long long len, long long vstride, int nv, const double2* h,
+                          int hstride, int nd, const int* act, int nrhs, double2* partial, int nparts, double2* out,
+                          cudaStream_t s);
+void launch_multiaxpy(double2* w, const double2* V, long long len, long long vstride, int nv, const double2* h,
+                      int hstride, const int* act, int nrhs, cudaStream_t s);
+void launch_multiaxpy_add(double2* x, const double2* Z, long long len, long long vstride, int nv, const double2* c,
+                          int cstride, const int* nvr, const int* act, int nrhs, cudaStream_t s);
+void launch_scale(double2* y, const double2* x, long long len, const double* sc, const int* act, int nrhs,
+                  cudaStream_t s);
+void launch_d2f(float2* y, const double2* x, long long n, cudaStream_t s);
+void launch_f2d(double2* y, const float2* x, long long n, cudaStream_t s);
+void launch_d2bf(__nv_bfloat162* y, const double2* x, long long n, cudaStream_t s);
+
+// ---- coarse engine (coarse.cu) ----
+enum EngOp {
+    ENG_KFGMRES = 0,   // FGMRES_k_cycle of level l: x = fgmres(b, x0 = b)
+    ENG_KCYCLE = 1,    // k_cycle(l, b, x) accumulating into x
+    ENG_VCYCLE = 2,    // v_cycle(l, b, x) accumulating into x
+    ENG_SAP = 3,       // SAP(l, b, x, nu) with x in/out
+    ENG_APPLY = 4,     // x = D_l b
+    ENG_GMRES = 5,     // coarsest-style GMRES on level l: x = gmres(b, x0 = b)
+    ENG_RESTRICT = 6,  // x (level l+1) = P_l^dagger b
+    ENG_PROLONG = 7,   // x (level l) = P_l b (level l+1)
+};
+template <typename T>
+cudaError_t launch_engine_dev(const EngArgs<T>* dev_args, int op, int level, int nu, const cx<T>* in,
+                              long long in_stride, cx<T>* out, long long out_stride, int nsrc, int smem_bytes,
+                              cudaStream_t s);
+
+// ---- set-up (setup.cu) ----
+template <typename T>
+void launch_fine_hops(const cx<T>* U, cx<T>* hops, int nx, int nt, cudaStream_t s);
+template <typename T>
+void launch_coarse_links(const cx<T>* W, const cx<T>* hops, cx<T>* out, int nx, int nt, int K, int bx, int bt,
+                         int ntest, cx<T>* partial, int nchunk, cudaStream_t s);
+template <typename T>
+void launch_orthonormalize(cx<T>* W, int nx, int nt, int K, int bx, int bt, int ntest, cudaStream_t s);
+
+}  // namespace amgb

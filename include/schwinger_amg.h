@@ -1,0 +1,182 @@
+/*
+ * schwinger_amg.h -- C ABI of the B200 DD-alpha-AMG solver for the 2-D Schwinger-model
+ * Wilson-Dirac operator (libschwinger_amg.so).
+ *
+ * Every entry point returns an int status: AMG_OK (0), AMG_NOT_CONVERGED (1) when an
+ * iteration limit was reached, or a negative AMG_ERR_* code; amg_last_error() gives the
+ * message.  No entry point exits the process or traps on the device (the reference calls
+ * exit(1) on bad input, include/params.h:21-24, src/gauge_conf.cpp:20-23).
+ *
+ * Layouts at this boundary are the reference's, as contiguous interleaved complex128
+ * arrays:
+ *   fine spinor / source      psi[N][2]           n = x*Nt + t (src/variables.cpp:10-16)
+ *   gauge field               U[N][2]             U[n][mu], mu = 0 time, mu = 1 space
+ *   level-l vector            v[N_l][DOF_l]       dof = 2*c + spin (src/level.cpp:166)
+ *   test vectors of level l   W[Ntest_l][N_l][DOF_l]   (interpolator_columns, include/level.h:144)
+ *   coarse links of level l   G1[N_l][2][2][c][c], G2/G3[N_l][2][2][c][c][2]
+ *                             (include/level.h:126-128, 162-164, 169-185)
+ * Arrays with a trailing "nrhs" dimension are [nrhs][...] (one full vector per source).
+ * Pointers are host pointers unless the function name ends in _dev (device pointers).
+ */
+#ifndef SCHWINGER_AMG_H
+#define SCHWINGER_AMG_H
+
+#if defined(__GNUC__)
+#define AMG_API __attribute__((visibility("default")))
+#else
+#define AMG_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AMG_OK 0
+#define AMG_NOT_CONVERGED 1
+#define AMG_ERR_INVALID (-1)     /* bad argument or parameter */
+#define AMG_ERR_CUDA (-2)        /* CUDA runtime error */
+#define AMG_ERR_STATE (-3)       /* call order (e.g. solve before set-up) */
+#define AMG_ERR_NOMEM (-4)       /* device allocation failed */
+#define AMG_ERR_DEVICE_WAIT (-5) /* a bounded device-side wait gave up */
+#define AMG_ERR_UNSUPPORTED (-6) /* configuration outside what the kernels support */
+
+#define AMG_PREC_F64 0           /* everything FP64: the plain drop-in */
+#define AMG_PREC_MIXED 1         /* FP32 cycle (SAP, P, P^dagger, coarse levels) with BF16
+                                    test vectors inside the FP64 outer FGMRES */
+
+#define AMG_CYCLE_V 0            /* AMGV::cycle = 0 (include/variables.h:64) */
+#define AMG_CYCLE_K 1
+
+typedef struct amg_context* amg_ctx;
+
+/* Solver knobs.  Defaults (amg_params_default) are the reference's:
+ * src/variables.cpp:46-87 and include/params.h:63-65, with the values its main sets
+ * (K-cycle, Nit = 0, 4 SAP iterations on the test vectors; src/main.cpp:61-65, :129). */
+typedef struct amg_params {
+    int cycle;                 /* AMGV::cycle */
+    int nu1, nu2;              /* AMGV::nu1 / nu2: pre/post SAP iterations */
+    int nit;                   /* AMGV::Nit: bootstrap passes of the set-up */
+    int sap_tv_iters;          /* AMGV::SAP_test_vectors_iterations */
+    int sap_gmres_m;           /* SAPV::sap_gmres_restart_length */
+    int sap_gmres_restarts;    /* SAPV::sap_gmres_restarts */
+    double sap_gmres_tol;      /* SAPV::sap_gmres_tolerance */
+    double sap_tol;            /* SAPV::sap_tolerance */
+    int kcycle_m;              /* AMGV::fgmres_k_cycle_restart_length */
+    int kcycle_restarts;       /* AMGV::fgmres_k_cycle_restarts */
+    double kcycle_tol;         /* AMGV::fgmres_k_cycle_tol */
+    int coarse_m;              /* LevelV::GMRES_restart_len[maxLevel] */
+    int coarse_restarts;       /* LevelV::GMRES_restarts[maxLevel] */
+    double coarse_tol;         /* LevelV::GMRES_tol[maxLevel] */
+    int outer_m;               /* FGMRESV::fgmres_restart_length */
+    int outer_restarts;        /* FGMRESV::fgmres_restarts */
+    double outer_tol;          /* FGMRESV::fgmres_tolerance */
+    int precision;             /* AMG_PREC_F64 or AMG_PREC_MIXED */
+    int max_rhs;               /* largest number of sources per solve call (buffers) */
+    unsigned long long tv_seed;/* 0: the reference's draw (mt19937(50), src/amg.cpp:8-16) */
+} amg_params;
+
+/* Per-source result of a solve. */
+typedef struct amg_solve_info {
+    int iterations;            /* FGMRES::fgmres return value (src/fgmres.cpp:80, :87) */
+    int converged;             /* 1 if the FP64 true residual met the tolerance */
+    double rel_residual;       /* ||b - D x|| / ||b|| in FP64 */
+} amg_solve_info;
+
+/* ---- errors, version ------------------------------------------------------------- */
+AMG_API const char* amg_status_string(int status);
+AMG_API const char* amg_last_error(void);
+AMG_API int amg_version(void);
+
+/* ---- parameters ------------------------------------------------------------------ */
+AMG_API void amg_params_default(amg_params* p);
+
+/* readParameters (include/params.h:17-69): reads "level bx bt ntest sbx sbt" rows from a
+ * parameters.dat file into rows[max_rows][6]; *nrows receives the row count. */
+AMG_API int amg_read_parameters(const char* path, int* rows, int max_rows, int* nrows);
+
+/* ---- context ---------------------------------------------------------------------- */
+/* Replaces AlgebraicMG(GConf, m0, nu1, nu2) (include/amg.h:42-64) plus the lattice size
+ * and level count the reference fixes at compile time (include/config.h.in:3-5):
+ * nx = NS, nt = NT, levels = LEVELS, rows = the parameters.dat rows [levels-1][6]. */
+AMG_API int amg_create(amg_ctx* ctx, int nx, int nt, int levels, const int* rows, double m0,
+               const amg_params* params, int device);
+AMG_API int amg_destroy(amg_ctx ctx);
+AMG_API int amg_get_params(amg_ctx ctx, amg_params* out);
+/* mass::m0 (include/variables.h:20-22) */
+AMG_API int amg_set_mass(amg_ctx ctx, double m0);
+/* Level sizes as LevelV fills them: out[l] = {Nsites, NxSites, NtSites, DOF, Colors, Ntest}. */
+AMG_API int amg_level_info(amg_ctx ctx, int level, int* out6);
+
+/* GaugeConf::setGconf / read_conf (include/gauge_conf.h:34, src/gauge_conf.cpp:18-32):
+ * U[N][2] complex128.  Invalidates the set-up. */
+AMG_API int amg_set_gauge(amg_ctx ctx, const double* U);
+
+/* ---- fine operator ------------------------------------------------------------------ */
+/* D_phi / D_dagger_phi (src/dirac_operator.cpp:3-54; include/dirac_operator.h:14-24):
+ * out = D in (dagger = 0) or D^dagger in (dagger = 1), for nrhs sources. */
+AMG_API int amg_dirac_apply(amg_ctx ctx, const double* in, double* out, int nrhs, int dagger);
+AMG_API int amg_dirac_apply_dev(amg_ctx ctx, const void* in, void* out, int nrhs, int dagger);
+/* Stand-alone FP64 stencil on caller-owned device memory (no context): U_dev [N][2],
+ * in_dev / out_dev [nrhs][N][2] complex128, launched on `stream` (a cudaStream_t). */
+AMG_API int amg_dirac_apply_raw(const void* U_dev, const void* in_dev, void* out_dev, int nx, int nt,
+                        int nrhs, double m0, int dagger, void* stream);
+
+/* ---- set-up ------------------------------------------------------------------------ */
+/* Optional: the test vectors the set-up starts from on level l, W[Ntest_l][N_l][DOF_l]
+ * (the columns setUpPhase draws, src/amg.cpp:8-35).  Without it the set-up draws them. */
+AMG_API int amg_set_initial_test_vectors(amg_ctx ctx, int level, const double* W);
+/* AlgebraicMG::setUpPhase(Nit) (src/amg.cpp:3-88): smooth, orthonormalise, build the
+ * coarse links of every level, then params.nit bootstrap passes. */
+AMG_API int amg_setup(amg_ctx ctx);
+/* Level::interpolator_columns after set-up (include/level.h:144). */
+AMG_API int amg_get_test_vectors(amg_ctx ctx, int level, double* W);
+/* Level::G1/G2/G3 of level l >= 1 (built by makeCoarseLinks, src/level.cpp:242-301). */
+AMG_API int amg_get_coarse_links(amg_ctx ctx, int level, double* G1, double* G2, double* G3);
+
+/* ---- level operators (one source) -------------------------------------------------- */
+/* Level::D_operator (src/level.cpp:161-180) of level l. */
+AMG_API int amg_level_apply(amg_ctx ctx, int level, const double* in, double* out);
+/* Level::Pt_v (src/level.cpp:212-237): level l -> l+1. */
+AMG_API int amg_restrict(amg_ctx ctx, int level, const double* in, double* out);
+/* Level::P_v (src/level.cpp:182-209): level l+1 -> l. */
+AMG_API int amg_prolong(amg_ctx ctx, int level, const double* in, double* out);
+/* SAP_C::SAP (src/sap.cpp:64-174) on level l: nu iterations on D x = v, x in/out.
+ * Returns AMG_OK if the SAP tolerance was met, AMG_NOT_CONVERGED otherwise (the
+ * reference returns 1 / 0). */
+AMG_API int amg_sap(amg_ctx ctx, int level, const double* v, double* x, int nu);
+/* Level::GMRES_level_l::fgmres(b, b, x) on level l >= 1 with the coarsest-level knobs
+ * (include/level.h:66-85); *iterations receives the FGMRES count. */
+AMG_API int amg_level_gmres(amg_ctx ctx, int level, const double* b, double* x, int* iterations);
+/* One cycle from level l: AlgebraicMG::k_cycle / v_cycle(l, eta, psi) (src/amg.cpp:90-178),
+ * psi in/out (the caller zeroes it for a fresh cycle). */
+AMG_API int amg_cycle(amg_ctx ctx, int level, const double* eta, double* psi);
+/* FGMRES_k_cycle of level l >= 1 (include/amg.h:19-40): fgmres(b, x0 = b, x). */
+AMG_API int amg_kcycle_fgmres(amg_ctx ctx, int level, const double* b, double* x, int* iterations);
+
+/* ---- solve --------------------------------------------------------------------------- */
+/* FGMRES_AMG::fgmres(b, x0 = 0, x) (include/amg.h:99-145, src/fgmres.cpp:5-88) for nrhs
+ * sources at once: b, x [nrhs][N][2] host arrays; info[nrhs] optional. */
+AMG_API int amg_solve(amg_ctx ctx, const double* b, double* x, int nrhs, amg_solve_info* info);
+/* Same on device arrays (no host copies). */
+AMG_API int amg_solve_dev(amg_ctx ctx, const void* b_dev, void* x_dev, int nrhs, amg_solve_info* info);
+/* Residual history of source 0 of the last solve: |g_{j+1}| per Arnoldi step
+ * (the reference's Residuals_FGMRES_*.res, src/fgmres.cpp:45, :70-79). */
+AMG_API int amg_residual_history(amg_ctx ctx, double* out, int max_len, int* len);
+
+/* ---- adjoint (no reference counterpart beyond D_dagger_phi) ------------------------- */
+/* lambda = D^{-dagger} g through the same hierarchy: lambda = gamma5 D^{-1} gamma5 g. */
+AMG_API int amg_solve_adjoint(amg_ctx ctx, const double* g, double* lambda, int nrhs, amg_solve_info* info);
+AMG_API int amg_solve_adjoint_dev(amg_ctx ctx, const void* g_dev, void* lambda_dev, int nrhs, amg_solve_info* info);
+/* Fermion force: F[n][mu] = Re(lambda^dagger dD/dtheta_mu(n) x) for U = exp(i theta),
+ * summed over the nrhs pairs; F[N][2] float64. */
+AMG_API int amg_force(amg_ctx ctx, const double* lambda, const double* x, int nrhs, double* F);
+AMG_API int amg_force_dev(amg_ctx ctx, const void* lambda_dev, const void* x_dev, int nrhs, void* F_dev);
+
+/* ---- timing -------------------------------------------------------------------------- */
+/* Device milliseconds of the last amg_setup / solve call (CUDA events). */
+AMG_API int amg_last_timings(amg_ctx ctx, double* setup_ms, double* solve_ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
