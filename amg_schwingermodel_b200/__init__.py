@@ -31,6 +31,11 @@ def _c128(a, shape=None) -> np.ndarray:
     return a
 
 
+def launch_count() -> int:
+    """Kernels launched by the library so far (all contexts)."""
+    return int(lib().amg_launch_count())
+
+
 def read_parameters(path: str) -> list:
     """readParameters (include/params.h:17-69): the rows of a parameters.dat file."""
     rows = np.zeros((64, 6), dtype=np.int32)
@@ -207,12 +212,34 @@ class AMGContext:
         return [dict(iterations=i.iterations, converged=bool(i.converged), rel_residual=i.rel_residual)
                 for i in infos]
 
+    def solve_host_ptr(self, b_ptr: int, x_ptr: int, nrhs: int):
+        """amg_solve on raw host pointers (e.g. pinned buffers): copies in, solves, copies out."""
+        infos = (AmgSolveInfo * nrhs)()
+        check(lib().amg_solve(self._h, C.c_void_p(b_ptr), C.c_void_p(x_ptr), nrhs, infos), "amg_solve")
+        return [dict(iterations=i.iterations, converged=bool(i.converged), rel_residual=i.rel_residual)
+                for i in infos]
+
     def residual_history(self) -> np.ndarray:
         n = C.c_int(0)
         check(lib().amg_residual_history(self._h, None, 0, C.byref(n)), "amg_residual_history")
         out = np.zeros(max(n.value, 1), dtype=np.float64)
         check(lib().amg_residual_history(self._h, _cptr(out), n.value, C.byref(n)), "amg_residual_history")
         return out[: n.value]
+
+    def stream(self) -> int:
+        """The cudaStream_t (as an integer) all calls on this context run on."""
+        return lib().amg_get_stream(self._h) or 0
+
+    def profile(self, enable: bool = True) -> None:
+        check(lib().amg_profile(self._h, int(enable)), "amg_profile")
+
+    def profile_report(self) -> dict:
+        out = {}
+        for name, slot in _lib.PROF_SLOTS.items():
+            ms, n, b = C.c_double(0), C.c_longlong(0), C.c_double(0)
+            check(lib().amg_profile_query(self._h, slot, C.byref(ms), C.byref(n), C.byref(b)), "amg_profile_query")
+            out[name] = dict(ms=ms.value, launches=n.value, bytes=b.value)
+        return out
 
     def timings(self):
         s, v = C.c_double(0), C.c_double(0)

@@ -86,7 +86,13 @@ SIGNATURES = {
     "amg_force": (_I, [_P, _P, _P, _I, _P]),
     "amg_force_dev": (_I, [_P, _P, _P, _I, _P]),
     "amg_last_timings": (_I, [_P, C.POINTER(_D), C.POINTER(_D)]),
+    "amg_profile": (_I, [_P, _I]),
+    "amg_profile_query": (_I, [_P, _I, C.POINTER(_D), C.POINTER(C.c_longlong), C.POINTER(_D)]),
+    "amg_launch_count": (C.c_longlong, []),
+    "amg_get_stream": (_P, [_P]),
 }
+
+PROF_SLOTS = {"sap": 0, "engine": 1, "restrict": 2, "prolong": 3, "fine_op": 4, "blas": 5}
 
 
 def lib() -> C.CDLL:

@@ -16,6 +16,7 @@
 
 namespace amgb {
 
+long long g_launches = 0;
 static thread_local std::string g_last_error;
 void set_last_error(const char* msg, const char* file, int line) {
     g_last_error = std::string(msg) + " (" + file + ":" + std::to_string(line) + ")";
@@ -178,11 +179,59 @@ struct amg_context {
     std::vector<double> history;
     double last_setup_ms = 0, last_solve_ms = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // per-kernel-class timing with CUDA events on the context's stream (amg_profile)
+    struct ProfSlot { double ms = 0; long long n = 0; double bytes = 0; };
+    int prof_on = 0;
+    ProfSlot prof[AMG_PROF_SLOTS];
+    struct Pending { int slot; cudaEvent_t a, b; double bytes; };
+    std::vector<Pending> prof_pending;
+    std::vector<cudaEvent_t> ev_pool;
+    ~amg_context() {
+        for (auto& p : prof_pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
+        for (auto e : ev_pool) cudaEventDestroy(e);
+    }
 };
 
 namespace {
 
 using cd = std::complex<double>;
+
+cudaEvent_t prof_event(amg_context* c) {
+    if (!c->ev_pool.empty()) { cudaEvent_t e = c->ev_pool.back(); c->ev_pool.pop_back(); return e; }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+// Records an event pair around the launches of one kernel class when profiling is on.
+struct ProfScope {
+    amg_context* c;
+    int slot;
+    double bytes;
+    cudaEvent_t a = nullptr;
+    ProfScope(amg_context* c_, int slot_, double bytes_) : c(c_), slot(slot_), bytes(bytes_) {
+        if (c->prof_on) { a = prof_event(c); cudaEventRecord(a, c->stream); }
+    }
+    ~ProfScope() {
+        if (!a) return;
+        cudaEvent_t b = prof_event(c);
+        cudaEventRecord(b, c->stream);
+        c->prof_pending.push_back({slot, a, b, bytes});
+    }
+};
+void prof_harvest(amg_context* c) {
+    if (c->prof_pending.empty()) return;
+    cudaStreamSynchronize(c->stream);
+    for (auto& p : c->prof_pending) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, p.a, p.b);
+        c->prof[p.slot].ms += ms;
+        c->prof[p.slot].n += 1;
+        c->prof[p.slot].bytes += p.bytes;
+        c->ev_pool.push_back(p.a);
+        c->ev_pool.push_back(p.b);
+    }
+    c->prof_pending.clear();
+}
 
 long long vlen0(const amg_context* c) { return 2LL * c->N; }
 
@@ -294,6 +343,7 @@ template <typename T>
 int run_engine(amg_context* c, PrecSet<T>& ps, int op, int level, int nu, const cx<T>* in, long long in_stride,
                cx<T>* out, long long out_stride, int nsrc) {
     if (nsrc > ps.eng_cap) return fail(AMG_ERR_INVALID, "engine capacity %d < %d sources", ps.eng_cap, nsrc);
+    ProfScope ps_(c, AMG_PROF_ENGINE, 0.0);
     CK(launch_engine_dev<T>(ps.eng_args.template as<EngArgs<T>>(), op, level, nu, in, in_stride, out, out_stride,
                             nsrc, ps.eng_smem, c->stream));
     return AMG_OK;
@@ -327,6 +377,9 @@ int restrict_chunks(amg_context* c, int R) {
 template <typename T>
 void fine_restrict(amg_context* c, PrecSet<T>& ps, const cx<T>* v, cx<T>* out, int R) {
     const LevelHost& h0 = c->lv[0];
+    ProfScope ps_(c, AMG_PROF_RESTRICT,
+                  (double)h0.ntest * c->N * 2 * (ps.w0_bf16 ? 4.0 : (double)sizeof(cx<T>)) +
+                      (double)R * c->N * 2 * sizeof(cx<T>));
     const int nchunk = restrict_chunks<T>(c, R);
     if (ps.w0_bf16)
         launch_restrict0<float, __nv_bfloat162>(ps.W0.template as<__nv_bfloat162>(), (const cx<float>*)v,
@@ -340,6 +393,9 @@ void fine_restrict(amg_context* c, PrecSet<T>& ps, const cx<T>* v, cx<T>* out, i
 template <typename T>
 void fine_prolong_add(amg_context* c, PrecSet<T>& ps, const cx<T>* vc, cx<T>* psi, int R) {
     const LevelHost& h0 = c->lv[0];
+    ProfScope ps_(c, AMG_PROF_PROLONG,
+                  (double)h0.ntest * c->N * 2 * (ps.w0_bf16 ? 4.0 : (double)sizeof(cx<T>)) +
+                      (double)R * c->N * 2 * 2 * sizeof(cx<T>));
     if (ps.w0_bf16)
         launch_prolong0_add<float, __nv_bfloat162>(ps.W0.template as<__nv_bfloat162>(), (const cx<float>*)vc,
                                                     (cx<float>*)psi, c->nx, c->nt, h0.bx, h0.bt, h0.ntest, R,
@@ -372,6 +428,7 @@ int fine_sap(amg_context* c, PrecSet<T>& ps, const cx<T>* v, long long vstride, 
     const T m0 = (T)c->m0;
     k_set_int<<<1, 256, 0, c->stream>>>(act, 1, R);
     k_set_int<<<1, 256, 0, c->stream>>>(conv, 0, R);
+    count_launch(2);
     launch_norm2<T>(v, len, vstride, R, partial, vnorm2, c->stream);
     launch_residual<T>(U, v, vstride, x, r, c->nx, c->nt, R, m0, nullptr, nullptr, nullptr, c->stream);
     const int S = h.sxe * h.ste;
@@ -382,14 +439,23 @@ int fine_sap(amg_context* c, PrecSet<T>& ps, const cx<T>* v, long long vstride, 
     const int* d_black = d_red + h.ncol;
     for (int it = 0; it < nu; it++) {
         for (int colour = 0; colour < 2; colour++) {
-            CK(launch_sap0<T>(U, r, x, colour == 0 ? d_red : d_black, h.ncol, R, c->nx, c->nt, h.sbt, h.sxe, h.ste,
-                              m0, p.sap_gmres_m, p.sap_gmres_restarts, (T)p.sap_gmres_tol, use_smem, scratch,
-                              nullptr, act, c->stream));
+            {
+                ProfScope ps_(c, AMG_PROF_SAP, (double)h.ncol * S * (2.0 + 6.0 * R) * sizeof(cx<T>));
+                CK(launch_sap0<T>(U, r, x, colour == 0 ? d_red : d_black, h.ncol, R, c->nx, c->nt, h.sbt, h.sxe,
+                                  h.ste, m0, p.sap_gmres_m, p.sap_gmres_restarts, (T)p.sap_gmres_tol, use_smem,
+                                  scratch, nullptr, act, c->stream));
+            }
             const bool last = (colour == 1) && (it == nu - 1);
             if (last && !need_ret) break;
-            launch_residual<T>(U, v, vstride, x, r, c->nx, c->nt, R, m0, partial, colour == 1 ? norm2 : nullptr,
-                               act, c->stream);
-            if (colour == 1) k_sap_check<<<1, 256, 0, c->stream>>>(norm2, vnorm2, p.sap_tol, act, conv, R);
+            {
+                ProfScope ps_(c, AMG_PROF_FINE_OP, (double)c->N * (2.0 + 6.0 * R) * sizeof(cx<T>));
+                launch_residual<T>(U, v, vstride, x, r, c->nx, c->nt, R, m0, partial,
+                                   colour == 1 ? norm2 : nullptr, act, c->stream);
+            }
+            if (colour == 1) {
+                k_sap_check<<<1, 256, 0, c->stream>>>(norm2, vnorm2, p.sap_tol, act, conv, R);
+                count_launch(1);
+            }
         }
     }
     CKL();
@@ -522,16 +588,23 @@ int outer_fgmres(amg_context* c, const double2* b, double2* x, int R, amg_solve_
             double2* Vj = V + (long long)j * vstride;
             double2* Zj = Z + (long long)j * vstride;
             CKR(precondition(c, Vj, Zj, R));
-            launch_dirac<double>(U, Zj, w, c->nx, c->nt, R, c->m0, 0, c->stream);
+            {
+                ProfScope ps_(c, AMG_PROF_FINE_OP, (double)c->N * (2.0 + 4.0 * R) * sizeof(double2));
+                launch_dirac<double>(U, Zj, w, c->nx, c->nt, R, c->m0, 0, c->stream);
+            }
             const int nv = j + 1;
             double2* d1 = dots;
             double2* d2 = dots + (size_t)R * (nv + 1);
             double2* d3 = d2 + (size_t)R * (nv + 1);
-            launch_multidot(w, V, len, vstride, nv, R, dpart, np, d1, c->stream);
-            launch_axpy_multidot(w, V, len, vstride, nv, d1, nv + 1, nv, arn_d, R, dpart, np, d2, c->stream);
-            launch_axpy_multidot(w, V, len, vstride, nv, d2, nv + 1, 0, arn_d, R, dpart, np, d3, c->stream);
-            k_inv_norm<<<1, 256, 0, c->stream>>>(d3, 1, 0, scal, arn_d, wm_d, R);
-            launch_scale(V + (long long)(j + 1) * vstride, w, len, scal, wm_d, R, c->stream);
+            {
+                ProfScope ps_(c, AMG_PROF_BLAS, (double)R * len * sizeof(double2) * (3.0 * (nv + 1) + 5.0));
+                launch_multidot(w, V, len, vstride, nv, R, dpart, np, d1, c->stream);
+                launch_axpy_multidot(w, V, len, vstride, nv, d1, nv + 1, nv, arn_d, R, dpart, np, d2, c->stream);
+                launch_axpy_multidot(w, V, len, vstride, nv, d2, nv + 1, 0, arn_d, R, dpart, np, d3, c->stream);
+                k_inv_norm<<<1, 256, 0, c->stream>>>(d3, 1, 0, scal, arn_d, wm_d, R);
+                count_launch(1);
+                launch_scale(V + (long long)(j + 1) * vstride, w, len, scal, wm_d, R, c->stream);
+            }
             std::vector<double2> hd((size_t)R * (2 * (nv + 1) + 1));
             CK(cudaMemcpyAsync(hd.data(), dots, hd.size() * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
             CK(cudaStreamSynchronize(c->stream));
@@ -604,6 +677,7 @@ int outer_fgmres(amg_context* c, const double2* b, double2* x, int R, amg_solve_
         }
     }
     CKL();
+    prof_harvest(c);
     if (info)
         for (int r = 0; r < R; r++) {
             info[r].iterations = iters[r];
@@ -1293,6 +1367,28 @@ int amg_force(amg_ctx c, const double* lambda, const double* x, int nrhs, double
 int amg_force_dev(amg_ctx c, const void* lambda, const void* x, int nrhs, void* F) {
     (void)c; (void)lambda; (void)x; (void)nrhs; (void)F;
     return fail(AMG_ERR_UNSUPPORTED, "force not built yet");
+}
+
+long long amg_launch_count(void) { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
+
+void* amg_get_stream(amg_ctx c) { return c ? (void*)c->stream : nullptr; }
+
+int amg_profile(amg_ctx c, int enable) {
+    if (!c) return fail(AMG_ERR_INVALID, "null context");
+    prof_harvest(c);
+    c->prof_on = enable ? 1 : 0;
+    for (auto& s : c->prof) s = amg_context::ProfSlot{};
+    return AMG_OK;
+}
+
+int amg_profile_query(amg_ctx c, int slot, double* ms, long long* launches, double* bytes) {
+    if (!c) return fail(AMG_ERR_INVALID, "null context");
+    if (slot < 0 || slot >= AMG_PROF_SLOTS) return fail(AMG_ERR_INVALID, "profile slot %d", slot);
+    prof_harvest(c);
+    if (ms) *ms = c->prof[slot].ms;
+    if (launches) *launches = c->prof[slot].n;
+    if (bytes) *bytes = c->prof[slot].bytes;
+    return AMG_OK;
 }
 
 int amg_last_timings(amg_ctx c, double* setup_ms, double* solve_ms) {

@@ -39,6 +39,7 @@ cudaError_t launch_engine_dev(const EngArgs<T>* dev_args, int op, int level, int
     cudaError_t e = cudaFuncSetAttribute(k_engine<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
     if (e != cudaSuccess) return e;
     k_engine<T><<<nsrc, kEngineThreads, smem_bytes, s>>>(dev_args, op, level, nu, in, in_stride, out, out_stride);
+    count_launch(1);
     return cudaGetLastError();
 }
 

@@ -448,6 +448,7 @@ __global__ void k_d2bf(__nv_bfloat162* __restrict__ y, const double2* __restrict
 template <typename T>
 void launch_dirac(const cx<T>* U, const cx<T>* in, cx<T>* out, int nx, int nt, int nrhs, T m0, int dagger,
                   cudaStream_t s) {
+    count_launch(1);
     dim3 grid((nx * nt + 255) / 256, nrhs);
     if (dagger) k_dirac<T, true><<<grid, 256, 0, s>>>(U, in, out, nx, nt, m0);
     else k_dirac<T, false><<<grid, 256, 0, s>>>(U, in, out, nx, nt, m0);
@@ -456,6 +457,7 @@ void launch_dirac(const cx<T>* U, const cx<T>* in, cx<T>* out, int nx, int nt, i
 template <typename T>
 void launch_residual(const cx<T>* U, const cx<T>* b, long long bstride, const cx<T>* x, cx<T>* r, int nx, int nt,
                      int nrhs, T m0, double* partial, double* norm2_out, const int* act, cudaStream_t s) {
+    count_launch(norm2_out ? 2 : 1);
     const int nblk = (nx * nt + 255) / 256;
     dim3 grid(nblk, nrhs);
     k_residual<T><<<grid, 256, 0, s>>>(U, b, bstride, x, r, nx, nt, m0, norm2_out ? partial : nullptr, act);
@@ -477,6 +479,7 @@ __global__ void __launch_bounds__(256) k_norm2(const cx<T>* __restrict__ v, long
 template <typename T>
 void launch_norm2(const cx<T>* v, long long len, long long stride, int nrhs, double* partial, double* out,
                   cudaStream_t s) {
+    count_launch(2);
     const int np = 296;
     dim3 grid(np, nrhs);
     k_norm2<T><<<grid, 256, 0, s>>>(v, len, stride, partial);
@@ -487,6 +490,7 @@ int residual_partials(int nx, int nt) { return (nx * nt + 255) / 256; }
 template <typename T, typename TW>
 void launch_restrict0(const TW* W, const cx<T>* v, cx<T>* out, cx<T>* partial, int nx, int nt, int bx, int bt,
                       int ntest, int nrhs, int nchunk, cudaStream_t s) {
+    count_launch(2);
     const int xe = nx / bx, te = nt / bt, nblk = bx * bt;
     dim3 grid(nchunk, nblk, nrhs);
     const int smem = 4 * ntest * 8 * sizeof(T) * 2;
@@ -500,6 +504,7 @@ void launch_restrict0(const TW* W, const cx<T>* v, cx<T>* out, cx<T>* partial, i
 template <typename T, typename TW>
 void launch_prolong0_add(const TW* W, const cx<T>* vc, cx<T>* psi, int nx, int nt, int bx, int bt, int ntest,
                          int nrhs, cudaStream_t s) {
+    count_launch(1);
     const int xe = nx / bx, te = nt / bt;
     k_prolong0_add<T, TW><<<(nx * nt + 255) / 256, 256, 0, s>>>(W, vc, psi, nx, nt, bt, xe, te, ntest, bx * bt, nrhs);
 }
@@ -515,6 +520,7 @@ template <typename T>
 cudaError_t launch_sap0(const cx<T>* U, const cx<T>* r, cx<T>* x, const int* blocks, int ncol, int nrhs, int nx,
                         int nt, int sbt, int sxe, int ste, T m0, int m, int restarts, T tol, int use_smem,
                         cx<T>* gscratch, int* iters, const int* act, cudaStream_t s) {
+    count_launch(1);
     const int bytes = sap0_smem_bytes<T>(sxe * ste, m, use_smem);
     cudaError_t e = cudaFuncSetAttribute(k_sap0_blocks<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e != cudaSuccess) return e;
@@ -526,6 +532,7 @@ cudaError_t launch_sap0(const cx<T>* U, const cx<T>* r, cx<T>* x, const int* blo
 
 void launch_multidot(const double2* w, const double2* V, long long len, long long vstride, int nv, int nrhs,
                      double2* partial, int nparts, double2* out, cudaStream_t s) {
+    count_launch(2);
     dim3 grid(nparts, nrhs);
     k_multidot<<<grid, 256, 0, s>>>(w, V, len, vstride, nv, nrhs, partial);
     k_multidot_sum<<<nrhs * (nv + 1), 256, 0, s>>>(partial, nparts, out);
@@ -533,28 +540,35 @@ void launch_multidot(const double2* w, const double2* V, long long len, long lon
 void launch_axpy_multidot(double2* w, const double2* V, long long len, long long vstride, int nv, const double2* h,
                           int hstride, int nd, const int* act, int nrhs, double2* partial, int nparts, double2* out,
                           cudaStream_t s) {
+    count_launch(2);
     dim3 grid(nparts, nrhs);
     k_axpy_multidot<<<grid, 256, 0, s>>>(w, V, len, vstride, nv, h, hstride, nd, act, partial);
     k_multidot_sum<<<nrhs * (nd + 1), 256, 0, s>>>(partial, nparts, out);
 }
 void launch_multiaxpy(double2* w, const double2* V, long long len, long long vstride, int nv, const double2* h,
                       int hstride, const int* act, int nrhs, cudaStream_t s) {
+    count_launch(1);
     dim3 grid(592, nrhs);
     k_multiaxpy<<<grid, 256, 0, s>>>(w, V, len, vstride, nv, h, hstride, act);
 }
 void launch_multiaxpy_add(double2* x, const double2* Z, long long len, long long vstride, int nv, const double2* c,
                           int cstride, const int* nvr, const int* act, int nrhs, cudaStream_t s) {
+    count_launch(1);
     dim3 grid(592, nrhs);
     k_multiaxpy_add<<<grid, 256, 0, s>>>(x, Z, len, vstride, nv, c, cstride, nvr, act);
 }
 void launch_scale(double2* y, const double2* x, long long len, const double* sc, const int* act, int nrhs,
                   cudaStream_t s) {
+    count_launch(1);
     dim3 grid(592, nrhs);
     k_scale<<<grid, 256, 0, s>>>(y, x, len, sc, act);
 }
-void launch_d2f(float2* y, const double2* x, long long n, cudaStream_t s) { k_d2f<<<592, 256, 0, s>>>(y, x, n); }
-void launch_f2d(double2* y, const float2* x, long long n, cudaStream_t s) { k_f2d<<<592, 256, 0, s>>>(y, x, n); }
-void launch_d2bf(__nv_bfloat162* y, const double2* x, long long n, cudaStream_t s) { k_d2bf<<<592, 256, 0, s>>>(y, x, n); }
+void launch_d2f(float2* y, const double2* x, long long n, cudaStream_t s) {
+    count_launch(1); k_d2f<<<592, 256, 0, s>>>(y, x, n); }
+void launch_f2d(double2* y, const float2* x, long long n, cudaStream_t s) {
+    count_launch(1); k_f2d<<<592, 256, 0, s>>>(y, x, n); }
+void launch_d2bf(__nv_bfloat162* y, const double2* x, long long n, cudaStream_t s) {
+    count_launch(1); k_d2bf<<<592, 256, 0, s>>>(y, x, n); }
 
 #define INST(T)                                                                                                 \
     template void launch_dirac<T>(const cx<T>*, const cx<T>*, cx<T>*, int, int, int, T, int, cudaStream_t);     \

@@ -7,6 +7,10 @@ namespace amgb {
 
 void set_last_error(const char* msg, const char* file, int line);
 
+// number of kernels this library has launched (all contexts); read by amg_launch_count
+extern long long g_launches;
+inline void count_launch(int n = 1) { __atomic_add_fetch(&g_launches, (long long)n, __ATOMIC_RELAXED); }
+
 // ---- fine lattice (fine.cu) ----
 template <typename T>
 void launch_dirac(const cx<T>* U, const cx<T>* in, cx<T>* out, int nx, int nt, int nrhs, T m0, int dagger,

@@ -198,12 +198,14 @@ __global__ void __launch_bounds__(256) k_orthonormalize(cx<T>* __restrict__ W, i
 
 template <typename T>
 void launch_fine_hops(const cx<T>* U, cx<T>* hops, int nx, int nt, cudaStream_t s) {
+    count_launch(1);
     k_fine_hops<T><<<(nx * nt + 255) / 256, 256, 0, s>>>(U, hops, nx, nt);
 }
 
 template <typename T>
 void launch_coarse_links(const cx<T>* W, const cx<T>* hops, cx<T>* out, int nx, int nt, int K, int bx, int bt,
                          int ntest, cx<T>* partial, int nchunk, cudaStream_t s) {
+    count_launch(1);
     constexpr int EPT = 20;
     const int Kc = 2 * ntest, nout = 5 * Kc * Kc;
     const int ysz_bytes = 5 * K * ntest * 2 * (int)sizeof(cx<T>);
@@ -215,13 +217,17 @@ void launch_coarse_links(const cx<T>* W, const cx<T>* hops, cx<T>* out, int nx, 
     const int nblk = bx * bt;
     dim3 grid(nchunk, nblk);
     for (int e0 = 0; e0 < nout; e0 += 256 * EPT)
+    {
         k_coarse_links<T, EPT><<<grid, 256, smem, s>>>(W, hops, partial, nx, nt, K, bx, bt, ntest, nchunk, tile, e0);
+        count_launch(1);
+    }
     const long long tot = (long long)nblk * nout;
     k_sum_chunks<T><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(partial, out, nout, nchunk, nblk);
 }
 
 template <typename T>
 void launch_orthonormalize(cx<T>* W, int nx, int nt, int K, int bx, int bt, int ntest, cudaStream_t s) {
+    count_launch(1);
     k_orthonormalize<T><<<2 * bx * bt, 256, 0, s>>>(W, nx, nt, K, bx, bt, ntest);
 }
 

@@ -172,7 +172,25 @@ AMG_API int amg_solve_adjoint_dev(amg_ctx ctx, const void* g_dev, void* lambda_d
 AMG_API int amg_force(amg_ctx ctx, const double* lambda, const double* x, int nrhs, double* F);
 AMG_API int amg_force_dev(amg_ctx ctx, const void* lambda_dev, const void* x_dev, int nrhs, void* F_dev);
 
-/* ---- timing -------------------------------------------------------------------------- */
+/* ---- timing and profiling ---------------------------------------------------------- */
+/* Kernel classes timed by amg_profile (CUDA events on the context's stream around each
+ * launch): the fine SAP block solves, the coarse-level engine, fine restriction and
+ * prolongation, the fine stencil / residual, and the outer FGMRES orthogonalisation. */
+#define AMG_PROF_SAP 0
+#define AMG_PROF_ENGINE 1
+#define AMG_PROF_RESTRICT 2
+#define AMG_PROF_PROLONG 3
+#define AMG_PROF_FINE_OP 4
+#define AMG_PROF_BLAS 5
+#define AMG_PROF_SLOTS 6
+/* Enables (1) or disables (0) per-class timing and clears the accumulated values. */
+AMG_API int amg_profile(amg_ctx ctx, int enable);
+/* Accumulated device milliseconds, launch count and algorithmic bytes of one class. */
+AMG_API int amg_profile_query(amg_ctx ctx, int slot, double* ms, long long* launches, double* bytes);
+/* Number of CUDA kernels the library has launched so far (all contexts). */
+AMG_API long long amg_launch_count(void);
+/* The cudaStream_t every call on this context runs on (for callers that time or order work). */
+AMG_API void* amg_get_stream(amg_ctx ctx);
 /* Device milliseconds of the last amg_setup / solve call (CUDA events). */
 AMG_API int amg_last_timings(amg_ctx ctx, double* setup_ms, double* solve_ms);
 

@@ -258,6 +258,45 @@ int main(int argc, char** argv) {
 
     if (!(int)jd(job, "solve", 1)) { g_manifest.close(); return 0; }
 
+    // Bounded CPU sample on a given hierarchy: the reference's AlgebraicMG is constructed
+    // without its set-up, the test vectors and coarse links are loaded from
+    // hier_tv_l<l>.bin / hier_g{1,2,3}_l<l>.bin, and one outer iteration (the preconditioner
+    // of FGMRES_AMG::preconditioner, include/amg.h:134-144, plus D_phi) is timed.
+    if ((int)jd(job, "load_hierarchy", 0)) {
+        AlgebraicMG amgh(GConf, m0, AMGV::nu1, AMGV::nu2);
+        for (int l = 0; l < AMGV::levels; l++) {
+            Level& L = *amgh.levels[l];
+            std::string sl = std::to_string(l);
+            if (l < AMGV::levels - 1) {
+                std::ifstream f(g_dir + "/hier_tv_l" + sl + ".bin", std::ios::binary);
+                if (!f) { std::cerr << "missing hierarchy test vectors l" << l << "\n"; return 3; }
+                for (auto& v : L.interpolator_columns)
+                    for (auto& row : v) f.read(reinterpret_cast<char*>(row.data()), (std::streamsize)(row.size() * sizeof(c_double)));
+            }
+            if (l > 0) {
+                for (auto pr : {std::make_pair("g1", &L.G1), std::make_pair("g2", &L.G2), std::make_pair("g3", &L.G3)}) {
+                    std::ifstream f(g_dir + "/hier_" + pr.first + "_l" + sl + ".bin", std::ios::binary);
+                    if (!f) { std::cerr << "missing hierarchy links l" << l << "\n"; return 3; }
+                    f.read(reinterpret_cast<char*>(pr.second->data()), (std::streamsize)(pr.second->size() * sizeof(c_double)));
+                }
+            }
+        }
+        const int reps = std::max(1, (int)jd(job, "outer_iteration_reps", 1));
+        spinor v(N, c_vector(2, 0)), z(N, c_vector(2, 0)), w(N, c_vector(2, 0));
+        double nb = std::sqrt(std::real(dot(rhs, rhs)));
+        for (int n = 0; n < N; n++) for (int a = 0; a < 2; a++) v[n][a] = rhs[n][a] / nb;
+        for (int r = 0; r < reps; r++) {
+            double t1 = now_s();
+            for (auto& row : z) { row[0] = 0; row[1] = 0; }
+            if (AMGV::cycle == 1) amgh.k_cycle(0, v, z); else amgh.v_cycle(0, v, z);
+            D_phi(GConf.Conf, z, w, m0);
+            info << "outer_iteration_seconds_" << r << " " << (now_s() - t1) << "\n";
+        }
+        dump_spinor("sample_z", z);
+        g_manifest.close();
+        return 0;
+    }
+
     spinor x0(N, c_vector(2, 0)), x(N, c_vector(2, 0));
     // FGMRES_AMG keeps its dim1/dim2 arguments by reference (include/amg.h:125-126), so they
     // must outlive the object; src/tests.cpp:72 passes the literal 2, a dangling reference.
@@ -317,6 +356,28 @@ int main(int argc, char** argv) {
                 info << "kfgmres1_iters " << it << "\n";
             }
         }
+    }
+
+    // Bounded CPU sample: one outer FGMRES iteration of the reference -- the preconditioner
+    // application (FGMRES_AMG::preconditioner: zero, then one cycle from level 0) plus the
+    // D_phi of the Arnoldi step -- timed `outer_iteration_reps` times.
+    if ((int)jd(job, "outer_iteration_reps", 0) > 0) {
+        const int reps = (int)jd(job, "outer_iteration_reps", 0);
+        spinor v(N, c_vector(2, 0)), z(N, c_vector(2, 0)), w(N, c_vector(2, 0));
+        double nb = std::sqrt(std::real(dot(rhs, rhs)));
+        for (int n = 0; n < N; n++) for (int a = 0; a < 2; a++) v[n][a] = rhs[n][a] / nb;
+        double t1 = now_s();
+        for (int r = 0; r < reps; r++) {
+            double t2 = now_s();
+            for (auto& row : z) { row[0] = 0; row[1] = 0; }
+            if (AMGV::cycle == 1) amg.k_cycle(0, v, z); else amg.v_cycle(0, v, z);
+            D_phi(GConf.Conf, z, w, m0);
+            info << "outer_iteration_seconds_" << r << " " << (now_s() - t2) << "\n";
+        }
+        info << "outer_iteration_seconds " << (now_s() - t1) / reps << "\n";
+        info << "setup_seconds " << t_setup << "\n";
+        g_manifest.close();
+        return 0;
     }
 
     // The outer solve (src/tests.cpp:67-82): FGMRES_AMG::fgmres(rhs, x0 = 0, x).
