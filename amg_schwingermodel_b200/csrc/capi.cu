@@ -5,6 +5,7 @@
 #include <cmath>
 #include <complex>
 #include <cstdarg>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <random>
@@ -153,6 +154,8 @@ struct PrecSet {
     DevBuf eng_args, eng_work, eng_status, red_black;
     EngArgs<T> eh{};
     int eng_smem = 0, eng_cap = 0;
+    int max_cluster = 1;             // largest engine cluster the slabs are sized for
+    int cluster_cache[17] = {0};     // engine_max_clusters(c) + 1, 0 = not queried
     DevBuf r0, eta1, psi1, rpart, sap_r, sap_scratch;
     int ready = 0;
 };
@@ -264,6 +267,14 @@ __global__ void k_inv_norm(const double2* n2, int stride, int off, double* scale
 
 int ensure_capacity(amg_context* c, int R);
 
+int engine_cluster_limit() {
+    const char* e = getenv("AMG_ENGINE_CLUSTER");
+    int v = e ? atoi(e) : 16;
+    int p = 1;
+    while (p * 2 <= v && p < 16) p *= 2;
+    return p;
+}
+
 // ---------------------------------------------------------------------------------
 // engine arguments for one precision
 // ---------------------------------------------------------------------------------
@@ -322,13 +333,19 @@ int build_engine(amg_context* c, PrecSet<T>& ps, int nsrc) {
                 return fail(AMG_ERR_UNSUPPORTED, "level %d: %d SAP blocks per colour exceed %d", l, h.ncol, kEngineThreads);
         }
     }
+    long long io = 2;
+    for (int l = 1; l < c->L; l++) io = std::max<long long>(io, (long long)c->lv[l].n * c->lv[l].K);
+    a.off_io = off;
+    a.io_len = al(io);
+    off += 2 * a.io_len;
     a.smem_red = sm;
     sm += 2 * (kEngineThreads / 32) * (int)sizeof(T) + 64;
     if (sm > 200 * 1024) return fail(AMG_ERR_UNSUPPORTED, "engine scalar state needs %d bytes of shared memory", sm);
     ps.eng_smem = sm;
     a.slab = std::max<long long>(off, 2);
     ps.eng_cap = std::max(nsrc, 1);
-    CKR(ps.eng_work.alloc((size_t)a.slab * ps.eng_cap * sizeof(cx<T>)));
+    ps.max_cluster = engine_cluster_limit();
+    CKR(ps.eng_work.alloc((size_t)a.slab * ps.eng_cap * ps.max_cluster * sizeof(cx<T>)));
     CKR(ps.eng_status.alloc(sizeof(int) * (ps.eng_cap + 4)));
     a.work = ps.eng_work.template as<cx<T>>();
     a.status = ps.eng_status.template as<int>();
@@ -339,13 +356,26 @@ int build_engine(amg_context* c, PrecSet<T>& ps, int nsrc) {
     return AMG_OK;
 }
 
+// Cluster size for `nsrc` concurrent engine sources: the largest power of two up to the
+// configured limit (AMG_ENGINE_CLUSTER, default 16) whose clusters all fit on the device at
+// once, so one launch serves every source in a single wave.
+template <typename T>
+int pick_cluster(PrecSet<T>& ps, int nsrc) {
+    for (int cs = ps.max_cluster; cs > 1; cs >>= 1) {
+        if (!ps.cluster_cache[cs]) ps.cluster_cache[cs] = engine_max_clusters<T>(cs, ps.eng_smem) + 1;
+        if (ps.cluster_cache[cs] - 1 >= nsrc) return cs;
+    }
+    return 1;
+}
+
 template <typename T>
 int run_engine(amg_context* c, PrecSet<T>& ps, int op, int level, int nu, const cx<T>* in, long long in_stride,
                cx<T>* out, long long out_stride, int nsrc) {
     if (nsrc > ps.eng_cap) return fail(AMG_ERR_INVALID, "engine capacity %d < %d sources", ps.eng_cap, nsrc);
+    const int cs = pick_cluster(ps, nsrc);
     ProfScope ps_(c, AMG_PROF_ENGINE, 0.0);
     CK(launch_engine_dev<T>(ps.eng_args.template as<EngArgs<T>>(), op, level, nu, in, in_stride, out, out_stride,
-                            nsrc, ps.eng_smem, c->stream));
+                            nsrc, ps.eng_smem, cs, c->stream));
     return AMG_OK;
 }
 

@@ -64,6 +64,8 @@ struct EngArgs {
     cx<T>* work;                 // per-source slabs
     long long slab;              // elements per slab
     int smem_red;                // byte offset of the reduction scratch
+    long long off_io;            // slab offset of the entry op's input / output copies
+    long long io_len;            // elements of each copy
     int* status;                 // [nsrc] per-source result code / iteration count
     int* flags;                  // error flag (bit 0: recursion bound, bit 1: unsupported)
 };
@@ -202,6 +204,21 @@ __device__ void v_add(cx<T>* d, const cx<T>* s, int n) {
 }
 
 // ---------------------------------------------------------------------------------
+// engine context per CTA (one source)
+// ---------------------------------------------------------------------------------
+template <typename T>
+struct Eng {
+    const EngArgs<T>* a;
+    cx<T>* slab;
+    char* smem;
+    T* red;
+    int crank, csize;           // rank in the thread-block cluster serving this source, cluster size
+
+    __device__ const EngLevel<T>& L(int l) const { return a->lv[l]; }
+    __device__ cx<T>* work(long long off) const { return slab + off; }
+};
+
+// ---------------------------------------------------------------------------------
 // level geometry helpers
 // ---------------------------------------------------------------------------------
 __device__ __forceinline__ int nb_site(int x, int t, int nx, int nt, int hop) {
@@ -221,13 +238,47 @@ __device__ __forceinline__ int hop_sign(int t, int nt, int hop) {
     return 1;
 }
 
-// Level::D_operator (src/level.cpp:161-180) for l >= 1:
-// out = (m0+2) in - sum_hop sign * G_hop in(neighbour)
+// Hardware barrier over the thread-block cluster with release/acquire ordering of every
+// memory access before it (global stores into other CTAs' slabs included).
+__device__ __forceinline__ void cluster_barrier() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// Rows [e0, e1) of a partitioned operator output computed by this CTA, and the distance
+// (in elements) from this CTA's slab to the slab of cluster rank q.
 template <typename T>
-__device__ __noinline__ void dc_apply(const EngLevel<T>& L, T m0, const cx<T>* in, cx<T>* out) {
+__device__ __forceinline__ void part_range(const Eng<T>& E, int tot, int& e0, int& e1) {
+    const int per = (tot + E.csize - 1) / E.csize;
+    e0 = min(tot, E.crank * per);
+    e1 = min(tot, e0 + per);
+}
+template <typename T>
+__device__ __forceinline__ void part_store(const Eng<T>& E, cx<T>* out, int e, cx<T> v) {
+    if (E.csize == 1) { out[e] = v; return; }
+    const long long slab = E.a->slab;
+    for (int q = 0; q < E.csize; q++) out[(long long)(q - E.crank) * slab + e] = v;
+}
+template <typename T>
+__device__ __forceinline__ void part_begin(const Eng<T>& E) {
+    if (E.csize > 1) cluster_barrier();
+}
+template <typename T>
+__device__ __forceinline__ void part_end(const Eng<T>& E) {
+    if (E.csize > 1) cluster_barrier();
+    else __syncthreads();
+}
+
+// Level::D_operator (src/level.cpp:161-180) for l >= 1:
+// out = (m0+2) in - sum_hop sign * G_hop in(neighbour).  With a cluster, every CTA computes
+// a slice of the rows and stores it into every CTA's copy of `out`.
+template <typename T>
+__device__ __noinline__ void dc_apply(const Eng<T>& E, const EngLevel<T>& L, T m0, const cx<T>* in, cx<T>* out) {
     const int K = L.K, tot = L.n * K;
     const T mass = m0 + T(2);
-    for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+    int e0, e1;
+    part_range(E, tot, e0, e1);
+    part_begin(E);
+    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
         const int xs = e / K, i = e - xs * K;
         const int x = xs / L.nt, t = xs - x * L.nt;
         cx<T> acc = czero<T>();
@@ -242,9 +293,9 @@ __device__ __noinline__ void dc_apply(const EngLevel<T>& L, T m0, const cx<T>* i
             if (hop_sign(t, L.nt, h) < 0) acc -= s; else acc += s;
         }
         cx<T> self = in[e];
-        out[e] = mass * self - acc;
+        part_store(E, out, e, mass * self - acc);
     }
-    __syncthreads();
+    part_end(E);
 }
 
 // SAP block bookkeeping (SAP_C::SchwarzBlocks, src/sap.cpp:3-39): block b covers
@@ -262,11 +313,14 @@ __device__ __forceinline__ int sap_site(const EngLevel<T>& L, int block, int m, 
 // SAP_level_l::D_local (src/level.cpp:304-368) on all blocks of one colour at once:
 // in/out are [ncol][spb][K]; neighbours outside the block are dropped.
 template <typename T>
-__device__ __noinline__ void dlocal_apply(const EngLevel<T>& L, T m0, const int* blocks, int nblk,
+__device__ __noinline__ void dlocal_apply(const Eng<T>& E, const EngLevel<T>& L, T m0, const int* blocks, int nblk,
                                           const cx<T>* in, cx<T>* out) {
     const int K = L.K, spb = L.sxe * L.ste, seglen = spb * K, tot = nblk * seglen;
     const T mass = m0 + T(2);
-    for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+    int e0, e1;
+    part_range(E, tot, e0, e1);
+    part_begin(E);
+    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
         const int seg = e / seglen, r = e - seg * seglen;
         const int m = r / K, i = r - m * K;
         const int block = blocks[seg];
@@ -294,9 +348,9 @@ __device__ __noinline__ void dlocal_apply(const EngLevel<T>& L, T m0, const int*
             for (int j = 0; j < K; j++) cfma(s, a[(long long)j * K], v[j]);
             if (hop_sign(t, L.nt, h) < 0) acc -= s; else acc += s;
         }
-        out[e] = mass * base[r] - acc;
+        part_store(E, out, e, mass * base[r] - acc);
     }
-    __syncthreads();
+    part_end(E);
 }
 
 // gather / scatter between a level vector and the colour's block segments
@@ -325,9 +379,12 @@ __device__ void sap_scatter_add(const EngLevel<T>& L, const int* blocks, int nbl
 
 // Level::Pt_v (src/level.cpp:212-237): out[nc][2cc+s] = sum_{n in nc, c} conj(W_cc[n][2c+s]) v[n][2c+s]
 template <typename T>
-__device__ __noinline__ void restrict_v(const EngLevel<T>& L, const cx<T>* v, cx<T>* out) {
+__device__ __noinline__ void restrict_v(const Eng<T>& E, const EngLevel<T>& L, const cx<T>* v, cx<T>* out) {
     const int K = L.K, col = K / 2, nblk = L.bx * L.bt, tot = nblk * 2 * L.ntest;
-    for (int o = threadIdx.x; o < tot; o += blockDim.x) {
+    int e0, e1;
+    part_range(E, tot, e0, e1);
+    part_begin(E);
+    for (int o = e0 + threadIdx.x; o < e1; o += blockDim.x) {
         const int nc = o / (2 * L.ntest), r = o - nc * 2 * L.ntest, cc = r >> 1, s = r & 1;
         const int bxi = nc / L.bt, bti = nc - bxi * L.bt;
         const cx<T>* w = L.W + (long long)cc * L.n * K;
@@ -337,25 +394,29 @@ __device__ __noinline__ void restrict_v(const EngLevel<T>& L, const cx<T>* v, cx
                 const long long n = (long long)(bxi * L.xe + mx) * L.nt + (bti * L.te + mt);
                 for (int c = 0; c < col; c++) cfmac(acc, w[n * K + 2 * c + s], v[n * K + 2 * c + s]);
             }
-        out[o] = acc;
+        part_store(E, out, o, acc);
     }
-    __syncthreads();
+    part_end(E);
 }
 
 // out (+)= P vc: Level::P_v (src/level.cpp:182-209), out[n][2c+s] = sum_cc W_cc[n][2c+s] vc[nc][2cc+s]
 template <typename T>
-__device__ __noinline__ void prolong_v(const EngLevel<T>& L, const cx<T>* vc, cx<T>* out, int accumulate) {
+__device__ __noinline__ void prolong_v(const Eng<T>& E, const EngLevel<T>& L, const cx<T>* vc, cx<T>* out,
+                                       int accumulate) {
     const int K = L.K, tot = L.n * K;
-    for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+    int e0, e1;
+    part_range(E, tot, e0, e1);
+    part_begin(E);
+    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
         const int n = e / K, d = e - n * K, s = d & 1;
         const int x = n / L.nt, t = n - x * L.nt;
         const int nc = (x / L.xe) * L.bt + (t / L.te);
         const cx<T>* pv = vc + (long long)nc * 2 * L.ntest + s;
         cx<T> acc = czero<T>();
         for (int cc = 0; cc < L.ntest; cc++) cfma(acc, L.W[(long long)cc * L.n * K + e], pv[2 * cc]);
-        out[e] = accumulate ? out[e] + acc : acc;
+        part_store(E, out, e, accumulate ? out[e] + acc : acc);
     }
-    __syncthreads();
+    part_end(E);
 }
 
 // ---------------------------------------------------------------------------------
@@ -518,19 +579,7 @@ __device__ void seg_fgmres(const Seg<T>& sp, Op& op, Pre& pre, const cx<T>* b, c
     }
 }
 
-// ---------------------------------------------------------------------------------
-// engine context per CTA (one source)
-// ---------------------------------------------------------------------------------
-template <typename T>
-struct Eng {
-    const EngArgs<T>* a;
-    cx<T>* slab;
-    char* smem;
-    T* red;
 
-    __device__ const EngLevel<T>& L(int l) const { return a->lv[l]; }
-    __device__ cx<T>* work(long long off) const { return slab + off; }
-};
 
 // SAP_C::SAP (src/sap.cpp:64-174) on coarse level l: nu red/black sweeps of block GMRES,
 // every block of a colour solved; returns 1 if ||v - D x|| < sap_tol * ||v||.
@@ -551,18 +600,17 @@ __device__ __noinline__ int eng_sap(const Eng<T>& E, int l, const cx<T>* v, cx<T
 
     seg_dot(sp1, v, v, st.red);
     const T vnorm = sqrt(st.red[0].x);
-    dc_apply(L, p.m0, x, r);
+    dc_apply(E, L, p.m0, x, r);
     v_sub<T>(r, v, r, nvec);
-    auto op = [&](const cx<T>* in, cx<T>* out) { dlocal_apply(L, p.m0, nullptr, 0, in, out); };
-    for (int it = 0; it < nu; it++) {
+        for (int it = 0; it < nu; it++) {
         for (int colour = 0; colour < 2; colour++) {
             const int* blocks = colour == 0 ? L.red : L.black;
             sap_gather(L, blocks, nseg, r, bseg);
-            auto lop = [&](const cx<T>* in, cx<T>* out) { dlocal_apply(L, p.m0, blocks, nseg, in, out); };
+            auto lop = [&](const cx<T>* in, cx<T>* out) { dlocal_apply(E, L, p.m0, blocks, nseg, in, out); };
             auto ident = [](int, const cx<T>*, cx<T>*, const int*) {};
             seg_fgmres(sps, lop, ident, bseg, xseg, Vseg, Vseg, wseg, st, p.sap_m, p.sap_restarts, p.sap_gmres_tol);
             sap_scatter_add(L, blocks, nseg, xseg, x);
-            dc_apply(L, p.m0, x, r);
+            dc_apply(E, L, p.m0, x, r);
             v_sub<T>(r, v, r, nvec);
         }
         seg_dot(sp1, r, r, st.red);
@@ -570,7 +618,6 @@ __device__ __noinline__ int eng_sap(const Eng<T>& E, int l, const cx<T>* v, cx<T
         __syncthreads();
         if (err < p.sap_tol * vnorm) return 1;
     }
-    (void)op;
     return 0;
 }
 
@@ -585,7 +632,7 @@ __device__ __noinline__ int eng_coarse_gmres(const Eng<T>& E, int l, const cx<T>
     cx<T>* w = V + (long long)(L.gm_m + 1) * nvec;
     GmState<T> st = gm_state_at<T>(E.smem + L.sm_cg, 1, L.gm_m);
     Seg<T> sp = make_seg<T>(1, nvec, E.red);
-    auto op = [&](const cx<T>* in, cx<T>* out) { dc_apply(L, p.m0, in, out); };
+    auto op = [&](const cx<T>* in, cx<T>* out) { dc_apply(E, L, p.m0, in, out); };
     auto ident = [](int, const cx<T>*, cx<T>*, const int*) {};
     seg_fgmres(sp, op, ident, b, x, V, V, w, st, L.gm_m, L.gm_restarts, L.gm_tol);
     return st.iters[0];
@@ -613,11 +660,11 @@ struct Cycles {
         cx<T>* etac = r + nvec;
         cx<T>* psic = etac + ncv;
         if (p.nu1 > 0) eng_sap(E, l, eta, psi, p.nu1);
-        dc_apply(L, p.m0, psi, r);
+        dc_apply(E, L, p.m0, psi, r);
         v_sub<T>(r, eta, r, nvec);
-        restrict_v(L, r, etac);
+        restrict_v(E, L, r, etac);
         Cycles<T, D - 1>::kfgmres(E, l + 1, etac, psic);
-        prolong_v(L, psic, psi, 1);
+        prolong_v(E, L, psic, psi, 1);
         if (p.nu2 > 0) eng_sap(E, l, eta, psi, p.nu2);
     }
     // AlgebraicMG::v_cycle (src/amg.cpp:90-132)
@@ -631,12 +678,12 @@ struct Cycles {
         cx<T>* etac = r + nvec;
         cx<T>* psic = etac + ncv;
         if (p.nu1 > 0) eng_sap(E, l, eta, psi, p.nu1);
-        dc_apply(L, p.m0, psi, r);
+        dc_apply(E, L, p.m0, psi, r);
         v_sub<T>(r, eta, r, nvec);
-        restrict_v(L, r, etac);
+        restrict_v(E, L, r, etac);
         v_zero<T>(psic, ncv);
         Cycles<T, D - 1>::vcycle(E, l + 1, etac, psic);
-        prolong_v(L, psic, psi, 1);
+        prolong_v(E, L, psic, psi, 1);
         if (p.nu2 > 0) eng_sap(E, l, eta, psi, p.nu2);
     }
     // FGMRES_k_cycle of level l (include/amg.h:19-40): fgmres(b, x0 = b, x) with
@@ -650,7 +697,7 @@ struct Cycles {
         cx<T>* w = Z + (long long)p.k_m * nvec;
         GmState<T> st = gm_state_at<T>(E.smem + L.sm_kfg, 1, p.k_m);
         Seg<T> sp = make_seg<T>(1, nvec, E.red);
-        auto op = [&](const cx<T>* in, cx<T>* out) { dc_apply(L, p.m0, in, out); };
+        auto op = [&](const cx<T>* in, cx<T>* out) { dc_apply(E, L, p.m0, in, out); };
         auto pre = [&](int, const cx<T>* v, cx<T>* z, const int*) { Cycles<T, D>::kcycle(E, l, v, z); };
         seg_fgmres(sp, op, pre, b, x, V, Z, w, st, p.k_m, p.k_restarts, p.k_tol);
         return st.iters[0];

@@ -3,7 +3,10 @@
 // BLAS-1 kernels of the outer FGMRES.
 //
 // Layout: psi[rhs][n][spin] complex (double2 or float2), n = x*Nt + t; U[n][mu].
+#include <cstdlib>
+
 #include "kernels.h"
+#include "sap_warp.cuh"
 
 namespace amgb {
 
@@ -487,6 +490,17 @@ void launch_norm2(const cx<T>* v, long long len, long long stride, int nrhs, dou
 }
 int residual_partials(int nx, int nt) { return (nx * nt + 255) / 256; }
 
+// AMG_SAP_KERNEL=cta selects the CTA-per-block SAP kernel for every block shape (A/B tests)
+static int g_sap0_warp = -1;
+int sap0_warp_enabled() {
+    if (g_sap0_warp < 0) {
+        const char* e = getenv("AMG_SAP_KERNEL");
+        g_sap0_warp = (e && e[0] == 'c') ? 0 : 1;
+    }
+    return g_sap0_warp;
+}
+void set_sap0_warp(int on) { g_sap0_warp = on; }
+
 template <typename T, typename TW>
 void launch_restrict0(const TW* W, const cx<T>* v, cx<T>* out, cx<T>* partial, int nx, int nt, int bx, int bt,
                       int ntest, int nrhs, int nchunk, cudaStream_t s) {
@@ -516,11 +530,37 @@ int sap0_smem_bytes(int S, int m, int use_smem) {
     return b;
 }
 
+template <typename T, int SPL, int WPB>
+cudaError_t launch_sap0_warp(const cx<T>* U, const cx<T>* r, cx<T>* x, const int* blocks, int ncol, int nrhs, int nx,
+                             int nt, int sbt, int sxe, int ste, T m0, int restarts, T tol, int* iters, const int* act,
+                             cudaStream_t s) {
+    const int bytes = sap0_warp_smem<T, 5, SPL>(WPB);
+    cudaError_t e = cudaFuncSetAttribute(k_sap0_warp<T, 5, SPL, WPB>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+    dim3 grid((ncol + WPB - 1) / WPB, nrhs);
+    k_sap0_warp<T, 5, SPL, WPB><<<grid, 32 * WPB, bytes, s>>>(U, r, x, blocks, ncol, nx, nt, sbt, sxe, ste, m0, restarts,
+                                                              tol, act, iters);
+    return cudaGetLastError();
+}
+
+// Blocks of 32, 64, 128 or 256 sites with the reference's restart length 5 take the
+// warp-per-block kernel; any other shape takes the CTA-per-block kernel above.
 template <typename T>
 cudaError_t launch_sap0(const cx<T>* U, const cx<T>* r, cx<T>* x, const int* blocks, int ncol, int nrhs, int nx,
                         int nt, int sbt, int sxe, int ste, T m0, int m, int restarts, T tol, int use_smem,
                         cx<T>* gscratch, int* iters, const int* act, cudaStream_t s) {
     count_launch(1);
+    const int S = sxe * ste;
+    if (m == 5 && sap0_warp_enabled()) {
+        constexpr int W = sizeof(T) == 8 ? 2 : 4;
+        switch (S) {
+            case 32: return launch_sap0_warp<T, 1, W>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
+            case 64: return launch_sap0_warp<T, 2, W>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
+            case 128: return launch_sap0_warp<T, 4, W>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
+            case 256: return launch_sap0_warp<T, 8, W>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
+            default: break;
+        }
+    }
     const int bytes = sap0_smem_bytes<T>(sxe * ste, m, use_smem);
     cudaError_t e = cudaFuncSetAttribute(k_sap0_blocks<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e != cudaSuccess) return e;

@@ -30,6 +30,8 @@ void launch_prolong0_add(const TW* W, const cx<T>* vc, cx<T>* psi, int nx, int n
                          int nrhs, cudaStream_t s);
 template <typename T>
 int sap0_smem_bytes(int S, int m, int use_smem);
+int sap0_warp_enabled();
+void set_sap0_warp(int on);
 template <typename T>
 cudaError_t launch_sap0(const cx<T>* U, const cx<T>* r, cx<T>* x, const int* blocks, int ncol, int nrhs, int nx,
                         int nt, int sbt, int sxe, int ste, T m0, int m, int restarts, T tol, int use_smem,
@@ -63,7 +65,9 @@ enum EngOp {
 template <typename T>
 cudaError_t launch_engine_dev(const EngArgs<T>* dev_args, int op, int level, int nu, const cx<T>* in,
                               long long in_stride, cx<T>* out, long long out_stride, int nsrc, int smem_bytes,
-                              cudaStream_t s);
+                              int csize, cudaStream_t s);
+template <typename T>
+int engine_max_clusters(int csize, int smem_bytes);
 
 // ---- set-up (setup.cu) ----
 template <typename T>

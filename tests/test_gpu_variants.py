@@ -1,0 +1,56 @@
+"""The alternative kernel paths give the reference's results too: the CTA-per-block and
+warp-per-block SAP solvers, and the coarse engine on one CTA or on thread-block clusters of
+4 and 16 CTAs.  Each variant runs in its own process (the choice is read from the
+environment once per process)."""
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+from conftest import ROOT
+
+pytestmark = pytest.mark.gpu
+
+SCRIPT = r"""
+import json, sys
+sys.path.insert(0, {root!r}); sys.path.insert(0, {tests!r})
+import numpy as np
+from conftest import load_golden, rel
+from oracle import restatement as R
+from amg_schwingermodel_b200 import AMGContext
+out = {{}}
+for name in ("c32_l3_k", "c64_l4_k", "c64_l2_k"):
+    g = load_golden(name); m = g["meta"]; job = m["job"]
+    ctx = AMGContext(m["ns"], m["nt"], m["rows"], m["m0"], cycle=job["cycle"], nu1=job["nu1"], nu2=job["nu2"],
+                     nit=job["nit"], sap_tv_iters=job["sap_tv_iters"], max_rhs=3)
+    ctx.set_gauge(g["gauge"])
+    for l, W in enumerate(R.reference_initial_test_vectors(R.read_parameters(m["ns"], m["nt"], m["rows"]))):
+        ctx.set_initial_test_vectors(l, W)
+    ctx.setup()
+    x, info = ctx.solve(g["rhs"])
+    # three sources at once: each must equal its single-source solve
+    b3 = np.stack([g["rhs"], g["probe_l0"], g["rhs"] * (1 + 2j)])
+    x3, info3 = ctx.solve(b3)
+    xs = [ctx.solve(b3[i])[0] for i in range(3)]
+    out[name] = dict(it=info[0]["iterations"], ref_it=m["iterations"], err=rel(x, g["x"]),
+                     batch_err=max(rel(x3[i], xs[i]) for i in range(3)),
+                     batch_it=[i["iterations"] for i in info3], res=max(i["rel_residual"] for i in info3))
+    ctx.close()
+print("RESULT" + json.dumps(out))
+"""
+
+
+@pytest.mark.parametrize("sap,cluster", [("cta", "1"), ("warp", "1"), ("warp", "4"), ("warp", "16")])
+def test_variant_matches_reference(sap, cluster):
+    env = dict(os.environ, AMG_SAP_KERNEL=sap, AMG_ENGINE_CLUSTER=cluster)
+    code = SCRIPT.format(root=str(ROOT), tests=str(ROOT / "tests"))
+    p = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr[-3000:]
+    res = json.loads(p.stdout.split("RESULT", 1)[1])
+    for name, r in res.items():
+        assert r["it"] == r["ref_it"], (name, r)
+        assert r["err"] < 1e-8, (name, r)
+        assert r["batch_err"] < 1e-12, (name, r)
+        assert r["res"] < 1e-10, (name, r)
