@@ -6,7 +6,7 @@
 #include <cstdlib>
 
 #include "kernels.h"
-#include "sap_warp.cuh"
+#include "sap_lean.cuh"
 
 namespace amgb {
 
@@ -490,12 +490,12 @@ void launch_norm2(const cx<T>* v, long long len, long long stride, int nrhs, dou
 }
 int residual_partials(int nx, int nt) { return (nx * nt + 255) / 256; }
 
-// AMG_SAP_KERNEL=cta selects the CTA-per-block SAP kernel for every block shape (A/B tests)
+// AMG_SAP_KERNEL=generic selects the generic SAP kernel for every block shape (A/B tests)
 static int g_sap0_warp = -1;
 int sap0_warp_enabled() {
     if (g_sap0_warp < 0) {
         const char* e = getenv("AMG_SAP_KERNEL");
-        g_sap0_warp = (e && e[0] == 'c') ? 0 : 1;
+        g_sap0_warp = (e && e[0] == 'g') ? 0 : 1;
     }
     return g_sap0_warp;
 }
@@ -530,21 +530,21 @@ int sap0_smem_bytes(int S, int m, int use_smem) {
     return b;
 }
 
-template <typename T, int SPL, int WPB>
-cudaError_t launch_sap0_warp(const cx<T>* U, const cx<T>* r, cx<T>* x, const int* blocks, int ncol, int nrhs, int nx,
+template <typename T, int SPT, int NW>
+cudaError_t launch_sap0_lean(const cx<T>* U, const cx<T>* r, cx<T>* x, const int* blocks, int ncol, int nrhs, int nx,
                              int nt, int sbt, int sxe, int ste, T m0, int restarts, T tol, int* iters, const int* act,
                              cudaStream_t s) {
-    const int bytes = sap0_warp_smem<T, 5, SPL>(WPB);
-    cudaError_t e = cudaFuncSetAttribute(k_sap0_warp<T, 5, SPL, WPB>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    const int bytes = sap0_lean_smem<T, 5, SPT, NW>();
+    cudaError_t e = cudaFuncSetAttribute(k_sap0_lean<T, 5, SPT, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e != cudaSuccess) return e;
-    dim3 grid((ncol + WPB - 1) / WPB, nrhs);
-    k_sap0_warp<T, 5, SPL, WPB><<<grid, 32 * WPB, bytes, s>>>(U, r, x, blocks, ncol, nx, nt, sbt, sxe, ste, m0, restarts,
-                                                              tol, act, iters);
+    dim3 grid(ncol, nrhs);
+    k_sap0_lean<T, 5, SPT, NW><<<grid, 32 * NW, bytes, s>>>(U, r, x, blocks, ncol, nx, nt, sbt, sxe, ste, m0, restarts,
+                                                            tol, act, iters);
     return cudaGetLastError();
 }
 
-// Blocks of 32, 64, 128 or 256 sites with the reference's restart length 5 take the
-// warp-per-block kernel; any other shape takes the CTA-per-block kernel above.
+// Blocks of 64 to 1024 sites with the reference's restart length 5 take the lean kernel
+// (sap_lean.cuh); any other shape or restart length takes the generic kernel above.
 template <typename T>
 cudaError_t launch_sap0(const cx<T>* U, const cx<T>* r, cx<T>* x, const int* blocks, int ncol, int nrhs, int nx,
                         int nt, int sbt, int sxe, int ste, T m0, int m, int restarts, T tol, int use_smem,
@@ -552,12 +552,12 @@ cudaError_t launch_sap0(const cx<T>* U, const cx<T>* r, cx<T>* x, const int* blo
     count_launch(1);
     const int S = sxe * ste;
     if (m == 5 && sap0_warp_enabled()) {
-        constexpr int W = sizeof(T) == 8 ? 2 : 4;
         switch (S) {
-            case 32: return launch_sap0_warp<T, 1, W>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
-            case 64: return launch_sap0_warp<T, 2, W>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
-            case 128: return launch_sap0_warp<T, 4, W>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
-            case 256: return launch_sap0_warp<T, 8, W>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
+            case 64: return launch_sap0_lean<T, 2, 1>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
+            case 128: return launch_sap0_lean<T, 2, 2>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
+            case 256: return launch_sap0_lean<T, 2, 4>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
+            case 512: return launch_sap0_lean<T, 2, 8>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
+            case 1024: return launch_sap0_lean<T, 4, 8>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
             default: break;
         }
     }

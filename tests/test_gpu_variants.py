@@ -1,6 +1,6 @@
-"""The alternative kernel paths give the reference's results too: the CTA-per-block and
-warp-per-block SAP solvers, and the coarse engine on one CTA or on thread-block clusters of
-4 and 16 CTAs.  Each variant runs in its own process (the choice is read from the
+"""The alternative kernel paths give the reference's results too: the generic and the lean
+fine-level SAP block solvers, and the coarse engine on one CTA or on thread-block clusters
+of 4 and 16 CTAs.  Each variant runs in its own process (the choice is read from the
 environment once per process)."""
 import json
 import os
@@ -42,7 +42,7 @@ print("RESULT" + json.dumps(out))
 """
 
 
-@pytest.mark.parametrize("sap,cluster", [("cta", "1"), ("warp", "1"), ("warp", "4"), ("warp", "16")])
+@pytest.mark.parametrize("sap,cluster", [("generic", "1"), ("lean", "1"), ("lean", "4"), ("lean", "16")])
 def test_variant_matches_reference(sap, cluster):
     env = dict(os.environ, AMG_SAP_KERNEL=sap, AMG_ENGINE_CLUSTER=cluster)
     code = SCRIPT.format(root=str(ROOT), tests=str(ROOT / "tests"))
