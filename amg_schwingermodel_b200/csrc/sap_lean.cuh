@@ -50,7 +50,7 @@ __device__ __forceinline__ void lean_sync() {
 }
 
 template <typename T, int M, int SPT, int NW>
-__global__ void __launch_bounds__(32 * NW) k_sap0_lean(const cx<T>* __restrict__ U, const cx<T>* __restrict__ r,
+__global__ void __launch_bounds__(32 * NW, (sizeof(T) == 4 ? 16 : 8) / NW) k_sap0_lean(const cx<T>* __restrict__ U, const cx<T>* __restrict__ r,
                                                        cx<T>* __restrict__ xg, const int* __restrict__ blocks,
                                                        int ncol, int nx, int nt, int sbt, int sxe, int ste, T m0,
                                                        int restarts, T tol, const int* __restrict__ act,
@@ -148,22 +148,22 @@ __global__ void __launch_bounds__(32 * NW) k_sap0_lean(const cx<T>* __restrict__
         return lean_sum2<T, NW>(s, T(0), part, buf).x;
     };
 
-    cx<T> b[SPT][2], x[SPT][2], w[SPT][2];
+    // the block's source b is the global residual, read through L1 where it is needed
+    const cx<T>* rb = r + off;
+    cx<T> x[SPT][2], w[SPT][2];
 #pragma unroll
     for (int k = 0; k < SPT; k++) {
-        b[k][0] = r[off + 2 * gs[k]];
-        b[k][1] = r[off + 2 * gs[k] + 1];
-        x[k][0] = b[k][0];
-        x[k][1] = b[k][1];
+        x[k][0] = __ldg(&rb[2 * gs[k]]);
+        x[k][1] = __ldg(&rb[2 * gs[k] + 1]);
     }
     // r = b - A x0 (x0 = b) into V0
-    store(V, b);
+    store(V, x);
+    const T normb = sqrt(norm2(x));
     lean_sync<T, NW>();
     apply(V, w);
 #pragma unroll
-    for (int k = 0; k < SPT; k++) { w[k][0] = b[k][0] - w[k][0]; w[k][1] = b[k][1] - w[k][1]; }
+    for (int k = 0; k < SPT; k++) { w[k][0] = x[k][0] - w[k][0]; w[k][1] = x[k][1] - w[k][1]; }
     T err = sqrt(norm2(w));
-    const T normb = sqrt(norm2(b));
     int maxit = M;
     int ret = restarts * M;
     for (int kk = 0; kk < restarts; kk++) {
@@ -216,32 +216,33 @@ __global__ void __launch_bounds__(32 * NW) k_sap0_lean(const cx<T>* __restrict__
                     Vn[S + m] = inv * w[k][1];
                 }
             }
-            // rotation(j) (src/fgmres.cpp:90-104): every thread computes it, thread 0 stores
-            col[j + 1] = mk<T>(hn, T(0));
-#pragma unroll
-            for (int i = 0; i < j; i++) {
-                const cx<T> c = cn[i], s = sn[i];
-                const cx<T> temp = cmulc(c, col[i]) + cmulc(s, col[i + 1]);
-                col[i + 1] = cmul(c, col[i + 1]) - cmul(s, col[i]);
-                col[i] = temp;
-            }
-            const T den = sqrt(cnorm2(col[j]) + cnorm2(col[j + 1]));
-            const cx<T> snj = mk<T>(col[j + 1].x / den, col[j + 1].y / den);
-            const cx<T> cnj = mk<T>(col[j].x / den, col[j].y / den);
-            col[j] = cmulc(cnj, col[j]) + cmulc(snj, col[j + 1]);
-            const cx<T> gj = gv[j];
-            const cx<T> gj1 = -cmul(snj, gj);
+            // rotation(j) (src/fgmres.cpp:90-104): warp 0 computes it, lane 0 stores it
             lean_sync<T, NW>();
-            if (tid == 0) {
+            if (tid < 32) {
+                col[j + 1] = mk<T>(hn, T(0));
 #pragma unroll
-                for (int i = 0; i <= j; i++) H[i * M + j] = col[i];
-                sn[j] = snj;
-                cn[j] = cnj;
-                gv[j + 1] = gj1;
-                gv[j] = cmulc(cnj, gj);
+                for (int i = 0; i < j; i++) {
+                    const cx<T> c = cn[i], s = sn[i];
+                    const cx<T> temp = cmulc(c, col[i]) + cmulc(s, col[i + 1]);
+                    col[i + 1] = cmul(c, col[i + 1]) - cmul(s, col[i]);
+                    col[i] = temp;
+                }
+                const T den = sqrt(cnorm2(col[j]) + cnorm2(col[j + 1]));
+                const cx<T> snj = mk<T>(col[j + 1].x / den, col[j + 1].y / den);
+                const cx<T> cnj = mk<T>(col[j].x / den, col[j].y / den);
+                col[j] = cmulc(cnj, col[j]) + cmulc(snj, col[j + 1]);
+                const cx<T> gj = gv[j];
+                if (tid == 0) {
+#pragma unroll
+                    for (int i = 0; i <= j; i++) H[i * M + j] = col[i];
+                    sn[j] = snj;
+                    cn[j] = cnj;
+                    gv[j + 1] = -cmul(snj, gj);
+                    gv[j] = cmulc(cnj, gj);
+                }
             }
             lean_sync<T, NW>();
-            if (sqrt(cnorm2(gj1)) < tol * normb) {
+            if (sqrt(cnorm2(gv[j + 1])) < tol * normb) {
                 maxit = j + 1;
                 break;
             }
@@ -274,7 +275,10 @@ __global__ void __launch_bounds__(32 * NW) k_sap0_lean(const cx<T>* __restrict__
         lean_sync<T, NW>();
         apply(V + 2 * S, w);
 #pragma unroll
-        for (int k = 0; k < SPT; k++) { w[k][0] = b[k][0] - w[k][0]; w[k][1] = b[k][1] - w[k][1]; }
+        for (int k = 0; k < SPT; k++) {
+            w[k][0] = __ldg(&rb[2 * gs[k]]) - w[k][0];
+            w[k][1] = __ldg(&rb[2 * gs[k] + 1]) - w[k][1];
+        }
         err = sqrt(norm2(w));
         if (err < tol * normb) {
             ret = kk * M + maxit;
