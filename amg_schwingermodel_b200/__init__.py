@@ -241,6 +241,13 @@ class AMGContext:
             out[name] = dict(ms=ms.value, launches=n.value, bytes=b.value)
         return out
 
+    def engine_counters(self) -> dict:
+        """Coarse-level operation counts since the previous call, per level."""
+        o = np.zeros(6 * 6, dtype=np.int64)
+        check(lib().amg_engine_counters(self._h, _cptr(o), o.size), "amg_engine_counters")
+        names = ("apply", "local_apply", "kfgmres_steps", "gmres_steps", "sap_steps", "sap_calls")
+        return {l: dict(zip(names, map(int, o[6 * l: 6 * l + 6]))) for l in range(1, self.levels)}
+
     def timings(self):
         s, v = C.c_double(0), C.c_double(0)
         check(lib().amg_last_timings(self._h, C.byref(s), C.byref(v)), "amg_last_timings")

@@ -90,6 +90,7 @@ SIGNATURES = {
     "amg_profile_query": (_I, [_P, _I, C.POINTER(_D), C.POINTER(C.c_longlong), C.POINTER(_D)]),
     "amg_launch_count": (C.c_longlong, []),
     "amg_get_stream": (_P, [_P]),
+    "amg_engine_counters": (_I, [_P, _P, _I]),
 }
 
 PROF_SLOTS = {"sap": 0, "engine": 1, "restrict": 2, "prolong": 3, "fine_op": 4, "blas": 5}

@@ -255,11 +255,19 @@ __global__ void k_sap_check(const double* norm2, const double* vnorm2, double to
     if (i >= R || !act[i]) return;
     if (sqrt(norm2[i]) < tol * sqrt(vnorm2[i])) { act[i] = 0; conv[i] = 1; }
 }
-// scale[r] = 1/sqrt(n2[r]) when positive; wmask[r] = arn[r] && n2[r] > 0
-__global__ void k_inv_norm(const double2* n2, int stride, int off, double* scale, const int* arn, int* wmask, int R) {
+// Re-orthogonalise a source only when the first Gram-Schmidt pass cancelled more than half of
+// |w|^2 ("twice is enough": |w'| < |w| / sqrt(2)); d1[r][nv] = |w|^2, d2[r][nv] = |w'|^2.
+__global__ void k_reorth_flag(const double2* d1, const double2* d2, int nv, const int* arn, int* flag, int R) {
     const int i = threadIdx.x;
     if (i >= R) return;
-    const double v = n2[i * stride + off].x;
+    flag[i] = (arn[i] && d2[i * (nv + 1) + nv].x < 0.5 * d1[i * (nv + 1) + nv].x) ? 1 : 0;
+}
+// scale[r] = 1/|w_final|, wmask[r] = arn[r] && |w_final| > 0, |w_final|^2 from pass 2 or pass 3
+__global__ void k_inv_norm2(const double2* d2, const double2* d3, const int* flag, int nv, double* scale,
+                            const int* arn, int* wmask, int R) {
+    const int i = threadIdx.x;
+    if (i >= R) return;
+    const double v = flag[i] ? d3[i].x : d2[i * (nv + 1) + nv].x;
     const double h = sqrt(v);
     scale[i] = h > 0 ? 1.0 / h : 0.0;
     wmask[i] = (arn[i] && h > 0) ? 1 : 0;
@@ -306,6 +314,7 @@ int build_engine(amg_context* c, PrecSet<T>& ps, int nsrc) {
     for (int l = 1; l < c->L; l++) {
         const LevelHost& h = c->lv[l];
         EngLevel<T>& e = a.lv[l];
+        e.level = l;
         e.nx = h.nx; e.nt = h.nt; e.n = h.n; e.K = h.K; e.coarsest = h.coarsest;
         e.bx = h.bx; e.bt = h.bt; e.xe = h.xe; e.te = h.te; e.ntest = h.ntest;
         e.W = h.coarsest ? nullptr : ps.W[l].template as<cx<T>>();
@@ -346,11 +355,13 @@ int build_engine(amg_context* c, PrecSet<T>& ps, int nsrc) {
     ps.eng_cap = std::max(nsrc, 1);
     ps.max_cluster = engine_cluster_limit();
     CKR(ps.eng_work.alloc((size_t)a.slab * ps.eng_cap * ps.max_cluster * sizeof(cx<T>)));
-    CKR(ps.eng_status.alloc(sizeof(int) * (ps.eng_cap + 4)));
+    CKR(ps.eng_status.alloc(sizeof(int) * (ps.eng_cap + 4) + sizeof(unsigned long long) * kMaxLevels * ENG_NCOUNT));
     a.work = ps.eng_work.template as<cx<T>>();
     a.status = ps.eng_status.template as<int>();
     a.flags = a.status + ps.eng_cap;
+    a.counters = reinterpret_cast<unsigned long long*>(a.status + ps.eng_cap + 4);
     CK(cudaMemsetAsync(a.flags, 0, sizeof(int), c->stream));
+    CK(cudaMemsetAsync(a.counters, 0, sizeof(unsigned long long) * kMaxLevels * ENG_NCOUNT, c->stream));
     CKR(ps.eng_args.alloc(sizeof(EngArgs<T>)));
     CK(cudaMemcpyAsync(ps.eng_args.p, &a, sizeof a, cudaMemcpyHostToDevice, c->stream));
     return AMG_OK;
@@ -390,7 +401,7 @@ int alloc_fine(amg_context* c, PrecSet<T>& ps, int R) {
     CKR(ps.psi1.alloc((size_t)R * h1.n * h1.K * sizeof(cx<T>)));
     const int nblk = h0.bx * h0.bt;
     const int spb = h0.xe * h0.te;
-    int nchunk = std::max(1, std::min(std::max(1, spb / 256), (592 + nblk - 1) / nblk));
+    int nchunk = std::max(1, std::min(std::max(1, spb / 128), (1184 + nblk - 1) / nblk));
     CKR(ps.rpart.alloc((size_t)R * nblk * nchunk * 2 * h0.ntest * sizeof(cx<T>)));
     return AMG_OK;
 }
@@ -401,7 +412,7 @@ int restrict_chunks(amg_context* c, int R) {
     const int nblk = h0.bx * h0.bt;
     const int spb = h0.xe * h0.te;
     (void)R;
-    return std::max(1, std::min(std::max(1, spb / 256), (592 + nblk - 1) / nblk));
+    return std::max(1, std::min(std::max(1, spb / 128), (1184 + nblk - 1) / nblk));
 }
 
 template <typename T>
@@ -568,6 +579,7 @@ int outer_fgmres(amg_context* c, const double2* b, double2* x, int R, amg_solve_
     int* arn_d = act_d + c->Rcap;
     int* wm_d = arn_d + c->Rcap;
     int* nvr_d = wm_d + c->Rcap;
+    int* ro_d = nvr_d + c->Rcap;
     double2* eta_d = c->etab.as<double2>();
     const double2* U = c->d.U.as<double2>();
     const int np = std::min<long long>(592, (len + 255) / 256);
@@ -627,16 +639,20 @@ int outer_fgmres(amg_context* c, const double2* b, double2* x, int R, amg_solve_
             double2* d2 = dots + (size_t)R * (nv + 1);
             double2* d3 = d2 + (size_t)R * (nv + 1);
             {
-                ProfScope ps_(c, AMG_PROF_BLAS, (double)R * len * sizeof(double2) * (3.0 * (nv + 1) + 5.0));
-                launch_multidot(w, V, len, vstride, nv, R, dpart, np, d1, c->stream);
+                // classical Gram-Schmidt, re-orthogonalised only where the first pass cancelled
+                ProfScope ps_(c, AMG_PROF_BLAS, (double)R * len * sizeof(double2) * (2.0 * (nv + 1) + 4.0));
+                launch_multidot(w, V, len, vstride, nv, R, dpart, np, d1, arn_d, c->stream);
                 launch_axpy_multidot(w, V, len, vstride, nv, d1, nv + 1, nv, arn_d, R, dpart, np, d2, c->stream);
-                launch_axpy_multidot(w, V, len, vstride, nv, d2, nv + 1, 0, arn_d, R, dpart, np, d3, c->stream);
-                k_inv_norm<<<1, 256, 0, c->stream>>>(d3, 1, 0, scal, arn_d, wm_d, R);
-                count_launch(1);
+                k_reorth_flag<<<1, 256, 0, c->stream>>>(d1, d2, nv, arn_d, ro_d, R);
+                launch_axpy_multidot(w, V, len, vstride, nv, d2, nv + 1, 0, ro_d, R, dpart, np, d3, c->stream);
+                k_inv_norm2<<<1, 256, 0, c->stream>>>(d2, d3, ro_d, nv, scal, arn_d, wm_d, R);
+                count_launch(2);
                 launch_scale(V + (long long)(j + 1) * vstride, w, len, scal, wm_d, R, c->stream);
             }
             std::vector<double2> hd((size_t)R * (2 * (nv + 1) + 1));
+            std::vector<int> ro(R);
             CK(cudaMemcpyAsync(hd.data(), dots, hd.size() * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+            CK(cudaMemcpyAsync(ro.data(), ro_d, R * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
             CK(cudaStreamSynchronize(c->stream));
             for (int r = 0; r < R; r++) {
                 if (!arn[r]) continue;
@@ -647,9 +663,10 @@ int outer_fgmres(amg_context* c, const double2* b, double2* x, int R, amg_solve_
                 for (int i = 0; i <= j; i++) {
                     const double2 a = hd[(size_t)r * (nv + 1) + i];
                     const double2 bq = hd[(size_t)R * (nv + 1) + (size_t)r * (nv + 1) + i];
-                    Hr[i * m + j] = cd(a.x + bq.x, a.y + bq.y);
+                    Hr[i * m + j] = ro[r] ? cd(a.x + bq.x, a.y + bq.y) : cd(a.x, a.y);
                 }
-                const double hn2 = hd[(size_t)2 * R * (nv + 1) + r].x;
+                const double hn2 = ro[r] ? hd[(size_t)2 * R * (nv + 1) + r].x
+                                         : hd[(size_t)R * (nv + 1) + (size_t)r * (nv + 1) + nv].x;
                 Hr[(j + 1) * m + j] = cd(std::sqrt(hn2), 0);
                 // rotation(j) (src/fgmres.cpp:90-104)
                 for (int i = 0; i < j; i++) {
@@ -733,7 +750,7 @@ int ensure_capacity(amg_context* c, int R) {
     CKR(c->partial.alloc(np * Rn * 24 * sizeof(double2)));
     CKR(c->dots.alloc((size_t)Rn * 3 * 24 * sizeof(double2)));
     CKR(c->scal.alloc((size_t)Rn * sizeof(double)));
-    CKR(c->masks.alloc((size_t)4 * Rn * sizeof(int)));
+    CKR(c->masks.alloc((size_t)5 * Rn * sizeof(int)));
     CKR(c->etab.alloc((size_t)Rn * m * sizeof(double2)));
     CKR(c->sap_flags.alloc((size_t)2 * Rn * sizeof(int)));
     CKR(c->norms.alloc((size_t)2 * Rn * sizeof(double)));
@@ -1397,6 +1414,18 @@ int amg_force(amg_ctx c, const double* lambda, const double* x, int nrhs, double
 int amg_force_dev(amg_ctx c, const void* lambda, const void* x, int nrhs, void* F) {
     (void)c; (void)lambda; (void)x; (void)nrhs; (void)F;
     return fail(AMG_ERR_UNSUPPORTED, "force not built yet");
+}
+
+int amg_engine_counters(amg_ctx c, long long* out, int len) {
+    if (!c || !out) return fail(AMG_ERR_INVALID, "null argument");
+    PrecSet<double>& d = c->d;
+    std::vector<unsigned long long> v(kMaxLevels * ENG_NCOUNT, 0), w(kMaxLevels * ENG_NCOUNT, 0);
+    if (d.eh.counters) CK(cudaMemcpy(v.data(), d.eh.counters, v.size() * 8, cudaMemcpyDeviceToHost));
+    if (c->f.ready && c->f.eh.counters) CK(cudaMemcpy(w.data(), c->f.eh.counters, w.size() * 8, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < len && i < (int)v.size(); i++) out[i] = (long long)(v[i] + w[i]);
+    if (d.eh.counters) CK(cudaMemset(d.eh.counters, 0, v.size() * 8));
+    if (c->f.ready && c->f.eh.counters) CK(cudaMemset(c->f.eh.counters, 0, w.size() * 8));
+    return AMG_OK;
 }
 
 long long amg_launch_count(void) { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }

@@ -21,6 +21,7 @@ enum { HOP_SELF = 0, HOP_R0 = 1, HOP_R1 = 2, HOP_L0 = 3, HOP_L1 = 4 };
 // Per-level description used by the engine (device copy lives in kernel parameters).
 template <typename T>
 struct EngLevel {
+    int level;                  // index of this level in the hierarchy
     int nx, nt, n, K;           // lattice and dof per site
     int coarsest;
     // aggregation to level l+1
@@ -68,7 +69,12 @@ struct EngArgs {
     long long io_len;            // elements of each copy
     int* status;                 // [nsrc] per-source result code / iteration count
     int* flags;                  // error flag (bit 0: recursion bound, bit 1: unsupported)
+    unsigned long long* counters;  // [kMaxLevels][ENG_NCOUNT] operation counts (tracing)
 };
+
+// engine operation counters, per level
+enum { CNT_APPLY = 0, CNT_LOCAL_APPLY = 1, CNT_KFG_STEP = 2, CNT_GMRES_STEP = 3, CNT_SAP_STEP = 4, CNT_SAP_CALL = 5,
+       ENG_NCOUNT = 6 };
 
 // ---------------------------------------------------------------------------------
 // FGMRES scalar state for nseg independent segments
@@ -218,6 +224,12 @@ struct Eng {
     __device__ cx<T>* work(long long off) const { return slab + off; }
 };
 
+template <typename T>
+__device__ __forceinline__ void eng_count(const Eng<T>& E, int level, int what, unsigned long long n = 1) {
+    if (E.a->counters && E.crank == 0 && threadIdx.x == 0)
+        atomicAdd(&E.a->counters[level * ENG_NCOUNT + what], n);
+}
+
 // ---------------------------------------------------------------------------------
 // level geometry helpers
 // ---------------------------------------------------------------------------------
@@ -276,6 +288,7 @@ __device__ __noinline__ void dc_apply(const Eng<T>& E, const EngLevel<T>& L, T m
     const int K = L.K, tot = L.n * K;
     const T mass = m0 + T(2);
     int e0, e1;
+    eng_count(E, L.level, CNT_APPLY);
     part_range(E, tot, e0, e1);
     part_begin(E);
     for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
@@ -318,6 +331,7 @@ __device__ __noinline__ void dlocal_apply(const Eng<T>& E, const EngLevel<T>& L,
     const int K = L.K, spb = L.sxe * L.ste, seglen = spb * K, tot = nblk * seglen;
     const T mass = m0 + T(2);
     int e0, e1;
+    eng_count(E, L.level, CNT_LOCAL_APPLY);
     part_range(E, tot, e0, e1);
     part_begin(E);
     for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
@@ -429,8 +443,8 @@ __device__ __noinline__ void prolong_v(const Eng<T>& E, const EngLevel<T>& L, co
 // Returns in st.iters[s] the reference's return value (k*m + maxIt or restarts*m).
 // ---------------------------------------------------------------------------------
 template <typename T, class Op, class Pre>
-__device__ void seg_fgmres(const Seg<T>& sp, Op& op, Pre& pre, const cx<T>* b, cx<T>* x,
-                           cx<T>* V, cx<T>* Z, cx<T>* w, const GmState<T>& st, int m,
+__device__ void seg_fgmres(const Eng<T>* E, int cnt_level, int cnt_what, const Seg<T>& sp, Op& op, Pre& pre,
+                           const cx<T>* b, cx<T>* x, cx<T>* V, cx<T>* Z, cx<T>* w, const GmState<T>& st, int m,
                            int restarts, T tol) {
     const int nseg = sp.nseg, seglen = sp.seglen, tot = nseg * seglen;
     const long long vstride = tot;
@@ -478,6 +492,7 @@ __device__ void seg_fgmres(const Seg<T>& sp, Op& op, Pre& pre, const cx<T>* b, c
             int anyarn = 0;
             for (int s = 0; s < nseg; s++) anyarn |= st.arn[s];
             if (!anyarn) break;
+            if (E) eng_count(*E, cnt_level, cnt_what);
             cx<T>* Vj = V + (long long)j * vstride;
             cx<T>* Zj = (Z == V) ? Vj : Z + (long long)j * vstride;
             pre(j, Vj, Zj, st.arn);
@@ -598,6 +613,7 @@ __device__ __noinline__ int eng_sap(const Eng<T>& E, int l, const cx<T>* v, cx<T
     Seg<T> sp1 = make_seg<T>(1, nvec, E.red);
     Seg<T> sps = make_seg<T>(nseg, seglen, E.red);
 
+    eng_count(E, l, CNT_SAP_CALL);
     seg_dot(sp1, v, v, st.red);
     const T vnorm = sqrt(st.red[0].x);
     dc_apply(E, L, p.m0, x, r);
@@ -608,7 +624,8 @@ __device__ __noinline__ int eng_sap(const Eng<T>& E, int l, const cx<T>* v, cx<T
             sap_gather(L, blocks, nseg, r, bseg);
             auto lop = [&](const cx<T>* in, cx<T>* out) { dlocal_apply(E, L, p.m0, blocks, nseg, in, out); };
             auto ident = [](int, const cx<T>*, cx<T>*, const int*) {};
-            seg_fgmres(sps, lop, ident, bseg, xseg, Vseg, Vseg, wseg, st, p.sap_m, p.sap_restarts, p.sap_gmres_tol);
+            seg_fgmres(&E, l, CNT_SAP_STEP, sps, lop, ident, bseg, xseg, Vseg, Vseg, wseg, st, p.sap_m, p.sap_restarts,
+                       p.sap_gmres_tol);
             sap_scatter_add(L, blocks, nseg, xseg, x);
             dc_apply(E, L, p.m0, x, r);
             v_sub<T>(r, v, r, nvec);
@@ -634,7 +651,7 @@ __device__ __noinline__ int eng_coarse_gmres(const Eng<T>& E, int l, const cx<T>
     Seg<T> sp = make_seg<T>(1, nvec, E.red);
     auto op = [&](const cx<T>* in, cx<T>* out) { dc_apply(E, L, p.m0, in, out); };
     auto ident = [](int, const cx<T>*, cx<T>*, const int*) {};
-    seg_fgmres(sp, op, ident, b, x, V, V, w, st, L.gm_m, L.gm_restarts, L.gm_tol);
+    seg_fgmres(&E, l, CNT_GMRES_STEP, sp, op, ident, b, x, V, V, w, st, L.gm_m, L.gm_restarts, L.gm_tol);
     return st.iters[0];
 }
 
@@ -699,7 +716,7 @@ struct Cycles {
         Seg<T> sp = make_seg<T>(1, nvec, E.red);
         auto op = [&](const cx<T>* in, cx<T>* out) { dc_apply(E, L, p.m0, in, out); };
         auto pre = [&](int, const cx<T>* v, cx<T>* z, const int*) { Cycles<T, D>::kcycle(E, l, v, z); };
-        seg_fgmres(sp, op, pre, b, x, V, Z, w, st, p.k_m, p.k_restarts, p.k_tol);
+        seg_fgmres(&E, l, CNT_KFG_STEP, sp, op, pre, b, x, V, Z, w, st, p.k_m, p.k_restarts, p.k_tol);
         return st.iters[0];
     }
 };

@@ -105,53 +105,50 @@ __global__ void k_sum_partials(const double* __restrict__ partial, int nparts, d
 //   out[rhs][nc][2cc+s] = sum_{n in block nc} conj(W[cc][n][s]) v[rhs][n][s]
 // Grid (chunk, block, rhs); per-chunk partials reduced by k_restrict0_sum in chunk order.
 // ---------------------------------------------------------------------------------
+// Multi-source form of the level-0 restriction: one CTA per (chunk of an aggregation
+// block, block) serves every source, one warp per source at a time, so the chunk's test
+// vectors come from DRAM once and from L1 for the other sources; each warp reduces its
+// own source's 2*ntest sums with shuffles.
 template <typename T, typename TW, int NV>
-__global__ void __launch_bounds__(256) k_restrict0(const TW* __restrict__ W, const cx<T>* __restrict__ v,
-                                                   cx<T>* __restrict__ partial, int nx, int nt, int bt, int xe,
-                                                   int te, int nchunk, int ntest) {
-    extern __shared__ __align__(16) unsigned char smraw_r[];
-    T* red = reinterpret_cast<T*>(smraw_r);
+__global__ void __launch_bounds__(256) k_restrict0m(const TW* __restrict__ W, const cx<T>* __restrict__ v,
+                                                    cx<T>* __restrict__ partial, int nx, int nt, int bt, int xe,
+                                                    int te, int nchunk, int ntest, int nrhs) {
     const int N = nx * nt;
-    const int chunk = blockIdx.x, nc = blockIdx.y, rhs = blockIdx.z;
+    const int chunk = blockIdx.x, nc = blockIdx.y;
     const int bxi = nc / bt, bti = nc - bxi * bt;
     const int spb = xe * te;
     const int per = (spb + nchunk - 1) / nchunk;
     const int q0 = chunk * per, q1 = min(spb, q0 + per);
-    const cx<T>* vv = v + (long long)rhs * N * 2;
-    cx<T> acc[NV][2];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int rhs = wid; rhs < nrhs; rhs += nw) {
+        const cx<T>* vv = v + (long long)rhs * N * 2;
+        cx<T> acc[NV][2];
 #pragma unroll
-    for (int k = 0; k < NV; k++) { acc[k][0] = czero<T>(); acc[k][1] = czero<T>(); }
-    for (int q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
-        const int mx = q / te, mt = q - mx * te;
-        const long long n = (long long)(bxi * xe + mx) * nt + (bti * te + mt);
-        const cx<T> p0 = vv[2 * n], p1 = vv[2 * n + 1];
+        for (int k = 0; k < NV; k++) { acc[k][0] = czero<T>(); acc[k][1] = czero<T>(); }
+        for (int q = q0 + lane; q < q1; q += 32) {
+            const int mx = q / te, mt = q - mx * te;
+            const long long n = (long long)(bxi * xe + mx) * nt + (bti * te + mt);
+            const cx<T> p0 = vv[2 * n], p1 = vv[2 * n + 1];
 #pragma unroll
-        for (int k = 0; k < NV; k++) {
-            if (k < ntest) {
-                cx<T> w0 = ccast<T>(load_cx(W + ((long long)k * N + n) * 2));
-                cx<T> w1 = ccast<T>(load_cx(W + ((long long)k * N + n) * 2 + 1));
-                cfmac(acc[k][0], w0, p0);
-                cfmac(acc[k][1], w1, p1);
+            for (int k = 0; k < NV; k++) {
+                if (k < ntest) {
+                    const cx<T> w0 = ccast<T>(load_cx(W + ((long long)k * N + n) * 2));
+                    const cx<T> w1 = ccast<T>(load_cx(W + ((long long)k * N + n) * 2 + 1));
+                    cfmac(acc[k][0], w0, p0);
+                    cfmac(acc[k][1], w1, p1);
+                }
             }
         }
-    }
-    // CTA reduction of 4*NV reals: warp shuffles, then one value per warp in smem
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+        cx<T>* out = partial + (((long long)rhs * gridDim.y + nc) * nchunk + chunk) * (2 * ntest);
 #pragma unroll
-    for (int k = 0; k < NV; k++) {
-        if (k >= ntest) break;
+        for (int k = 0; k < NV; k++) {
+            if (k >= ntest) break;
 #pragma unroll
-        for (int s = 0; s < 2; s++) {
-            T xr = warp_sum(acc[k][s].x), xi = warp_sum(acc[k][s].y);
-            if (lane == 0) { red[((k * 2 + s) * nw + wid) * 2] = xr; red[((k * 2 + s) * nw + wid) * 2 + 1] = xi; }
+            for (int s = 0; s < 2; s++) {
+                const T xr = warp_sum(acc[k][s].x), xi = warp_sum(acc[k][s].y);
+                if (lane == 0) out[2 * k + s] = mk<T>(xr, xi);
+            }
         }
-    }
-    __syncthreads();
-    for (int o = threadIdx.x; o < ntest * 2; o += blockDim.x) {
-        T sr = 0, si = 0;
-        for (int w = 0; w < nw; w++) { sr += red[(o * nw + w) * 2]; si += red[(o * nw + w) * 2 + 1]; }
-        // o = k*2 + s  ->  coarse dof 2k + s
-        partial[(((long long)rhs * gridDim.y + nc) * nchunk + chunk) * (2 * ntest) + o] = mk<T>(sr, si);
     }
 }
 
@@ -276,7 +273,7 @@ __global__ void __launch_bounds__(256) k_sap0_blocks(const cx<T>* __restrict__ U
     Seg<T> sp = make_seg<T>(1, len, red);
     auto op = [&](const cx<T>* in, cx<T>* out) { fine_block_apply(B, in, out); };
     auto ident = [](int, const cx<T>*, cx<T>*, const int*) {};
-    seg_fgmres(sp, op, ident, b, xs, V, V, w, st, m, restarts, tol);
+    seg_fgmres<T>(nullptr, 0, 0, sp, op, ident, b, xs, V, V, w, st, m, restarts, tol);
     cx<T>* xx = x + (long long)rhs * N * 2;
     for (int q = threadIdx.x; q < S; q += blockDim.x) {
         const int mx = q / ste, mt = q - mx * ste;
@@ -290,38 +287,6 @@ __global__ void __launch_bounds__(256) k_sap0_blocks(const cx<T>* __restrict__ U
 // ---------------------------------------------------------------------------------
 // BLAS-1 for the outer FGMRES (FP64).  Vectors are [rhs][len]; V bases [j][rhs][len].
 // ---------------------------------------------------------------------------------
-// partial[rhs][k][blk] = sum_e w[e] * conj(V_k[e]) for k < nv, and |w|^2 at k = nv
-__global__ void __launch_bounds__(256) k_multidot(const double2* __restrict__ w, const double2* __restrict__ V,
-                                                  long long len, long long vstride, int nv, int nrhs,
-                                                  double2* __restrict__ partial) {
-    __shared__ double red[2 * 8 * 24];
-    const int rhs = blockIdx.y;
-    const double2* ww = w + (long long)rhs * len;
-    double ax[24], ay[24];
-    for (int k = 0; k <= nv; k++) { ax[k] = 0; ay[k] = 0; }
-    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (long long)gridDim.x * blockDim.x) {
-        const double2 a = ww[e];
-#pragma unroll 4
-        for (int k = 0; k < nv; k++) {
-            const double2 b = V[(long long)k * vstride + (long long)rhs * len + e];
-            ax[k] += a.x * b.x + a.y * b.y;
-            ay[k] += a.y * b.x - a.x * b.y;
-        }
-        ax[nv] += a.x * a.x + a.y * a.y;
-    }
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    for (int k = 0; k <= nv; k++) {
-        double sx = warp_sum(ax[k]), sy = warp_sum(ay[k]);
-        if (lane == 0) { red[(k * 8 + wid) * 2] = sx; red[(k * 8 + wid) * 2 + 1] = sy; }
-    }
-    __syncthreads();
-    for (int k = threadIdx.x; k <= nv; k += blockDim.x) {
-        double sx = 0, sy = 0;
-        for (int q = 0; q < 8; q++) { sx += red[(k * 8 + q) * 2]; sy += red[(k * 8 + q) * 2 + 1]; }
-        partial[((long long)rhs * (nv + 1) + k) * gridDim.x + blockIdx.x] = make_double2(sx, sy);
-    }
-}
-
 __global__ void k_multidot_sum(const double2* __restrict__ partial, int nparts, double2* __restrict__ out) {
     __shared__ double red[64];
     const int o = blockIdx.x;   // (rhs, k) flattened
@@ -355,47 +320,64 @@ __global__ void __launch_bounds__(256) k_multiaxpy(double2* __restrict__ w, cons
     }
 }
 
-// w[rhs] -= sum_k h[rhs][k] V_k[rhs], then partial[rhs][k][blk] = sum_e w[e] conj(V_k[e]) for
-// k < nd and |w|^2 at k = nd, all from one pass over w and the basis (classical Gram-Schmidt
-// with re-orthogonalisation needs both halves back to back).
-__global__ void __launch_bounds__(256) k_axpy_multidot(double2* __restrict__ w, const double2* __restrict__ V,
-                                                       long long len, long long vstride, int nv,
-                                                       const double2* __restrict__ h, int hstride, int nd,
-                                                       const int* __restrict__ act, double2* __restrict__ partial) {
-    __shared__ double red[2 * 8 * 24];
+// One pass over w and the basis V_0..V_{nv-1} of every source (FP64):
+//   w -= sum_k h[k] V_k            (skipped when h is null)
+//   partial[k] = sum_e w[e] conj(V_k[e]) for k < nd, and |w|^2 at k = nd
+// with the accumulators in registers (NV bounds nv and nd at compile time); per-CTA
+// partials are reduced by k_multidot_sum in a fixed order.  Sources with act[rhs] = 0 are
+// skipped (their partials are not written).
+template <int NV>
+__global__ void __launch_bounds__(256) k_axpy_dots(double2* __restrict__ w, const double2* __restrict__ V,
+                                                   long long len, long long vstride, int nv,
+                                                   const double2* __restrict__ h, int hstride, int nd,
+                                                   const int* __restrict__ act, double2* __restrict__ partial) {
+    __shared__ double red[8][2 * (NV + 1)];
     const int rhs = blockIdx.y;
-    const bool on = !act || act[rhs];
+    if (act && !act[rhs]) return;
     double2* ww = w + (long long)rhs * len;
-    double ax[24], ay[24];
-    for (int k = 0; k <= nd; k++) { ax[k] = 0; ay[k] = 0; }
-    double2 hk[24];
-    for (int k = 0; k < nv; k++) hk[k] = h[(long long)rhs * hstride + k];
-    if (on) {
-        for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (long long)gridDim.x * blockDim.x) {
-            double2 a = ww[e];
-            for (int k = 0; k < nv; k++) {
-                const double2 b = V[(long long)k * vstride + (long long)rhs * len + e];
-                a.x -= hk[k].x * b.x - hk[k].y * b.y;
-                a.y -= hk[k].x * b.y + hk[k].y * b.x;
+    const double2* vb = V + (long long)rhs * len;
+    double ax[NV + 1], ay[NV + 1];
+    double2 hk[NV];
+#pragma unroll
+    for (int k = 0; k <= NV; k++) { ax[k] = 0; ay[k] = 0; }
+#pragma unroll
+    for (int k = 0; k < NV; k++) hk[k] = (h && k < nv) ? h[(long long)rhs * hstride + k] : make_double2(0, 0);
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (long long)gridDim.x * blockDim.x) {
+        double2 a = ww[e];
+        if (h) {
+#pragma unroll
+            for (int k = 0; k < NV; k++) {
+                if (k < nv) {
+                    const double2 b = vb[(long long)k * vstride + e];
+                    a.x -= hk[k].x * b.x - hk[k].y * b.y;
+                    a.y -= hk[k].x * b.y + hk[k].y * b.x;
+                }
             }
             ww[e] = a;
-            for (int k = 0; k < nd; k++) {
-                const double2 b = V[(long long)k * vstride + (long long)rhs * len + e];
+        }
+#pragma unroll
+        for (int k = 0; k < NV; k++) {
+            if (k < nd) {
+                const double2 b = vb[(long long)k * vstride + e];
                 ax[k] += a.x * b.x + a.y * b.y;
                 ay[k] += a.y * b.x - a.x * b.y;
             }
-            ax[nd] += a.x * a.x + a.y * a.y;
         }
+        ax[NV] += a.x * a.x + a.y * a.y;
     }
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    for (int k = 0; k <= nd; k++) {
-        double sx = warp_sum(ax[k]), sy = warp_sum(ay[k]);
-        if (lane == 0) { red[(k * 8 + wid) * 2] = sx; red[(k * 8 + wid) * 2 + 1] = sy; }
+#pragma unroll
+    for (int k = 0; k <= NV; k++) {
+        if (k < nd || k == NV) {
+            const double sx = warp_sum(ax[k]), sy = warp_sum(ay[k]);
+            if (lane == 0) { red[wid][2 * k] = sx; red[wid][2 * k + 1] = sy; }
+        }
     }
     __syncthreads();
     for (int k = threadIdx.x; k <= nd; k += blockDim.x) {
+        const int kk = (k == nd) ? NV : k;
         double sx = 0, sy = 0;
-        for (int q = 0; q < 8; q++) { sx += red[(k * 8 + q) * 2]; sy += red[(k * 8 + q) * 2 + 1]; }
+        for (int q = 0; q < 8; q++) { sx += red[q][2 * kk]; sy += red[q][2 * kk + 1]; }
         partial[((long long)rhs * (nd + 1) + k) * gridDim.x + blockIdx.x] = make_double2(sx, sy);
     }
 }
@@ -506,11 +488,11 @@ void launch_restrict0(const TW* W, const cx<T>* v, cx<T>* out, cx<T>* partial, i
                       int ntest, int nrhs, int nchunk, cudaStream_t s) {
     count_launch(2);
     const int xe = nx / bx, te = nt / bt, nblk = bx * bt;
-    dim3 grid(nchunk, nblk, nrhs);
-    const int smem = 4 * ntest * 8 * sizeof(T) * 2;
-    if (ntest <= 8) k_restrict0<T, TW, 8><<<grid, 256, smem, s>>>(W, v, partial, nx, nt, bt, xe, te, nchunk, ntest);
-    else if (ntest <= 16) k_restrict0<T, TW, 16><<<grid, 256, smem, s>>>(W, v, partial, nx, nt, bt, xe, te, nchunk, ntest);
-    else k_restrict0<T, TW, 32><<<grid, 256, smem, s>>>(W, v, partial, nx, nt, bt, xe, te, nchunk, ntest);
+    dim3 grid(nchunk, nblk);
+    const int thr = nrhs >= 8 ? 256 : 32 * nrhs;
+    if (ntest <= 8) k_restrict0m<T, TW, 8><<<grid, thr, 0, s>>>(W, v, partial, nx, nt, bt, xe, te, nchunk, ntest, nrhs);
+    else if (ntest <= 16) k_restrict0m<T, TW, 16><<<grid, thr, 0, s>>>(W, v, partial, nx, nt, bt, xe, te, nchunk, ntest, nrhs);
+    else k_restrict0m<T, TW, 32><<<grid, thr, 0, s>>>(W, v, partial, nx, nt, bt, xe, te, nchunk, ntest, nrhs);
     dim3 g2((nblk * 2 * ntest + 127) / 128, nrhs);
     k_restrict0_sum<T><<<g2, 128, 0, s>>>(partial, out, nblk, nchunk, 2 * ntest);
 }
@@ -570,21 +552,34 @@ cudaError_t launch_sap0(const cx<T>* U, const cx<T>* r, cx<T>* x, const int* blo
     return cudaGetLastError();
 }
 
-void launch_multidot(const double2* w, const double2* V, long long len, long long vstride, int nv, int nrhs,
-                     double2* partial, int nparts, double2* out, cudaStream_t s) {
-    count_launch(2);
+template <int NV>
+static void axpy_dots_nv(double2* w, const double2* V, long long len, long long vstride, int nv, const double2* h,
+                         int hstride, int nd, const int* act, int nrhs, double2* partial, int nparts, cudaStream_t s) {
     dim3 grid(nparts, nrhs);
-    k_multidot<<<grid, 256, 0, s>>>(w, V, len, vstride, nv, nrhs, partial);
-    k_multidot_sum<<<nrhs * (nv + 1), 256, 0, s>>>(partial, nparts, out);
+    k_axpy_dots<NV><<<grid, 256, 0, s>>>(w, V, len, vstride, nv, h, hstride, nd, act, partial);
 }
+
+// w -= sum_{k<nv} h[k] V_k (h may be null), then out[rhs][k] = <w, V_k> for k < nd and
+// out[rhs][nd] = |w|^2.
 void launch_axpy_multidot(double2* w, const double2* V, long long len, long long vstride, int nv, const double2* h,
                           int hstride, int nd, const int* act, int nrhs, double2* partial, int nparts, double2* out,
                           cudaStream_t s) {
     count_launch(2);
-    dim3 grid(nparts, nrhs);
-    k_axpy_multidot<<<grid, 256, 0, s>>>(w, V, len, vstride, nv, h, hstride, nd, act, partial);
+    const int n = nv > nd ? nv : nd;
+    if (n <= 4) axpy_dots_nv<4>(w, V, len, vstride, nv, h, hstride, nd, act, nrhs, partial, nparts, s);
+    else if (n <= 8) axpy_dots_nv<8>(w, V, len, vstride, nv, h, hstride, nd, act, nrhs, partial, nparts, s);
+    else if (n <= 12) axpy_dots_nv<12>(w, V, len, vstride, nv, h, hstride, nd, act, nrhs, partial, nparts, s);
+    else if (n <= 16) axpy_dots_nv<16>(w, V, len, vstride, nv, h, hstride, nd, act, nrhs, partial, nparts, s);
+    else axpy_dots_nv<24>(w, V, len, vstride, nv, h, hstride, nd, act, nrhs, partial, nparts, s);
     k_multidot_sum<<<nrhs * (nd + 1), 256, 0, s>>>(partial, nparts, out);
 }
+
+void launch_multidot(const double2* w, const double2* V, long long len, long long vstride, int nv, int nrhs,
+                     double2* partial, int nparts, double2* out, const int* act, cudaStream_t s) {
+    launch_axpy_multidot(const_cast<double2*>(w), V, len, vstride, 0, nullptr, 0, nv, act, nrhs, partial, nparts, out,
+                         s);
+}
+
 void launch_multiaxpy(double2* w, const double2* V, long long len, long long vstride, int nv, const double2* h,
                       int hstride, const int* act, int nrhs, cudaStream_t s) {
     count_launch(1);

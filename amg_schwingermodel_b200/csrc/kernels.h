@@ -37,7 +37,7 @@ cudaError_t launch_sap0(const cx<T>* U, const cx<T>* r, cx<T>* x, const int* blo
                         int nt, int sbt, int sxe, int ste, T m0, int m, int restarts, T tol, int use_smem,
                         cx<T>* gscratch, int* iters, const int* act, cudaStream_t s);
 void launch_multidot(const double2* w, const double2* V, long long len, long long vstride, int nv, int nrhs,
-                     double2* partial, int nparts, double2* out, cudaStream_t s);
+                     double2* partial, int nparts, double2* out, const int* act, cudaStream_t s);
 void launch_axpy_multidot(double2* w, const double2* V, long long len, long long vstride, int nv, const double2* h,
                           int hstride, int nd, const int* act, int nrhs, double2* partial, int nparts, double2* out,
                           cudaStream_t s);

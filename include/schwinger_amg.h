@@ -187,6 +187,10 @@ AMG_API int amg_force_dev(amg_ctx ctx, const void* lambda_dev, const void* x_dev
 AMG_API int amg_profile(amg_ctx ctx, int enable);
 /* Accumulated device milliseconds, launch count and algorithmic bytes of one class. */
 AMG_API int amg_profile_query(amg_ctx ctx, int slot, double* ms, long long* launches, double* bytes);
+/* Coarse-level operation counts since the last call (then reset), out[level*6 + k] for
+ * k = operator applies, block-local applies, K-cycle FGMRES steps, level GMRES steps, SAP
+ * block GMRES steps, SAP calls (a tracing aid; the reference keeps no such counts). */
+AMG_API int amg_engine_counters(amg_ctx ctx, long long* out, int len);
 /* Number of CUDA kernels the library has launched so far (all contexts). */
 AMG_API long long amg_launch_count(void);
 /* The cudaStream_t every call on this context runs on (for callers that time or order work). */
