@@ -335,21 +335,41 @@ int build_engine(amg_context* c, PrecSet<T>& ps, int nsrc) {
             const LevelHost& hn = c->lv[l + 1];
             const long long ncv = (long long)hn.n * hn.K;
             e.off_cyc = off; off += al(nvec + 2 * ncv);
-            const long long segtot = (long long)h.ncol * h.sxe * h.ste * h.K;
-            e.off_sap = off; off += al(nvec + (long long)(p.sap_gmres_m + 4) * segtot);
-            e.sm_sap = sm; sm += gm_state_bytes(h.ncol, p.sap_gmres_m, sizeof(T));
-            if (h.ncol > kEngineThreads)
-                return fail(AMG_ERR_UNSUPPORTED, "level %d: %d SAP blocks per colour exceed %d", l, h.ncol, kEngineThreads);
+            const long long seglen = (long long)h.sxe * h.ste * h.K;
+            e.off_sap = off; off += al(nvec + (long long)h.ncol * seglen);
+            e.sap_nteam = seglen <= 1024 ? 4 : 1;
+            e.sap_vec_smem = 0;
+            e.off_sapteam = off; off += al((long long)e.sap_nteam * (p.sap_gmres_m + 4) * seglen);
         }
     }
+    // whole-CTA reduction scratch and the team area of the SAP block solves
+    auto al16 = [](int v) { return (v + 15) & ~15; };
+    sm = al16(sm);
+    a.smem_red = sm;
+    sm += al16(2 * 2 * (kEngineThreads / 32) * (int)sizeof(T));
+    a.smem_team = sm;
+    const int tb_state = al16(gm_state_bytes(1, p.sap_gmres_m, sizeof(T)) + 64 * (int)sizeof(T));
+    int tb = tb_state;
+    for (int l = 1; l < c->L; l++) {
+        const LevelHost& h = c->lv[l];
+        if (h.coarsest) continue;
+        EngLevel<T>& e = a.lv[l];
+        const int seglen = h.sxe * h.ste * h.K;
+        const int with_vec = al16(tb_state + (p.sap_gmres_m + 4) * seglen * (int)sizeof(cx<T>));
+        if (sm + e.sap_nteam * std::max(tb, with_vec) <= 200 * 1024) {
+            e.sap_vec_smem = 1;
+            tb = std::max(tb, with_vec);
+        }
+    }
+    a.team_bytes = tb;
+    sm += 4 * tb;
     long long io = 2;
     for (int l = 1; l < c->L; l++) io = std::max<long long>(io, (long long)c->lv[l].n * c->lv[l].K);
     a.off_io = off;
     a.io_len = al(io);
     off += 2 * a.io_len;
-    a.smem_red = sm;
-    sm += 2 * (kEngineThreads / 32) * (int)sizeof(T) + 64;
-    if (sm > 200 * 1024) return fail(AMG_ERR_UNSUPPORTED, "engine scalar state needs %d bytes of shared memory", sm);
+    sm += 64;
+    if (sm > 227 * 1024) return fail(AMG_ERR_UNSUPPORTED, "engine shared memory needs %d bytes", sm);
     ps.eng_smem = sm;
     a.slab = std::max<long long>(off, 2);
     ps.eng_cap = std::max(nsrc, 1);

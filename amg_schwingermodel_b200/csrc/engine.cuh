@@ -43,6 +43,9 @@ struct EngLevel {
     // Level::gmres_l knobs of this level (LevelV::GMRES_*, include/params.h:51-53, 63-65)
     int gm_m, gm_restarts;
     T gm_tol;
+    // SAP block solves: teams per CTA, and whether a team's block vectors fit in shared memory
+    int sap_nteam, sap_vec_smem;
+    long long off_sapteam;      // slab offset of the team block vectors when not in shared memory
 };
 
 template <typename T>
@@ -64,7 +67,9 @@ struct EngArgs {
     EngParams<T> p;
     cx<T>* work;                 // per-source slabs
     long long slab;              // elements per slab
-    int smem_red;                // byte offset of the reduction scratch
+    int smem_red;                // byte offset of the whole-CTA reduction scratch (2*2*16 reals)
+    int smem_team;               // byte offset of the team area (SAP block solves)
+    int team_bytes;              // bytes per team in that area
     long long off_io;            // slab offset of the entry op's input / output copies
     long long io_len;            // elements of each copy
     int* status;                 // [nsrc] per-source result code / iteration count
@@ -122,65 +127,6 @@ __device__ inline GmState<T> gm_state_at(char* base, int nseg, int m) {
     s.arn = i; i += nseg;
     s.iters = i;
     return s;
-}
-
-// ---------------------------------------------------------------------------------
-// segmented vector space: nseg segments of seglen complex entries, contiguous
-// ---------------------------------------------------------------------------------
-template <typename T>
-struct Seg {
-    int nseg, seglen, tps;       // threads per segment (power of two)
-    T* red;                      // shared scratch [2 * blockDim.x / 32]
-};
-
-template <typename T>
-__device__ inline Seg<T> make_seg(int nseg, int seglen, T* red) {
-    Seg<T> s;
-    s.nseg = nseg; s.seglen = seglen; s.red = red;
-    int tps = blockDim.x / nseg;
-    int p = 1;
-    while (p * 2 <= tps) p *= 2;
-    s.tps = p;
-    return s;
-}
-
-// res[s] = sum_e a[e] * conj(b[e]) over segment s (the reference's dot, include/lin_alg_op.h:32-40)
-template <typename T>
-__device__ void seg_dot(const Seg<T>& sp, const cx<T>* a, const cx<T>* b, cx<T>* res) {
-    const int tid = threadIdx.x;
-    const int grp = tid / sp.tps, q = tid % sp.tps;
-    T ax = 0, ay = 0;
-    if (grp < sp.nseg) {
-        const cx<T>* pa = a + (long long)grp * sp.seglen;
-        const cx<T>* pb = b + (long long)grp * sp.seglen;
-        for (int e = q; e < sp.seglen; e += sp.tps) {
-            cx<T> u = pa[e], v = pb[e];
-            ax += u.x * v.x + u.y * v.y;
-            ay += u.y * v.x - u.x * v.y;
-        }
-    }
-    const int w = (sp.tps < 32) ? sp.tps : 32;
-    for (int o = w / 2; o > 0; o >>= 1) {
-        ax += __shfl_xor_sync(0xffffffffu, ax, o);
-        ay += __shfl_xor_sync(0xffffffffu, ay, o);
-    }
-    if (sp.tps <= 32) {
-        __syncthreads();
-        if (grp < sp.nseg && q == 0) res[grp] = mk<T>(ax, ay);
-        __syncthreads();
-        return;
-    }
-    const int lane = tid & 31, wid = tid >> 5;
-    __syncthreads();
-    if (lane == 0) { sp.red[2 * wid] = ax; sp.red[2 * wid + 1] = ay; }
-    __syncthreads();
-    if (grp < sp.nseg && q == 0) {
-        const int wpg = sp.tps / 32;
-        T sx = 0, sy = 0;
-        for (int k = 0; k < wpg; k++) { sx += sp.red[2 * (grp * wpg + k)]; sy += sp.red[2 * (grp * wpg + k) + 1]; }
-        res[grp] = mk<T>(sx, sy);
-    }
-    __syncthreads();
 }
 
 // ---------------------------------------------------------------------------------
@@ -273,6 +219,7 @@ __device__ __forceinline__ void part_store(const Eng<T>& E, cx<T>* out, int e, c
 template <typename T>
 __device__ __forceinline__ void part_begin(const Eng<T>& E) {
     if (E.csize > 1) cluster_barrier();
+    else __syncthreads();
 }
 template <typename T>
 __device__ __forceinline__ void part_end(const Eng<T>& E) {
@@ -434,207 +381,285 @@ __device__ __noinline__ void prolong_v(const Eng<T>& E, const EngLevel<T>& L, co
 }
 
 // ---------------------------------------------------------------------------------
-// FGMRES (src/fgmres.cpp:5-115) for nseg independent segments, x0 = b (the only start the
-// multigrid uses below the fine level: src/amg.cpp:138, :161, src/sap.cpp:61).
-// op(in, out) applies the operator to all segments; pre(j) fills Z_j from V_j (Z may
-// alias V for the identity preconditioner).  Per segment it follows the reference:
-// modified Gram-Schmidt, Givens rotations, Arnoldi exit on |g_{j+1}| < tol*||b||, a true
-// residual after each cycle, and maxIt carried over restart cycles.
-// Returns in st.iters[s] the reference's return value (k*m + maxIt or restarts*m).
+// Teams: a whole CTA (hardware barrier 0) or a slice of it with its own named barrier.
+// ---------------------------------------------------------------------------------
+struct Team {
+    int tid, size, nw, bar;     // thread index in the team, threads, warps, barrier id
+};
+__device__ __forceinline__ Team whole_cta() { return Team{(int)threadIdx.x, (int)blockDim.x, (int)(blockDim.x >> 5), 0}; }
+__device__ __forceinline__ void team_sync(const Team& tm) {
+    if (tm.bar == 0) __syncthreads();
+    else asm volatile("bar.sync %0, %1;" ::"r"(tm.bar), "r"(tm.size) : "memory");
+}
+// Sum of (ax, ay) over the team; every thread receives it.  `part` holds 2*2*nw reals used as
+// two alternating buffers, so one barrier per reduction suffices.
+template <typename T>
+__device__ __forceinline__ cx<T> team_sum2(const Team& tm, T* part, int& buf, T ax, T ay) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        ax += __shfl_xor_sync(0xffffffffu, ax, o);
+        ay += __shfl_xor_sync(0xffffffffu, ay, o);
+    }
+    if (tm.nw == 1) return mk<T>(ax, ay);
+    T* pb = part + buf * tm.nw * 2;
+    const int lane = tm.tid & 31, wid = tm.tid >> 5;
+    if (lane == 0) { pb[2 * wid] = ax; pb[2 * wid + 1] = ay; }
+    team_sync(tm);
+    T sx = 0, sy = 0;
+    for (int k = 0; k < tm.nw; k++) { sx += pb[2 * k]; sy += pb[2 * k + 1]; }
+    buf ^= 1;
+    return mk<T>(sx, sy);
+}
+
+// ---------------------------------------------------------------------------------
+// FGMRES (src/fgmres.cpp:5-115) of one team on one vector of n entries with x0 = b (the
+// only start the multigrid uses below the fine level: src/amg.cpp:138, :161,
+// src/sap.cpp:61).  op(in, out) and pre(j, V_j, Z_j) are collective operations that start by
+// synchronising (so earlier writes to their input are visible) and end synchronised;
+// between them every thread only touches its own entries e = tid, tid + size, ...  The
+// arithmetic is the reference's: modified Gram-Schmidt, Givens rotations, Arnoldi exit on
+// |g_{j+1}| < tol*||b||, a true residual after each cycle, and maxIt carried over restart
+// cycles.  Z may alias V (identity preconditioner).  Returns k*m + maxIt or restarts*m.
 // ---------------------------------------------------------------------------------
 template <typename T, class Op, class Pre>
-__device__ void seg_fgmres(const Eng<T>* E, int cnt_level, int cnt_what, const Seg<T>& sp, Op& op, Pre& pre,
-                           const cx<T>* b, cx<T>* x, cx<T>* V, cx<T>* Z, cx<T>* w, const GmState<T>& st, int m,
-                           int restarts, T tol) {
-    const int nseg = sp.nseg, seglen = sp.seglen, tot = nseg * seglen;
-    const long long vstride = tot;
-    const int tid = threadIdx.x;
-    // setZeros (include/fgmres.h:93-120): H, g, V, Z are zero at the start of every call
-    for (int e = tid; e < nseg * (m + 1) * m; e += blockDim.x) st.H[e] = czero<T>();
-    for (int e = tid; e < nseg * (m + 1); e += blockDim.x) st.g[e] = czero<T>();
-    for (int e = tid; e < nseg * m; e += blockDim.x) { st.cn[e] = czero<T>(); st.sn[e] = czero<T>(); st.eta[e] = czero<T>(); }
-    for (long long e = tid; e < (long long)(m + 1) * vstride; e += blockDim.x) V[e] = czero<T>();
+__device__ int team_fgmres(const Team& tm, T* part, const Eng<T>* E, int cnt_level, int cnt_what, Op& op, Pre& pre,
+                           const cx<T>* b, cx<T>* x, cx<T>* V, cx<T>* Z, cx<T>* w, const GmState<T>& st, int n,
+                           int m, int restarts, T tol) {
+    int buf = 0;
+    const int tid = tm.tid, ts = tm.size;
+    // setZeros (include/fgmres.h:93-120)
+    for (long long e = tid; e < (long long)(m + 1) * n; e += ts) V[e] = czero<T>();
     if (Z != V)
-        for (long long e = tid; e < (long long)m * vstride; e += blockDim.x) Z[e] = czero<T>();
-    // x = x0 = b; r = b - A x into V0
-    for (int e = tid; e < tot; e += blockDim.x) x[e] = b[e];
-    __syncthreads();
-    op(x, w);
-    for (int e = tid; e < tot; e += blockDim.x) V[e] = b[e] - w[e];
-    __syncthreads();
-    seg_dot(sp, V, V, st.red);
-    for (int s = tid; s < nseg; s += blockDim.x) {
-        st.err[s] = sqrt(st.red[s].x);
-        st.maxit[s] = m;
-        st.act[s] = 1;
-        st.iters[s] = restarts * m;
+        for (long long e = tid; e < (long long)m * n; e += ts) Z[e] = czero<T>();
+    if (tid == 0) {
+        for (int q = 0; q < (m + 1) * m; q++) st.H[q] = czero<T>();
+        for (int q = 0; q <= m; q++) st.g[q] = czero<T>();
+        for (int q = 0; q < m; q++) { st.cn[q] = czero<T>(); st.sn[q] = czero<T>(); st.eta[q] = czero<T>(); }
     }
-    __syncthreads();
-    seg_dot(sp, b, b, st.red);
-    for (int s = tid; s < nseg; s += blockDim.x) st.normb[s] = sqrt(st.red[s].x);
-    __syncthreads();
-
+    for (int e = tid; e < n; e += ts) x[e] = b[e];
+    op(x, w);
+    T rr = 0, bb = 0;
+    for (int e = tid; e < n; e += ts) {
+        const cx<T> r = b[e] - w[e];
+        V[e] = r;
+        rr += cnorm2(r);
+        bb += cnorm2(b[e]);
+    }
+    cx<T> s2 = team_sum2(tm, part, buf, rr, bb);
+    T err = sqrt(s2.x);
+    const T normb = sqrt(s2.y);
+    int maxit = m, ret = restarts * m;
     for (int k = 0; k < restarts; k++) {
-        int any = 0;
-        for (int s = 0; s < nseg; s++) any |= st.act[s];
-        if (!any) break;
-        // V0 = r / beta, g0 = beta
-        for (int s = tid; s < nseg; s += blockDim.x) {
-            st.arn[s] = st.act[s];
-            if (st.act[s]) st.g[s * (m + 1)] = mk<T>(st.err[s], T(0));
+        {
+            const T inv = T(1) / err;
+            for (int e = tid; e < n; e += ts) V[e] = inv * V[e];
         }
-        for (int e = tid; e < tot; e += blockDim.x) {
-            const int s = e / seglen;
-            if (st.act[s]) { T inv = T(1) / st.err[s]; V[e] = inv * V[e]; }
-        }
-        __syncthreads();
+        if (tid == 0) st.g[0] = mk<T>(err, T(0));
         for (int j = 0; j < m; j++) {
-            int anyarn = 0;
-            for (int s = 0; s < nseg; s++) anyarn |= st.arn[s];
-            if (!anyarn) break;
             if (E) eng_count(*E, cnt_level, cnt_what);
-            cx<T>* Vj = V + (long long)j * vstride;
-            cx<T>* Zj = (Z == V) ? Vj : Z + (long long)j * vstride;
-            pre(j, Vj, Zj, st.arn);
+            cx<T>* Vj = V + (long long)j * n;
+            cx<T>* Zj = (Z == V) ? Vj : Z + (long long)j * n;
+            pre(j, Vj, Zj);
             op(Zj, w);
             for (int i = 0; i <= j; i++) {
-                const cx<T>* Vi = V + (long long)i * vstride;
-                seg_dot(sp, w, Vi, st.red);
-                for (int s = tid; s < nseg; s += blockDim.x)
-                    if (st.arn[s]) st.H[s * (m + 1) * m + i * m + j] = st.red[s];
-                for (int e = tid; e < tot; e += blockDim.x) {
-                    const int s = e / seglen;
-                    if (st.arn[s]) { cx<T> h = st.red[s]; cx<T> vv = Vi[e]; cx<T> ww = w[e]; cfma(ww, -h, vv); w[e] = ww; }
+                const cx<T>* Vi = V + (long long)i * n;
+                T ax = 0, ay = 0;
+                for (int e = tid; e < n; e += ts) {
+                    const cx<T> u = w[e], vv = Vi[e];
+                    ax += u.x * vv.x + u.y * vv.y;
+                    ay += u.y * vv.x - u.x * vv.y;
                 }
-                __syncthreads();
+                const cx<T> h = team_sum2(tm, part, buf, ax, ay);
+                if (tid == 0) st.H[i * m + j] = h;
+                for (int e = tid; e < n; e += ts) {
+                    cx<T> ww = w[e];
+                    cfma(ww, -h, Vi[e]);
+                    w[e] = ww;
+                }
             }
-            seg_dot(sp, w, w, st.red);
-            for (int e = tid; e < tot; e += blockDim.x) {
-                const int s = e / seglen;
-                const T h = sqrt(st.red[s].x);
-                if (st.arn[s] && h > T(0)) { T inv = T(1) / h; V[(long long)(j + 1) * vstride + e] = inv * w[e]; }
+            T nn = 0;
+            for (int e = tid; e < n; e += ts) nn += cnorm2(w[e]);
+            const T hn = sqrt(team_sum2(tm, part, buf, nn, T(0)).x);
+            if (hn > T(0)) {
+                const T inv = T(1) / hn;
+                cx<T>* Vn = V + (long long)(j + 1) * n;
+                for (int e = tid; e < n; e += ts) Vn[e] = inv * w[e];
             }
-            __syncthreads();
-            // rotation(j) (src/fgmres.cpp:90-104) and the g update, one thread per segment
-            for (int s = tid; s < nseg; s += blockDim.x) {
-                if (!st.arn[s]) continue;
-                cx<T>* H = st.H + s * (m + 1) * m;
-                cx<T>* cn = st.cn + s * m;
-                cx<T>* sn = st.sn + s * m;
-                cx<T>* g = st.g + s * (m + 1);
-                H[(j + 1) * m + j] = mk<T>(sqrt(st.red[s].x), T(0));
+            // rotation(j) (src/fgmres.cpp:90-104) by the team's first thread
+            if (tid == 0) {
+                cx<T>* H = st.H;
+                H[(j + 1) * m + j] = mk<T>(hn, T(0));
                 for (int i = 0; i < j; i++) {
-                    cx<T> hij = H[i * m + j], hi1 = H[(i + 1) * m + j];
-                    cx<T> temp = cmulc(cn[i], hij) + cmulc(sn[i], hi1);
-                    H[(i + 1) * m + j] = cmul(cn[i], hi1) - cmul(sn[i], hij);
+                    const cx<T> hij = H[i * m + j], hi1 = H[(i + 1) * m + j];
+                    const cx<T> temp = cmulc(st.cn[i], hij) + cmulc(st.sn[i], hi1);
+                    H[(i + 1) * m + j] = cmul(st.cn[i], hi1) - cmul(st.sn[i], hij);
                     H[i * m + j] = temp;
                 }
-                cx<T> hjj = H[j * m + j], hj1 = H[(j + 1) * m + j];
+                const cx<T> hjj = H[j * m + j], hj1 = H[(j + 1) * m + j];
                 const T den = sqrt(cnorm2(hjj) + cnorm2(hj1));
-                sn[j] = mk<T>(hj1.x / den, hj1.y / den);
-                cn[j] = mk<T>(hjj.x / den, hjj.y / den);
-                H[j * m + j] = cmulc(cn[j], hjj) + cmulc(sn[j], hj1);
+                st.sn[j] = mk<T>(hj1.x / den, hj1.y / den);
+                st.cn[j] = mk<T>(hjj.x / den, hjj.y / den);
+                H[j * m + j] = cmulc(st.cn[j], hjj) + cmulc(st.sn[j], hj1);
                 H[(j + 1) * m + j] = czero<T>();
-                cx<T> gj = g[j];
-                g[j + 1] = -cmul(sn[j], gj);
-                g[j] = cmulc(cn[j], gj);
-                const cx<T> gj1 = g[j + 1];
-                if (sqrt(cnorm2(gj1)) < tol * st.normb[s]) {
-                    st.maxit[s] = j + 1;
-                    st.arn[s] = 0;
-                }
+                const cx<T> gj = st.g[j];
+                st.g[j + 1] = -cmul(st.sn[j], gj);
+                st.g[j] = cmulc(st.cn[j], gj);
+                st.arn[0] = (sqrt(cnorm2(st.g[j + 1])) < tol * normb) ? 0 : 1;
             }
-            __syncthreads();
+            team_sync(tm);
+            if (st.arn[0] == 0) {
+                maxit = j + 1;
+                break;
+            }
         }
         // solve_upper_triangular (src/fgmres.cpp:107-115)
-        for (int s = tid; s < nseg; s += blockDim.x) {
-            if (!st.act[s]) continue;
-            const cx<T>* H = st.H + s * (m + 1) * m;
-            const cx<T>* g = st.g + s * (m + 1);
-            cx<T>* eta = st.eta + s * m;
-            const int n = st.maxit[s];
-            for (int i = n - 1; i >= 0; i--) {
-                cx<T> o = g[i];
-                for (int jj = i + 1; jj < n; jj++) o -= cmul(H[i * m + jj], eta[jj]);
-                eta[i] = cdiv(o, H[i * m + i]);
+        if (tid == 0) {
+            for (int i = maxit - 1; i >= 0; i--) {
+                cx<T> o = st.g[i];
+                for (int jj = i + 1; jj < maxit; jj++) o -= cmul(st.H[i * m + jj], st.eta[jj]);
+                st.eta[i] = cdiv(o, st.H[i * m + i]);
             }
         }
-        __syncthreads();
-        // x += sum_j eta_j Z_j
-        for (int e = tid; e < tot; e += blockDim.x) {
-            const int s = e / seglen;
-            if (!st.act[s]) continue;
-            const cx<T>* eta = st.eta + s * m;
+        team_sync(tm);
+        for (int e = tid; e < n; e += ts) {
             cx<T> acc = x[e];
-            const int n = st.maxit[s];
-            for (int jj = 0; jj < n; jj++) {
-                const cx<T>* Zj = (Z == V) ? V + (long long)jj * vstride : Z + (long long)jj * vstride;
-                cfma(acc, eta[jj], Zj[e]);
+            for (int jj = 0; jj < maxit; jj++) {
+                const cx<T>* Zq = (Z == V) ? V + (long long)jj * n : Z + (long long)jj * n;
+                cfma(acc, st.eta[jj], Zq[e]);
             }
             x[e] = acc;
         }
-        __syncthreads();
         // true residual into V0
         op(x, w);
-        for (int e = tid; e < tot; e += blockDim.x) {
-            const int s = e / seglen;
-            if (st.act[s]) V[e] = b[e] - w[e];
+        rr = 0;
+        for (int e = tid; e < n; e += ts) {
+            const cx<T> r = b[e] - w[e];
+            V[e] = r;
+            rr += cnorm2(r);
         }
-        __syncthreads();
-        seg_dot(sp, V, V, st.red);
-        for (int s = tid; s < nseg; s += blockDim.x) {
-            if (!st.act[s]) continue;
-            st.err[s] = sqrt(st.red[s].x);
-            if (st.err[s] < tol * st.normb[s]) {
-                st.iters[s] = k * m + st.maxit[s];
-                st.act[s] = 0;
+        err = sqrt(team_sum2(tm, part, buf, rr, T(0)).x);
+        if (err < tol * normb) {
+            ret = k * m + maxit;
+            break;
+        }
+    }
+    return ret;
+}
+
+// SAP_level_l::D_local (src/level.cpp:304-368) for one block, by one team: out[m][i] for the
+// block's sites m (local order) from in[m][j]; neighbours outside the block are dropped.
+template <typename T>
+__device__ void dlocal_block(const Team& tm, const EngLevel<T>& L, T m0, int block, const cx<T>* in, cx<T>* out) {
+    const int K = L.K, spb = L.sxe * L.ste, n = spb * K;
+    const T mass = m0 + T(2);
+    const int bxi = block / L.sbt, bti = block - bxi * L.sbt;
+    for (int e = tm.tid; e < n; e += tm.size) {
+        const int m = e / K, i = e - m * K;
+        const int mx = m / L.ste, mt = m - mx * L.ste;
+        const int x = bxi * L.sxe + mx, t = bti * L.ste + mt;
+        const int xs = x * L.nt + t;
+        const cx<T>* lk = L.links + (long long)xs * 5 * K * K + i;
+        cx<T> acc = czero<T>();
+#pragma unroll 1
+        for (int h = 0; h < 5; h++) {
+            int nx_ = x, nt_ = t;
+            switch (h) {
+                case HOP_R0: nt_ = (t + 1 == L.nt) ? 0 : t + 1; break;
+                case HOP_R1: nx_ = (x + 1 == L.nx) ? 0 : x + 1; break;
+                case HOP_L0: nt_ = (t == 0) ? L.nt - 1 : t - 1; break;
+                case HOP_L1: nx_ = (x == 0) ? L.nx - 1 : x - 1; break;
+                default: break;
             }
+            const int nbx = nx_ / L.sxe, nbt = nt_ / L.ste;
+            if (nbx * L.sbt + nbt != block) continue;
+            const int ml = (nx_ - nbx * L.sxe) * L.ste + (nt_ - nbt * L.ste);
+            const cx<T>* v = in + (long long)ml * K;
+            const cx<T>* a = lk + (long long)h * K * K;
+            cx<T> s = czero<T>();
+            for (int j = 0; j < K; j++) cfma(s, a[(long long)j * K], v[j]);
+            if (hop_sign(t, L.nt, h) < 0) acc -= s; else acc += s;
         }
-        __syncthreads();
+        out[e] = mass * in[e] - acc;
     }
 }
 
-
-
-// SAP_C::SAP (src/sap.cpp:64-174) on coarse level l: nu red/black sweeps of block GMRES,
-// every block of a colour solved; returns 1 if ||v - D x|| < sap_tol * ||v||.
+// SAP_C::SAP (src/sap.cpp:64-174) on coarse level l: nu red/black sweeps; the blocks of a
+// colour are spread over the teams of every CTA of the cluster (first one per CTA), each
+// team runs the block GMRES with its vectors in its own shared-memory area, the block
+// solutions are broadcast to every CTA, and the residual update is shared.  Returns 1 if
+// ||v - D x|| < sap_tol * ||v||.
 template <typename T>
 __device__ __noinline__ int eng_sap(const Eng<T>& E, int l, const cx<T>* v, cx<T>* x, int nu) {
     const EngLevel<T>& L = E.L(l);
     const EngParams<T>& p = E.a->p;
     const int nvec = L.n * L.K;
-    const int spb = L.sxe * L.ste, seglen = spb * L.K, nseg = L.ncol, segtot = nseg * seglen;
+    const int spb = L.sxe * L.ste, seglen = spb * L.K, ncol = L.ncol, m = p.sap_m;
     cx<T>* r = E.work(L.off_sap);
-    cx<T>* bseg = r + nvec;
-    cx<T>* xseg = bseg + segtot;
-    cx<T>* wseg = xseg + segtot;
-    cx<T>* Vseg = wseg + segtot;
-    GmState<T> st = gm_state_at<T>(E.smem + L.sm_sap, nseg, p.sap_m);
-    Seg<T> sp1 = make_seg<T>(1, nvec, E.red);
-    Seg<T> sps = make_seg<T>(nseg, seglen, E.red);
+    cx<T>* xall = r + nvec;                                   // [ncol][seglen]
+    const Team cta = whole_cta();
+    T* cpart = E.red;
+    int cbuf = 0;
+    const int nteam = L.sap_nteam, tsize = blockDim.x / nteam, team = threadIdx.x / tsize;
+    const Team tm{(int)threadIdx.x - team * tsize, tsize, tsize >> 5, team + 1};
+    char* tsm = E.smem + E.a->smem_team + team * E.a->team_bytes;
+    const GmState<T> st = gm_state_at<T>(tsm, 1, m);
+    T* tpart = reinterpret_cast<T*>(tsm + gm_state_bytes(1, m, sizeof(T)));
+    cx<T>* tv = L.sap_vec_smem ? reinterpret_cast<cx<T>*>(tsm + gm_state_bytes(1, m, sizeof(T)) + 64 * sizeof(T))
+                               : E.work(L.off_sapteam) + (long long)team * (m + 4) * seglen;
+    cx<T>* bv = tv;
+    cx<T>* xv = bv + seglen;
+    cx<T>* wv = xv + seglen;
+    cx<T>* Vv = wv + seglen;
 
     eng_count(E, l, CNT_SAP_CALL);
-    seg_dot(sp1, v, v, st.red);
-    const T vnorm = sqrt(st.red[0].x);
+    T vv = 0;
+    for (int e = threadIdx.x; e < nvec; e += blockDim.x) vv += cnorm2(v[e]);
+    const T vnorm = sqrt(team_sum2(cta, cpart, cbuf, vv, T(0)).x);
     dc_apply(E, L, p.m0, x, r);
-    v_sub<T>(r, v, r, nvec);
-        for (int it = 0; it < nu; it++) {
+    for (int e = threadIdx.x; e < nvec; e += blockDim.x) r[e] = v[e] - r[e];
+    const int nslot = E.csize * nteam, slot = team * E.csize + E.crank;
+    for (int it = 0; it < nu; it++) {
         for (int colour = 0; colour < 2; colour++) {
             const int* blocks = colour == 0 ? L.red : L.black;
-            sap_gather(L, blocks, nseg, r, bseg);
-            auto lop = [&](const cx<T>* in, cx<T>* out) { dlocal_apply(E, L, p.m0, blocks, nseg, in, out); };
-            auto ident = [](int, const cx<T>*, cx<T>*, const int*) {};
-            seg_fgmres(&E, l, CNT_SAP_STEP, sps, lop, ident, bseg, xseg, Vseg, Vseg, wseg, st, p.sap_m, p.sap_restarts,
-                       p.sap_gmres_tol);
-            sap_scatter_add(L, blocks, nseg, xseg, x);
+            __syncthreads();                                  // r complete before the gathers
+            for (int bi = slot; bi < ncol; bi += nslot) {
+                const int block = blocks[bi];
+                const int bxi = block / L.sbt, bti = block - bxi * L.sbt;
+                for (int e = tm.tid; e < seglen; e += tm.size) {
+                    const int mm = e / L.K, i = e - mm * L.K;
+                    const int mx = mm / L.ste, mt = mm - mx * L.ste;
+                    bv[e] = r[(long long)((bxi * L.sxe + mx) * L.nt + bti * L.ste + mt) * L.K + i];
+                }
+                auto lop = [&](const cx<T>* in, cx<T>* out) {
+                    team_sync(tm);
+                    dlocal_block(tm, L, p.m0, block, in, out);
+                    team_sync(tm);
+                };
+                auto ident = [](int, const cx<T>*, cx<T>*) {};
+                team_fgmres(tm, tpart, &E, l, CNT_SAP_STEP, lop, ident, bv, xv, Vv, Vv, wv, st, seglen, m,
+                            p.sap_restarts, p.sap_gmres_tol);
+                // broadcast the block solution to every CTA of the cluster
+                for (int e = tm.tid; e < seglen; e += tm.size) part_store(E, xall + (long long)bi * seglen, e, xv[e]);
+                team_sync(tm);
+            }
+            if (E.csize > 1) cluster_barrier(); else __syncthreads();
+            // x += solutions of this colour (every CTA, its own copy)
+            for (int e = threadIdx.x; e < ncol * seglen; e += blockDim.x) {
+                const int s = e / seglen, q = e - s * seglen, mm = q / L.K, i = q - mm * L.K;
+                const int block = blocks[s];
+                const int bxi = block / L.sbt, bti = block - bxi * L.sbt;
+                const int mx = mm / L.ste, mt = mm - mx * L.ste;
+                x[(long long)((bxi * L.sxe + mx) * L.nt + bti * L.ste + mt) * L.K + i] += xall[e];
+            }
             dc_apply(E, L, p.m0, x, r);
-            v_sub<T>(r, v, r, nvec);
+            for (int e = threadIdx.x; e < nvec; e += blockDim.x) r[e] = v[e] - r[e];
         }
-        seg_dot(sp1, r, r, st.red);
-        const T err = sqrt(st.red[0].x);
-        __syncthreads();
+        T rr = 0;
+        for (int e = threadIdx.x; e < nvec; e += blockDim.x) rr += cnorm2(r[e]);
+        const T err = sqrt(team_sum2(cta, cpart, cbuf, rr, T(0)).x);
         if (err < p.sap_tol * vnorm) return 1;
     }
+    __syncthreads();
     return 0;
 }
 
@@ -647,12 +672,14 @@ __device__ __noinline__ int eng_coarse_gmres(const Eng<T>& E, int l, const cx<T>
     const int nvec = L.n * L.K;
     cx<T>* V = E.work(L.off_cg);
     cx<T>* w = V + (long long)(L.gm_m + 1) * nvec;
-    GmState<T> st = gm_state_at<T>(E.smem + L.sm_cg, 1, L.gm_m);
-    Seg<T> sp = make_seg<T>(1, nvec, E.red);
+    const GmState<T> st = gm_state_at<T>(E.smem + L.sm_cg, 1, L.gm_m);
+    const Team cta = whole_cta();
     auto op = [&](const cx<T>* in, cx<T>* out) { dc_apply(E, L, p.m0, in, out); };
-    auto ident = [](int, const cx<T>*, cx<T>*, const int*) {};
-    seg_fgmres(&E, l, CNT_GMRES_STEP, sp, op, ident, b, x, V, V, w, st, L.gm_m, L.gm_restarts, L.gm_tol);
-    return st.iters[0];
+    auto ident = [](int, const cx<T>*, cx<T>*) {};
+    const int it = team_fgmres(cta, E.red, &E, l, CNT_GMRES_STEP, op, ident, b, x, V, V, w, st, nvec, L.gm_m,
+                               L.gm_restarts, L.gm_tol);
+    __syncthreads();
+    return it;
 }
 
 template <typename T, int D> struct Cycles;
@@ -712,12 +739,14 @@ struct Cycles {
         cx<T>* V = E.work(L.off_kfg);
         cx<T>* Z = V + (long long)(p.k_m + 1) * nvec;
         cx<T>* w = Z + (long long)p.k_m * nvec;
-        GmState<T> st = gm_state_at<T>(E.smem + L.sm_kfg, 1, p.k_m);
-        Seg<T> sp = make_seg<T>(1, nvec, E.red);
+        const GmState<T> st = gm_state_at<T>(E.smem + L.sm_kfg, 1, p.k_m);
+        const Team cta = whole_cta();
         auto op = [&](const cx<T>* in, cx<T>* out) { dc_apply(E, L, p.m0, in, out); };
-        auto pre = [&](int, const cx<T>* v, cx<T>* z, const int*) { Cycles<T, D>::kcycle(E, l, v, z); };
-        seg_fgmres(&E, l, CNT_KFG_STEP, sp, op, pre, b, x, V, Z, w, st, p.k_m, p.k_restarts, p.k_tol);
-        return st.iters[0];
+        auto pre = [&](int, const cx<T>* v, cx<T>* z) { Cycles<T, D>::kcycle(E, l, v, z); };
+        const int it = team_fgmres(cta, E.red, &E, l, CNT_KFG_STEP, op, pre, b, x, V, Z, w, st, nvec, p.k_m,
+                                   p.k_restarts, p.k_tol);
+        __syncthreads();
+        return it;
     }
 };
 

@@ -270,10 +270,15 @@ __global__ void __launch_bounds__(256) k_sap0_blocks(const cx<T>* __restrict__ U
     }
     __syncthreads();
     B.u = u;
-    Seg<T> sp = make_seg<T>(1, len, red);
-    auto op = [&](const cx<T>* in, cx<T>* out) { fine_block_apply(B, in, out); };
-    auto ident = [](int, const cx<T>*, cx<T>*, const int*) {};
-    seg_fgmres<T>(nullptr, 0, 0, sp, op, ident, b, xs, V, V, w, st, m, restarts, tol);
+    const Team cta = whole_cta();
+    auto op = [&](const cx<T>* in, cx<T>* out) {
+        __syncthreads();
+        fine_block_apply(B, in, out);
+    };
+    auto ident = [](int, const cx<T>*, cx<T>*) {};
+    const int it = team_fgmres<T>(cta, red, (const Eng<T>*)nullptr, 0, 0, op, ident, b, xs, V, V, w, st, len, m,
+                                  restarts, tol);
+    __syncthreads();
     cx<T>* xx = x + (long long)rhs * N * 2;
     for (int q = threadIdx.x; q < S; q += blockDim.x) {
         const int mx = q / ste, mt = q - mx * ste;
@@ -281,7 +286,7 @@ __global__ void __launch_bounds__(256) k_sap0_blocks(const cx<T>* __restrict__ U
         xx[2 * n] += xs[2 * q];
         xx[2 * n + 1] += xs[2 * q + 1];
     }
-    if (iters_out && threadIdx.x == 0) iters_out[rhs * gridDim.x + seg] = st.iters[0];
+    if (iters_out && threadIdx.x == 0) iters_out[rhs * gridDim.x + seg] = it;
 }
 
 // ---------------------------------------------------------------------------------
