@@ -227,6 +227,20 @@ __device__ __forceinline__ void part_end(const Eng<T>& E) {
     else __syncthreads();
 }
 
+// Threads cooperating on one output row of a dense coarse operator: every row's K columns
+// are split over TPR consecutive lanes so each thread keeps several independent L2 loads in
+// flight; the partial sums are combined with shuffles.
+constexpr int kTPR = 8;
+template <typename T>
+__device__ __forceinline__ cx<T> tpr_sum(cx<T> a) {
+#pragma unroll
+    for (int o = kTPR / 2; o > 0; o >>= 1) {
+        a.x += __shfl_xor_sync(0xffffffffu, a.x, o);
+        a.y += __shfl_xor_sync(0xffffffffu, a.y, o);
+    }
+    return a;
+}
+
 // Level::D_operator (src/level.cpp:161-180) for l >= 1:
 // out = (m0+2) in - sum_hop sign * G_hop in(neighbour).  With a cluster, every CTA computes
 // a slice of the rows and stores it into every CTA's copy of `out`.
@@ -238,22 +252,28 @@ __device__ __noinline__ void dc_apply(const Eng<T>& E, const EngLevel<T>& L, T m
     eng_count(E, L.level, CNT_APPLY);
     part_range(E, tot, e0, e1);
     part_begin(E);
-    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
-        const int xs = e / K, i = e - xs * K;
-        const int x = xs / L.nt, t = xs - x * L.nt;
+    const int g = threadIdx.x % kTPR, rows_per_pass = blockDim.x / kTPR;
+    for (int rb = e0; rb < e1; rb += rows_per_pass) {
+        const int e = rb + threadIdx.x / kTPR;
+        const bool on = e < e1;
         cx<T> acc = czero<T>();
-        const cx<T>* lk = L.links + (long long)xs * 5 * K * K + i;
+        if (on) {
+            const int xs = e / K, i = e - xs * K;
+            const int x = xs / L.nt, t = xs - x * L.nt;
+            const cx<T>* lk = L.links + (long long)xs * 5 * K * K + i;
 #pragma unroll 1
-        for (int h = 0; h < 5; h++) {
-            const int nbs = nb_site(x, t, L.nx, L.nt, h);
-            const cx<T>* v = in + (long long)nbs * K;
-            const cx<T>* a = lk + (long long)h * K * K;
-            cx<T> s = czero<T>();
-            for (int j = 0; j < K; j++) cfma(s, a[(long long)j * K], v[j]);
-            if (hop_sign(t, L.nt, h) < 0) acc -= s; else acc += s;
+            for (int h = 0; h < 5; h++) {
+                const int nbs = nb_site(x, t, L.nx, L.nt, h);
+                const cx<T>* v = in + (long long)nbs * K;
+                const cx<T>* a = lk + (long long)h * K * K;
+                cx<T> s = czero<T>();
+#pragma unroll 4
+                for (int j = g; j < K; j += kTPR) cfma(s, a[(long long)j * K], v[j]);
+                if (hop_sign(t, L.nt, h) < 0) acc -= s; else acc += s;
+            }
         }
-        cx<T> self = in[e];
-        part_store(E, out, e, mass * self - acc);
+        acc = tpr_sum(acc);
+        if (on && g == 0) part_store(E, out, e, mass * in[e] - acc);
     }
     part_end(E);
 }
@@ -270,92 +290,32 @@ __device__ __forceinline__ int sap_site(const EngLevel<T>& L, int block, int m, 
     return x * L.nt + t;
 }
 
-// SAP_level_l::D_local (src/level.cpp:304-368) on all blocks of one colour at once:
-// in/out are [ncol][spb][K]; neighbours outside the block are dropped.
-template <typename T>
-__device__ __noinline__ void dlocal_apply(const Eng<T>& E, const EngLevel<T>& L, T m0, const int* blocks, int nblk,
-                                          const cx<T>* in, cx<T>* out) {
-    const int K = L.K, spb = L.sxe * L.ste, seglen = spb * K, tot = nblk * seglen;
-    const T mass = m0 + T(2);
-    int e0, e1;
-    eng_count(E, L.level, CNT_LOCAL_APPLY);
-    part_range(E, tot, e0, e1);
-    part_begin(E);
-    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
-        const int seg = e / seglen, r = e - seg * seglen;
-        const int m = r / K, i = r - m * K;
-        const int block = blocks[seg];
-        int x, t;
-        const int xs = sap_site(L, block, m, &x, &t);
-        const cx<T>* lk = L.links + (long long)xs * 5 * K * K + i;
-        const cx<T>* base = in + (long long)seg * seglen;
-        cx<T> acc = czero<T>();
-#pragma unroll 1
-        for (int h = 0; h < 5; h++) {
-            int nx_ = x, nt_ = t;
-            switch (h) {
-                case HOP_R0: nt_ = (t + 1 == L.nt) ? 0 : t + 1; break;
-                case HOP_R1: nx_ = (x + 1 == L.nx) ? 0 : x + 1; break;
-                case HOP_L0: nt_ = (t == 0) ? L.nt - 1 : t - 1; break;
-                case HOP_L1: nx_ = (x == 0) ? L.nx - 1 : x - 1; break;
-                default: break;
-            }
-            const int nbx = nx_ / L.sxe, nbt = nt_ / L.ste;
-            if (nbx * L.sbt + nbt != block) continue;
-            const int ml = (nx_ - nbx * L.sxe) * L.ste + (nt_ - nbt * L.ste);
-            const cx<T>* v = base + (long long)ml * K;
-            const cx<T>* a = lk + (long long)h * K * K;
-            cx<T> s = czero<T>();
-            for (int j = 0; j < K; j++) cfma(s, a[(long long)j * K], v[j]);
-            if (hop_sign(t, L.nt, h) < 0) acc -= s; else acc += s;
-        }
-        part_store(E, out, e, mass * base[r] - acc);
-    }
-    part_end(E);
-}
-
-// gather / scatter between a level vector and the colour's block segments
-template <typename T>
-__device__ void sap_gather(const EngLevel<T>& L, const int* blocks, int nblk, const cx<T>* v, cx<T>* seg) {
-    const int K = L.K, spb = L.sxe * L.ste, seglen = spb * K, tot = nblk * seglen;
-    for (int e = threadIdx.x; e < tot; e += blockDim.x) {
-        const int s = e / seglen, r = e - s * seglen, m = r / K, i = r - m * K;
-        int x, t;
-        const int xs = sap_site(L, blocks[s], m, &x, &t);
-        seg[e] = v[(long long)xs * K + i];
-    }
-    __syncthreads();
-}
-template <typename T>
-__device__ void sap_scatter_add(const EngLevel<T>& L, const int* blocks, int nblk, const cx<T>* seg, cx<T>* v) {
-    const int K = L.K, spb = L.sxe * L.ste, seglen = spb * K, tot = nblk * seglen;
-    for (int e = threadIdx.x; e < tot; e += blockDim.x) {
-        const int s = e / seglen, r = e - s * seglen, m = r / K, i = r - m * K;
-        int x, t;
-        const int xs = sap_site(L, blocks[s], m, &x, &t);
-        v[(long long)xs * K + i] += seg[e];
-    }
-    __syncthreads();
-}
-
 // Level::Pt_v (src/level.cpp:212-237): out[nc][2cc+s] = sum_{n in nc, c} conj(W_cc[n][2c+s]) v[n][2c+s]
 template <typename T>
 __device__ __noinline__ void restrict_v(const Eng<T>& E, const EngLevel<T>& L, const cx<T>* v, cx<T>* out) {
-    const int K = L.K, col = K / 2, nblk = L.bx * L.bt, tot = nblk * 2 * L.ntest;
+    const int K = L.K, col = K / 2, nblk = L.bx * L.bt, tot = nblk * 2 * L.ntest, nterm = L.xe * L.te * col;
     int e0, e1;
     part_range(E, tot, e0, e1);
     part_begin(E);
-    for (int o = e0 + threadIdx.x; o < e1; o += blockDim.x) {
-        const int nc = o / (2 * L.ntest), r = o - nc * 2 * L.ntest, cc = r >> 1, s = r & 1;
-        const int bxi = nc / L.bt, bti = nc - bxi * L.bt;
-        const cx<T>* w = L.W + (long long)cc * L.n * K;
+    const int g = threadIdx.x % kTPR, rows_per_pass = blockDim.x / kTPR;
+    for (int rb = e0; rb < e1; rb += rows_per_pass) {
+        const int o = rb + threadIdx.x / kTPR;
+        const bool on = o < e1;
         cx<T> acc = czero<T>();
-        for (int mx = 0; mx < L.xe; mx++)
-            for (int mt = 0; mt < L.te; mt++) {
+        if (on) {
+            const int nc = o / (2 * L.ntest), r = o - nc * 2 * L.ntest, cc = r >> 1, s = r & 1;
+            const int bxi = nc / L.bt, bti = nc - bxi * L.bt;
+            const cx<T>* w = L.W + (long long)cc * L.n * K;
+#pragma unroll 4
+            for (int q = g; q < nterm; q += kTPR) {
+                const int site = q / col, c = q - site * col;
+                const int mx = site / L.te, mt = site - mx * L.te;
                 const long long n = (long long)(bxi * L.xe + mx) * L.nt + (bti * L.te + mt);
-                for (int c = 0; c < col; c++) cfmac(acc, w[n * K + 2 * c + s], v[n * K + 2 * c + s]);
+                cfmac(acc, w[n * K + 2 * c + s], v[n * K + 2 * c + s]);
             }
-        part_store(E, out, o, acc);
+        }
+        acc = tpr_sum(acc);
+        if (on && g == 0) part_store(E, out, o, acc);
     }
     part_end(E);
 }
@@ -368,14 +328,21 @@ __device__ __noinline__ void prolong_v(const Eng<T>& E, const EngLevel<T>& L, co
     int e0, e1;
     part_range(E, tot, e0, e1);
     part_begin(E);
-    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
-        const int n = e / K, d = e - n * K, s = d & 1;
-        const int x = n / L.nt, t = n - x * L.nt;
-        const int nc = (x / L.xe) * L.bt + (t / L.te);
-        const cx<T>* pv = vc + (long long)nc * 2 * L.ntest + s;
+    const int g = threadIdx.x % kTPR, rows_per_pass = blockDim.x / kTPR;
+    for (int rb = e0; rb < e1; rb += rows_per_pass) {
+        const int e = rb + threadIdx.x / kTPR;
+        const bool on = e < e1;
         cx<T> acc = czero<T>();
-        for (int cc = 0; cc < L.ntest; cc++) cfma(acc, L.W[(long long)cc * L.n * K + e], pv[2 * cc]);
-        part_store(E, out, e, accumulate ? out[e] + acc : acc);
+        if (on) {
+            const int n = e / K, d = e - n * K, s = d & 1;
+            const int x = n / L.nt, t = n - x * L.nt;
+            const int nc = (x / L.xe) * L.bt + (t / L.te);
+            const cx<T>* pv = vc + (long long)nc * 2 * L.ntest + s;
+#pragma unroll 2
+            for (int cc = g; cc < L.ntest; cc += kTPR) cfma(acc, L.W[(long long)cc * L.n * K + e], pv[2 * cc]);
+        }
+        acc = tpr_sum(acc);
+        if (on && g == 0) part_store(E, out, e, accumulate ? out[e] + acc : acc);
     }
     part_end(E);
 }
@@ -553,33 +520,40 @@ __device__ void dlocal_block(const Team& tm, const EngLevel<T>& L, T m0, int blo
     const int K = L.K, spb = L.sxe * L.ste, n = spb * K;
     const T mass = m0 + T(2);
     const int bxi = block / L.sbt, bti = block - bxi * L.sbt;
-    for (int e = tm.tid; e < n; e += tm.size) {
-        const int m = e / K, i = e - m * K;
-        const int mx = m / L.ste, mt = m - mx * L.ste;
-        const int x = bxi * L.sxe + mx, t = bti * L.ste + mt;
-        const int xs = x * L.nt + t;
-        const cx<T>* lk = L.links + (long long)xs * 5 * K * K + i;
+    const int g = tm.tid % kTPR, rows_per_pass = tm.size / kTPR;
+    for (int rb = 0; rb < n; rb += rows_per_pass) {
+        const int e = rb + tm.tid / kTPR;
+        const bool on = e < n;
         cx<T> acc = czero<T>();
+        if (on) {
+            const int m = e / K, i = e - m * K;
+            const int mx = m / L.ste, mt = m - mx * L.ste;
+            const int x = bxi * L.sxe + mx, t = bti * L.ste + mt;
+            const int xs = x * L.nt + t;
+            const cx<T>* lk = L.links + (long long)xs * 5 * K * K + i;
 #pragma unroll 1
-        for (int h = 0; h < 5; h++) {
-            int nx_ = x, nt_ = t;
-            switch (h) {
-                case HOP_R0: nt_ = (t + 1 == L.nt) ? 0 : t + 1; break;
-                case HOP_R1: nx_ = (x + 1 == L.nx) ? 0 : x + 1; break;
-                case HOP_L0: nt_ = (t == 0) ? L.nt - 1 : t - 1; break;
-                case HOP_L1: nx_ = (x == 0) ? L.nx - 1 : x - 1; break;
-                default: break;
+            for (int h = 0; h < 5; h++) {
+                int nx_ = x, nt_ = t;
+                switch (h) {
+                    case HOP_R0: nt_ = (t + 1 == L.nt) ? 0 : t + 1; break;
+                    case HOP_R1: nx_ = (x + 1 == L.nx) ? 0 : x + 1; break;
+                    case HOP_L0: nt_ = (t == 0) ? L.nt - 1 : t - 1; break;
+                    case HOP_L1: nx_ = (x == 0) ? L.nx - 1 : x - 1; break;
+                    default: break;
+                }
+                const int nbx = nx_ / L.sxe, nbt = nt_ / L.ste;
+                if (nbx * L.sbt + nbt != block) continue;
+                const int ml = (nx_ - nbx * L.sxe) * L.ste + (nt_ - nbt * L.ste);
+                const cx<T>* v = in + (long long)ml * K;
+                const cx<T>* a = lk + (long long)h * K * K;
+                cx<T> s = czero<T>();
+#pragma unroll 4
+                for (int j = g; j < K; j += kTPR) cfma(s, a[(long long)j * K], v[j]);
+                if (hop_sign(t, L.nt, h) < 0) acc -= s; else acc += s;
             }
-            const int nbx = nx_ / L.sxe, nbt = nt_ / L.ste;
-            if (nbx * L.sbt + nbt != block) continue;
-            const int ml = (nx_ - nbx * L.sxe) * L.ste + (nt_ - nbt * L.ste);
-            const cx<T>* v = in + (long long)ml * K;
-            const cx<T>* a = lk + (long long)h * K * K;
-            cx<T> s = czero<T>();
-            for (int j = 0; j < K; j++) cfma(s, a[(long long)j * K], v[j]);
-            if (hop_sign(t, L.nt, h) < 0) acc -= s; else acc += s;
         }
-        out[e] = mass * in[e] - acc;
+        acc = tpr_sum(acc);
+        if (on && g == 0) out[e] = mass * in[e] - acc;
     }
 }
 

@@ -31,7 +31,7 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 NX = NT = 1024
-ROWS = [[0, 8, 8, 16, 64, 64], [1, 4, 4, 16, 4, 4], [2, 2, 2, 16, 2, 2]]
+ROWS = [[0, 8, 8, 16, 32, 32], [1, 4, 4, 16, 4, 4], [2, 2, 2, 16, 2, 2]]
 BETA, M0, TOL = 4.0, -0.05, 1e-10
 METRIC = "1024^2 solves/s at FP64 resid <=1e-10: mixed+batched vs FP64 GPU; D-apply GB/s"
 UNIT = "solves/s"
