@@ -272,7 +272,7 @@ __device__ __noinline__ void dc_apply(const Eng<T>& E, const EngLevel<T>& L, T m
                 if (hop_sign(t, L.nt, h) < 0) acc -= s; else acc += s;
             }
         }
-        acc = tpr_sum(acc);
+        acc = tpr_sum<T>(acc);
         if (on && g == 0) part_store(E, out, e, mass * in[e] - acc);
     }
     part_end(E);
@@ -314,7 +314,7 @@ __device__ __noinline__ void restrict_v(const Eng<T>& E, const EngLevel<T>& L, c
                 cfmac(acc, w[n * K + 2 * c + s], v[n * K + 2 * c + s]);
             }
         }
-        acc = tpr_sum(acc);
+        acc = tpr_sum<T>(acc);
         if (on && g == 0) part_store(E, out, o, acc);
     }
     part_end(E);
@@ -341,7 +341,7 @@ __device__ __noinline__ void prolong_v(const Eng<T>& E, const EngLevel<T>& L, co
 #pragma unroll 2
             for (int cc = g; cc < L.ntest; cc += kTPR) cfma(acc, L.W[(long long)cc * L.n * K + e], pv[2 * cc]);
         }
-        acc = tpr_sum(acc);
+        acc = tpr_sum<T>(acc);
         if (on && g == 0) part_store(E, out, e, accumulate ? out[e] + acc : acc);
     }
     part_end(E);
@@ -552,7 +552,7 @@ __device__ void dlocal_block(const Team& tm, const EngLevel<T>& L, T m0, int blo
                 if (hop_sign(t, L.nt, h) < 0) acc -= s; else acc += s;
             }
         }
-        acc = tpr_sum(acc);
+        acc = tpr_sum<T>(acc);
         if (on && g == 0) out[e] = mass * in[e] - acc;
     }
 }
