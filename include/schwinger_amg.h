@@ -120,6 +120,21 @@ AMG_API int amg_dirac_apply_dev(amg_ctx ctx, const void* in, void* out, int nrhs
  * in_dev / out_dev [nrhs][N][2] complex128, launched on `stream` (a cudaStream_t). */
 AMG_API int amg_dirac_apply_raw(const void* U_dev, const void* in_dev, void* out_dev, int nx, int nt,
                         int nrhs, double m0, int dagger, void* stream);
+/* Stand-alone FP64 level-0 restriction out = P^dagger v that allocates no device memory, for
+ * callers that may not allocate while they run (an application that owns all device memory
+ * through its own pool, or code inside a region where an allocation would synchronise or
+ * fail).  No counterpart in the reference: it computes what Level::Pt_v does at level 0
+ * (src/level.cpp:212-237) and what amg_restrict(ctx, 0, ...) returns.
+ *   W_dev   [ntest][N][2] complex128 test vectors (amg_get_test_vectors layout)
+ *   v_dev   [nrhs][N][2] complex128, out_dev [nrhs][bx*bt][2*ntest] complex128
+ *   bx, bt  aggregate counts along x and t (nx % bx == nt % bt == 0), ntest in [1, 32]
+ * Chunk partial sums go to a 4 MiB array owned by the library on every device; calls with
+ * nrhs * bx * bt * 2 * ntest * 16 > 4 MiB are rejected with AMG_ERR_INVALID.  The buffers
+ * belong to the current device.  The first call on a device looks up that array's address
+ * (make that first call before any stream capture).  All calls on a device share the array,
+ * so calls that overlap on the GPU (other streams, other host threads) race; serialise them. */
+AMG_API int amg_restrict_raw_noalloc(const void* W_dev, const void* v_dev, void* out_dev, int nx, int nt,
+                                     int bx, int bt, int ntest, int nrhs, void* stream);
 
 /* ---- set-up ------------------------------------------------------------------------ */
 /* Optional: the test vectors the set-up starts from on level l, W[Ntest_l][N_l][DOF_l]
