@@ -65,6 +65,7 @@ class AMGContext:
         self.rows = [list(map(int, r)) for r in rows]
         self.levels = len(self.rows) + 1
         self.m0 = float(m0)
+        self.device = int(device)
         p = params if params is not None else default_params(**param_over)
         self.params = p
         r = np.ascontiguousarray(np.array(self.rows, dtype=np.int32).reshape(-1))
@@ -218,6 +219,37 @@ class AMGContext:
         check(lib().amg_solve(self._h, C.c_void_p(b_ptr), C.c_void_p(x_ptr), nrhs, infos), "amg_solve")
         return [dict(iterations=i.iterations, converged=bool(i.converged), rel_residual=i.rel_residual)
                 for i in infos]
+
+    # ---- adjoint
+    def solve_adjoint(self, g):
+        """lambda = D^{-dagger} g on the same hierarchy; returns (lambda, infos)."""
+        g = _c128(g)
+        nrhs = 1 if g.ndim == 2 else g.shape[0]
+        lam = np.empty_like(g)
+        infos = (AmgSolveInfo * nrhs)()
+        check(lib().amg_solve_adjoint(self._h, _cptr(g), _cptr(lam), nrhs, infos), "amg_solve_adjoint")
+        return lam, [dict(iterations=i.iterations, converged=bool(i.converged), rel_residual=i.rel_residual)
+                     for i in infos]
+
+    def solve_adjoint_dev(self, g_ptr: int, lam_ptr: int, nrhs: int):
+        infos = (AmgSolveInfo * nrhs)()
+        check(lib().amg_solve_adjoint_dev(self._h, C.c_void_p(g_ptr), C.c_void_p(lam_ptr), nrhs, infos),
+              "amg_solve_adjoint_dev")
+        return [dict(iterations=i.iterations, converged=bool(i.converged), rel_residual=i.rel_residual)
+                for i in infos]
+
+    def force(self, lam, x) -> np.ndarray:
+        """F[n][mu] = -sum_r Re(lam_r^dagger dD/dtheta_mu(n) x_r), float64 [N][2]."""
+        lam = _c128(lam)
+        x = _c128(x, lam.shape)
+        nrhs = 1 if lam.ndim == 2 else lam.shape[0]
+        F = np.empty((self.N, 2), dtype=np.float64)
+        check(lib().amg_force(self._h, _cptr(lam), _cptr(x), nrhs, _cptr(F)), "amg_force")
+        return F
+
+    def force_dev(self, lam_ptr: int, x_ptr: int, nrhs: int, F_ptr: int) -> None:
+        check(lib().amg_force_dev(self._h, C.c_void_p(lam_ptr), C.c_void_p(x_ptr), nrhs, C.c_void_p(F_ptr)),
+              "amg_force_dev")
 
     def residual_history(self) -> np.ndarray:
         n = C.c_int(0)

@@ -173,7 +173,7 @@ struct amg_context {
     std::vector<LevelHost> lv;
     PrecSet<double> d;             // FP64 hierarchy (master)
     PrecSet<float> f;              // FP32 / BF16 copy for the mixed form
-    DevBuf hops0, linkpart, zero, boot_a, boot_b;
+    DevBuf hops0, linkpart, zero, boot_a, boot_b, adj;
     std::vector<int> have_init;
     int gauge_set = 0, setup_done = 0;
     // outer FGMRES
@@ -1124,6 +1124,13 @@ int amg_set_mass(amg_ctx c, double m0) {
     return AMG_OK;
 }
 
+int amg_set_cycle(amg_ctx c, int cycle) {
+    if (!c) return fail(AMG_ERR_INVALID, "null context");
+    if (cycle != AMG_CYCLE_K && cycle != AMG_CYCLE_V) return fail(AMG_ERR_INVALID, "cycle must be AMG_CYCLE_K or AMG_CYCLE_V");
+    c->p.cycle = cycle;
+    return AMG_OK;
+}
+
 int amg_level_info(amg_ctx c, int level, int* o) {
     if (!c || !o) return fail(AMG_ERR_INVALID, "null argument");
     if (level < 0 || level >= c->L) return fail(AMG_ERR_INVALID, "level %d out of range", level);
@@ -1174,6 +1181,19 @@ int amg_dirac_apply_raw(const void* U_dev, const void* in_dev, void* out_dev, in
                          dagger ? 1 : 0, (cudaStream_t)stream);
     CKL();
     return AMG_OK;
+}
+
+int amg_dirac_apply_host(const double* U, const double* in, double* out, int nx, int nt, int nrhs, double m0,
+                         int dagger) {
+    if (!U || !in || !out || nx < 2 || nt < 2 || nrhs < 1) return fail(AMG_ERR_INVALID, "bad argument");
+    const long long N = (long long)nx * nt;
+    DevBuf u, a, b;
+    CKR(to_dev(u, U, 2 * N, 0));
+    CKR(to_dev(a, in, 2 * N * nrhs, 0));
+    CKR(to_dev(b, nullptr, 2 * N * nrhs, 0));
+    launch_dirac<double>(u.as<double2>(), a.as<double2>(), b.as<double2>(), nx, nt, nrhs, m0, dagger ? 1 : 0, 0);
+    CKL();
+    return to_host(out, b, 2 * N * nrhs, 0);
 }
 
 int amg_set_initial_test_vectors(amg_ctx c, int level, const double* W) {
@@ -1419,21 +1439,67 @@ int amg_residual_history(amg_ctx c, double* out, int max_len, int* len) {
     return AMG_OK;
 }
 
-int amg_solve_adjoint(amg_ctx c, const double* g, double* lambda, int nrhs, amg_solve_info* info) {
-    (void)c; (void)g; (void)lambda; (void)nrhs; (void)info;
-    return fail(AMG_ERR_UNSUPPORTED, "adjoint solve not built yet");
-}
+// D^dagger lambda = g through the solve of D: lambda = gamma5 D^{-1} gamma5 g.  The FP64
+// true residual reported for D y = gamma5 g equals ||g - D^dagger lambda|| / ||g|| because
+// gamma5 is unitary.
 int amg_solve_adjoint_dev(amg_ctx c, const void* g, void* lambda, int nrhs, amg_solve_info* info) {
-    (void)c; (void)g; (void)lambda; (void)nrhs; (void)info;
-    return fail(AMG_ERR_UNSUPPORTED, "adjoint solve not built yet");
+    CKR(check_ready(c, 0, true));
+    if (!g || !lambda || nrhs < 1) return fail(AMG_ERR_INVALID, "bad argument");
+    CKR(select_device(c));
+    const long long n = (long long)nrhs * vlen0(c);
+    CKR(c->adj.alloc((size_t)n * sizeof(double2)));
+    launch_gamma5(c->adj.as<double2>(), (const double2*)g, n / 2, c->stream);
+    CKL();
+    const int rc = amg_solve_dev(c, c->adj.p, lambda, nrhs, info);
+    if (rc < 0) return rc;
+    launch_gamma5((double2*)lambda, (const double2*)lambda, n / 2, c->stream);
+    CKL();
+    CK(cudaStreamSynchronize(c->stream));
+    return rc;
 }
-int amg_force(amg_ctx c, const double* lambda, const double* x, int nrhs, double* F) {
-    (void)c; (void)lambda; (void)x; (void)nrhs; (void)F;
-    return fail(AMG_ERR_UNSUPPORTED, "force not built yet");
+
+int amg_solve_adjoint(amg_ctx c, const double* g, double* lambda, int nrhs, amg_solve_info* info) {
+    CKR(check_ready(c, 0, true));
+    if (!g || !lambda || nrhs < 1) return fail(AMG_ERR_INVALID, "bad argument");
+    CKR(select_device(c));
+    if (nrhs > c->Rcap) {
+        CKR(ensure_capacity(c, nrhs));
+        CKR(build_engine<double>(c, c->d, std::max(c->d.eng_cap, nrhs)));
+        if (c->p.precision == AMG_PREC_MIXED) CKR(build_engine<float>(c, c->f, std::max(c->f.eng_cap, nrhs)));
+    }
+    const long long n = (long long)nrhs * vlen0(c);
+    CK(cudaMemcpyAsync(c->b.p, g, (size_t)n * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+    const int rc = amg_solve_adjoint_dev(c, c->b.p, c->x.p, nrhs, info);
+    if (rc < 0) return rc;
+    CK(cudaMemcpyAsync(lambda, c->x.p, (size_t)n * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return rc;
 }
+
 int amg_force_dev(amg_ctx c, const void* lambda, const void* x, int nrhs, void* F) {
-    (void)c; (void)lambda; (void)x; (void)nrhs; (void)F;
-    return fail(AMG_ERR_UNSUPPORTED, "force not built yet");
+    if (!c || !lambda || !x || !F || nrhs < 1) return fail(AMG_ERR_INVALID, "bad argument");
+    if (!c->gauge_set) return fail(AMG_ERR_STATE, "gauge field not set");
+    CKR(select_device(c));
+    launch_force(c->d.U.as<double2>(), (const double2*)lambda, (const double2*)x, (double2*)F, c->nx, c->nt, nrhs,
+                 c->stream);
+    CKL();
+    CK(cudaStreamSynchronize(c->stream));
+    return AMG_OK;
+}
+
+int amg_force(amg_ctx c, const double* lambda, const double* x, int nrhs, double* F) {
+    if (!c || !lambda || !x || !F || nrhs < 1) return fail(AMG_ERR_INVALID, "bad argument");
+    if (!c->gauge_set) return fail(AMG_ERR_STATE, "gauge field not set");
+    CKR(select_device(c));
+    DevBuf a, b, f;
+    const long long n = (long long)nrhs * vlen0(c);
+    CKR(to_dev(a, lambda, n, c->stream));
+    CKR(to_dev(b, x, n, c->stream));
+    CKR(to_dev(f, nullptr, c->N, c->stream));
+    launch_force(c->d.U.as<double2>(), a.as<double2>(), b.as<double2>(), f.as<double2>(), c->nx, c->nt, nrhs,
+                 c->stream);
+    CKL();
+    return to_host(F, f, c->N, c->stream);
 }
 
 int amg_engine_counters(amg_ctx c, long long* out, int len) {

@@ -610,6 +610,69 @@ void launch_f2d(double2* y, const float2* x, long long n, cudaStream_t s) {
 void launch_d2bf(__nv_bfloat162* y, const double2* x, long long n, cudaStream_t s) {
     count_launch(1); k_d2bf<<<592, 256, 0, s>>>(y, x, n); }
 
+// ---------------------------------------------------------------------------------
+// Adjoint support.  gamma5 = diag(1, -1) on the spin index; D^dagger = gamma5 D gamma5
+// (the projectors of src/dirac_operator.cpp:3-27 swapped, as D_dagger_phi does, :30-54).
+// ---------------------------------------------------------------------------------
+__global__ void k_gamma5(double2* __restrict__ y, const double2* __restrict__ x, long long nsites) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nsites;
+         i += (long long)gridDim.x * blockDim.x) {
+        const double2 a = x[2 * i], b = x[2 * i + 1];
+        y[2 * i] = a;
+        y[2 * i + 1] = make_double2(-b.x, -b.y);
+    }
+}
+
+// Fermion force F[n][mu] = -sum_r Re(lam_r^dagger (dD/dtheta_mu(n)) x_r) for U = exp(i theta).
+// theta_mu(n) enters D through two hops of src/dirac_operator.cpp:11-22: row n, column
+// n+mu, -1/2 (1 - sigma_mu) U_mu(n) s; and row n+mu, column n, -1/2 (1 + sigma_mu) conj(U_mu(n)) s,
+// with s = -1 on the time hop across t = Nt-1 (the antiperiodic boundary, include/boundary.h:29-40).
+// With A = lam(n)^dagger (1 - sigma_mu) x(n+mu) and B = lam(n+mu)^dagger (1 + sigma_mu) x(n):
+//   F = s/2 (Im(conj(U) B) - Im(U A)).
+// One thread per site; the projector contractions are summed over sources before the link.
+__global__ void __launch_bounds__(256) k_force(const double2* __restrict__ U, const double2* __restrict__ lam,
+                                               const double2* __restrict__ x, double2* __restrict__ F, int nx,
+                                               int nt, int nrhs) {
+    const int N = nx * nt;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    const int xi = n / nt, t = n - xi * nt;
+    const int nT = xi * nt + (t + 1 == nt ? 0 : t + 1);
+    const int nX = (xi + 1 == nx ? 0 : xi + 1) * nt + t;
+    double2 A0 = czero<double>(), B0 = czero<double>(), A1 = czero<double>(), B1 = czero<double>();
+    for (int r = 0; r < nrhs; r++) {
+        const long long off = (long long)r * N * 2;
+        const double2 l0 = lam[off + 2 * n], l1 = lam[off + 2 * n + 1];
+        const double2 x0 = x[off + 2 * n], x1 = x[off + 2 * n + 1];
+        const double2 xt0 = x[off + 2 * nT], xt1 = x[off + 2 * nT + 1];
+        const double2 lt0 = lam[off + 2 * nT], lt1 = lam[off + 2 * nT + 1];
+        const double2 xs0 = x[off + 2 * nX], xs1 = x[off + 2 * nX + 1];
+        const double2 ls0 = lam[off + 2 * nX], ls1 = lam[off + 2 * nX + 1];
+        // time, sigma_0 = [[0,1],[1,0]]: (1 - s0) -> (l0 - l1)^* (x0 - x1), (1 + s0) -> (l0 + l1)^* (x0 + x1)
+        cfmac(A0, l0 - l1, xt0 - xt1);
+        cfmac(B0, lt0 + lt1, x0 + x1);
+        // space, sigma_1 = [[0,-i],[i,0]]: (1 - s1) -> (l0 + i l1)^* (x0 + i x1),
+        //                                  (1 + s1) -> (l0 - i l1)^* (x0 - i x1)
+        cfmac(A1, l0 + cmuli(l1), xs0 + cmuli(xs1));
+        cfmac(B1, ls0 - cmuli(ls1), x0 - cmuli(x1));
+    }
+    const double2 u0 = U[2 * n], u1 = U[2 * n + 1];
+    const double s0 = (t == nt - 1) ? -0.5 : 0.5;
+    const double f0 = s0 * ((u0.x * B0.y - u0.y * B0.x) - (u0.x * A0.y + u0.y * A0.x));
+    const double f1 = 0.5 * ((u1.x * B1.y - u1.y * B1.x) - (u1.x * A1.y + u1.y * A1.x));
+    F[n] = make_double2(f0, f1);
+}
+
+void launch_gamma5(double2* y, const double2* x, long long nsites, cudaStream_t s) {
+    count_launch(1);
+    k_gamma5<<<1184, 256, 0, s>>>(y, x, nsites);
+}
+void launch_force(const double2* U, const double2* lam, const double2* x, double2* F, int nx, int nt, int nrhs,
+                  cudaStream_t s) {
+    count_launch(1);
+    k_force<<<(nx * nt + 255) / 256, 256, 0, s>>>(U, lam, x, F, nx, nt, nrhs);
+}
+
 #define INST(T)                                                                                                 \
     template void launch_dirac<T>(const cx<T>*, const cx<T>*, cx<T>*, int, int, int, T, int, cudaStream_t);     \
     template void launch_residual<T>(const cx<T>*, const cx<T>*, long long, const cx<T>*, cx<T>*, int, int, int, T,\

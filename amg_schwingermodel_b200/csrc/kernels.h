@@ -51,6 +51,10 @@ void launch_d2f(float2* y, const double2* x, long long n, cudaStream_t s);
 void launch_f2d(double2* y, const float2* x, long long n, cudaStream_t s);
 void launch_d2bf(__nv_bfloat162* y, const double2* x, long long n, cudaStream_t s);
 
+void launch_gamma5(double2* y, const double2* x, long long nsites, cudaStream_t s);
+void launch_force(const double2* U, const double2* lam, const double2* x, double2* F, int nx, int nt, int nrhs,
+                  cudaStream_t s);
+
 // ---- coarse engine (coarse.cu) ----
 enum EngOp {
     ENG_KFGMRES = 0,   // FGMRES_k_cycle of level l: x = fgmres(b, x0 = b)

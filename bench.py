@@ -214,10 +214,12 @@ def run_ours(args, world, rank, local):
     sampler.start()
     l0 = launch_count()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push("timed")
     e0.record(stream)
     for _ in range(args.steps):
         infos = ctx.solve_dev(b_dev.data_ptr(), x_dev.data_ptr(), R)
     e1.record(stream)
+    torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     launches = launch_count() - l0
     clocks = sampler.stop()
@@ -285,10 +287,12 @@ def run_ours(args, world, rank, local):
     torch.cuda.synchronize()
     g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     nrep = 30
+    torch.cuda.nvtx.range_push("dapply")
     g0.record(ds)
     for _ in range(nrep):
         dirac_apply_raw(Ud.data_ptr(), vin.data_ptr(), vout.data_ptr(), NX, NT, nd, M0, False, ds.cuda_stream)
     g1.record(ds)
+    torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     d_ms = g0.elapsed_time(g1) / nrep
     d_bytes = N * (32 + nd * 64)

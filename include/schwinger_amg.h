@@ -104,6 +104,9 @@ AMG_API int amg_destroy(amg_ctx ctx);
 AMG_API int amg_get_params(amg_ctx ctx, amg_params* out);
 /* mass::m0 (include/variables.h:20-22) */
 AMG_API int amg_set_mass(amg_ctx ctx, double m0);
+/* Replaces assigning AMGV::cycle (include/variables.h:64) after creation: AMG_CYCLE_K or
+ * AMG_CYCLE_V for the amg_cycle, amg_solve and bootstrap calls that follow. */
+AMG_API int amg_set_cycle(amg_ctx ctx, int cycle);
 /* Level sizes as LevelV fills them: out[l] = {Nsites, NxSites, NtSites, DOF, Colors, Ntest}. */
 AMG_API int amg_level_info(amg_ctx ctx, int level, int* out6);
 
@@ -120,6 +123,11 @@ AMG_API int amg_dirac_apply_dev(amg_ctx ctx, const void* in, void* out, int nrhs
  * in_dev / out_dev [nrhs][N][2] complex128, launched on `stream` (a cudaStream_t). */
 AMG_API int amg_dirac_apply_raw(const void* U_dev, const void* in_dev, void* out_dev, int nx, int nt,
                         int nrhs, double m0, int dagger, void* stream);
+/* Stand-alone FP64 stencil on host arrays, no context: D_phi / D_dagger_phi
+ * (src/dirac_operator.cpp:3-54) with the reference's signature data (U[N][2], in/out
+ * [nrhs][N][2]); device buffers are allocated and freed inside the call. */
+AMG_API int amg_dirac_apply_host(const double* U, const double* in, double* out, int nx, int nt, int nrhs,
+                                 double m0, int dagger);
 /* Stand-alone FP64 level-0 restriction out = P^dagger v that allocates no device memory, for
  * callers that may not allocate while they run (an application that owns all device memory
  * through its own pool, or code inside a region where an allocation would synchronise or
@@ -179,11 +187,15 @@ AMG_API int amg_solve_dev(amg_ctx ctx, const void* b_dev, void* x_dev, int nrhs,
 AMG_API int amg_residual_history(amg_ctx ctx, double* out, int max_len, int* len);
 
 /* ---- adjoint (no reference counterpart beyond D_dagger_phi) ------------------------- */
-/* lambda = D^{-dagger} g through the same hierarchy: lambda = gamma5 D^{-1} gamma5 g. */
+/* lambda = D^{-dagger} g through the same hierarchy: lambda = gamma5 D^{-1} gamma5 g
+ * (D_dagger_phi = gamma5 D_phi gamma5, src/dirac_operator.cpp:3-54).  info[i].rel_residual
+ * is ||g - D^dagger lambda|| / ||g||. */
 AMG_API int amg_solve_adjoint(amg_ctx ctx, const double* g, double* lambda, int nrhs, amg_solve_info* info);
 AMG_API int amg_solve_adjoint_dev(amg_ctx ctx, const void* g_dev, void* lambda_dev, int nrhs, amg_solve_info* info);
-/* Fermion force: F[n][mu] = Re(lambda^dagger dD/dtheta_mu(n) x) for U = exp(i theta),
- * summed over the nrhs pairs; F[N][2] float64. */
+/* Fermion force: F[n][mu] = -sum_r Re(lambda_r^dagger dD/dtheta_mu(n) x_r) for U = exp(i theta),
+ * F[N][2] float64.  With x = D^{-1} b and lambda = D^{-dagger} eta this is dL/dtheta of
+ * L = Re(eta^dagger D^{-1} b); twice it with x = (D^dagger D)^{-1} phi and lambda = D x is the
+ * derivative of phi^dagger (D^dagger D)^{-1} phi. */
 AMG_API int amg_force(amg_ctx ctx, const double* lambda, const double* x, int nrhs, double* F);
 AMG_API int amg_force_dev(amg_ctx ctx, const void* lambda_dev, const void* x_dev, int nrhs, void* F_dev);
 

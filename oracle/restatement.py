@@ -257,6 +257,50 @@ def level_operator_matrix(G1, G2, G3, lp: LevelParams, m0: float) -> sp.csr_matr
 
 
 # --------------------------------------------------------------------------------------
+# Adjoint: gamma5, the fine operator as a sparse matrix, and the fermion force
+# (no reference code; derived from the reference's operator, src/level.cpp:87-180)
+# --------------------------------------------------------------------------------------
+def gamma5(v: np.ndarray) -> np.ndarray:
+    """gamma5 = diag(1, -1) on the spin index of a fine vector [..., N, 2];
+    D_dagger_phi = gamma5 D_phi gamma5 (src/dirac_operator.cpp:3-54)."""
+    out = np.array(v, dtype=np.complex128, copy=True)
+    out[..., 1] *= -1
+    return out
+
+
+def dirac_matrix(U: np.ndarray, m0: float, nx: int, nt: int) -> sp.csr_matrix:
+    """The fine Wilson-Dirac operator D (= Level::D_operator at level 0, built from
+    Level::makeDirac's links, src/level.cpp:87-180) as a sparse matrix on [N][2]."""
+    lp = LevelParams(0, nx, nt, 1)
+    G1, G2, G3 = make_dirac(U, lp)
+    return level_operator_matrix(G1, G2, G3, lp, m0)
+
+
+def force(U: np.ndarray, lam: np.ndarray, x: np.ndarray, nx: int, nt: int) -> np.ndarray:
+    """F[n][mu] = -sum_r Re(lam_r^dagger (dD/dtheta_mu(n)) x_r) for U = exp(i theta).
+
+    theta_mu(m) enters D (src/level.cpp:161-180 with the level-0 links of :87-125) through
+    G2[m][.][.][mu] = 1/2 (1 - sigma_mu) U_mu(m), applied with signR(m, mu) to x(m + mu), and
+    G3[m + mu][.][.][mu] = 1/2 (1 + sigma_mu) conj(U_mu(m)), applied with signL(m + mu, mu) to
+    x(m); d/dtheta multiplies the first by i and the second by -i.  Since D = (m0+2) - hops,
+    F = Re(lam(m)^dag i G2 signR x(m+mu)) + Re(lam(m+mu)^dag (-i) G3 signL x(m))."""
+    lp = LevelParams(0, nx, nt, 1)
+    R, Lf, sR, sL = boundary(lp)
+    _, G2, G3 = make_dirac(U, lp)
+    lam = np.asarray(lam).reshape(-1, lp.n, 2)
+    x = np.asarray(x).reshape(-1, lp.n, 2)
+    F = np.zeros((lp.n, 2))
+    for mu in range(2):
+        g2 = G2[:, :, :, 0, 0, mu]                       # [m][alf][bet]
+        fwd = R[:, mu]                                   # m + mu
+        g3 = G3[fwd, :, :, 0, 0, mu]                     # G3 of the row m + mu
+        t2 = np.einsum("rma,mab,rmb->m", np.conj(lam), g2, x[:, fwd])
+        t3 = np.einsum("rma,mab,rmb->m", np.conj(lam[:, fwd]), g3, x)
+        F[:, mu] = np.real(1j * t2 * sR[:, mu]) + np.real(-1j * t3 * sL[fwd, mu])
+    return F
+
+
+# --------------------------------------------------------------------------------------
 # Interpolation
 # --------------------------------------------------------------------------------------
 def site_block(lp: LevelParams) -> np.ndarray:

@@ -10,6 +10,11 @@ reference's outputs on them: index maps, D_phi / D_dagger_phi, the set-up hierar
 vectors and coarse links), per-level operator / P / P^dagger / SAP / GMRES probes, one
 preconditioner application, and the outer solve (x, iteration count, residual history).
 Large arrays are dropped for the bigger lattices to keep the files small.
+
+The adjoint fixture (ADJOINT) holds the reference's two solves behind the gradient of
+L = Re(eta^dagger D^{-1} b): x = D^{-1} b and y = D^{-1} gamma5 eta (so lambda = gamma5 y),
+each a full FGMRES_AMG run of the reference; the gauge field and the two sources are
+regenerated from the seeds in its meta.
 """
 from __future__ import annotations
 
@@ -22,7 +27,7 @@ import numpy as np
 ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
 
-from amg_schwingermodel_b200.inputs import gauge_field, gaussian_spinor  # noqa: E402
+from amg_schwingermodel_b200.inputs import gauge_angles, gauge_field, gaussian_spinor  # noqa: E402
 from oracle import ref_runner  # noqa: E402
 from oracle.restatement import read_parameters  # noqa: E402
 
@@ -35,6 +40,12 @@ CONFIGS = {
     "c32_l3_k_nit1": (32, [[0, 4, 4, 6, 2, 2], [1, 2, 2, 6, 2, 2]], 2.0, -0.1, 14, {"nit": 1}, False),
     "c64_l2_k": (64, [[0, 8, 8, 10, 4, 4]], 2.0, -0.1, 1, {}, False),
     "c64_l4_k": (64, [[0, 8, 8, 8, 4, 4], [1, 4, 4, 8, 4, 4], [2, 2, 2, 8, 2, 2]], 4.0, -0.05, 15, {}, False),
+}
+
+# name: (ns, rows, beta, m0, seed); inputs: theta = gauge_angles(ns, ns, beta, seed),
+# b = gaussian_spinor(N, 2, seed + 1000), eta = gaussian_spinor(N, 2, seed + 3000)
+ADJOINT = {
+    "adj128_l3": (128, [[0, 8, 8, 12, 4, 4], [1, 4, 4, 12, 4, 4]], 2.0, -0.1, 21),
 }
 
 SMALL_KEYS_ALWAYS = ("dphi", "ddagphi", "x", "cycle0_rhs")
@@ -72,8 +83,33 @@ def make(name: str, cfg) -> dict:
     return arrays
 
 
+def make_adjoint(name: str, cfg) -> dict:
+    ns, rows, beta, m0, seed = cfg
+    L = len(rows) + 1
+    ref_runner.build(ns, ns, L)
+    N = ns * ns
+    U = np.exp(1j * gauge_angles(ns, ns, beta, seed))
+    b = gaussian_spinor(N, 2, seed + 1000)
+    eta = gaussian_spinor(N, 2, seed + 3000)
+    g5eta = eta.copy()
+    g5eta[:, 1] *= -1
+    job = dict(cycle=1, nit=0, nu1=0, nu2=2, sap_tv_iters=4, dump_hierarchy=0)
+    ox = ref_runner.run(ns, ns, rows, U, b, m0=m0, **job)
+    oy = ref_runner.run(ns, ns, rows, U, g5eta, m0=m0, **job)
+    meta = dict(ns=ns, nt=ns, rows=rows, beta=beta, m0=m0, seed=seed, job=job,
+                iterations_x=int(ox["info:iterations"]), iterations_y=int(oy["info:iterations"]),
+                true_rel_residual_x=ox["info:true_rel_residual"], true_rel_residual_y=oy["info:true_rel_residual"])
+    return {"x": ox["x"], "y": oy["x"], "meta": np.array(json.dumps(meta))}
+
+
 def main(names=None):
     here = Path(__file__).resolve().parent
+    for name, cfg in ADJOINT.items():
+        if names and name not in names:
+            continue
+        arrays = make_adjoint(name, cfg)
+        np.savez_compressed(here / f"{name}.npz", **arrays)
+        print(name, (here / f"{name}.npz").stat().st_size // 1024, "KiB")
     for name, cfg in CONFIGS.items():
         if names and name not in names:
             continue
