@@ -4,9 +4,11 @@
 //
 // Layout: psi[rhs][n][spin] complex (double2 or float2), n = x*Nt + t; U[n][mu].
 #include <cstdlib>
+#include <type_traits>
 
 #include "kernels.h"
 #include "sap_lean.cuh"
+#include "sap_f32.cuh"
 
 namespace amgb {
 
@@ -18,77 +20,105 @@ namespace amgb {
 //        out0 = (m0+2) p0 - (t0+t1+t2+t3)/2,  out1 = (m0+2) p1 - (-t0 - i t1 + t2 + i t3)/2
 //   D^+: the (1 -/+ sigma) projectors swap between forward and backward hops.
 // ---------------------------------------------------------------------------------
-template <typename T, bool DAG>
-__device__ __forceinline__ void dirac_site(const cx<T>* __restrict__ U, const cx<T>* __restrict__ psi,
-                                           int n, int nx, int nt, T mass, cx<T>& o0, cx<T>& o1) {
+// The geometry and links of one site, loaded once and reused for every source.
+template <typename T>
+struct SiteOp {
+    int r0, r1, l0, l1;        // neighbours n+t, n+x, n-t, n-x
+    cx<T> u0, u1, ul0, ul1;    // U_0(n), U_1(n), conj(U_0(n-t)), conj(U_1(n-x))
+    T sR, sL;                  // antiperiodic signs of the two time hops
+};
+
+template <typename T>
+__device__ __forceinline__ SiteOp<T> site_op(const cx<T>* __restrict__ U, int n, int nx, int nt) {
+    SiteOp<T> o;
     const int x = n / nt, t = n - x * nt;
-    const int r0 = x * nt + ((t + 1 == nt) ? 0 : t + 1);
-    const int r1 = ((x + 1 == nx) ? 0 : x + 1) * nt + t;
-    const int l0 = x * nt + ((t == 0) ? nt - 1 : t - 1);
-    const int l1 = ((x == 0) ? nx - 1 : x - 1) * nt + t;
-    const cx<T> u0 = U[2 * n], u1 = U[2 * n + 1];
-    const cx<T> ul0 = cconj(U[2 * l0]), ul1 = cconj(U[2 * l1 + 1]);
-    const cx<T> a = psi[2 * r0], b = psi[2 * r0 + 1];
-    const cx<T> c = psi[2 * r1], d = psi[2 * r1 + 1];
-    const cx<T> e = psi[2 * l0], f = psi[2 * l0 + 1];
-    const cx<T> g = psi[2 * l1], h = psi[2 * l1 + 1];
-    const cx<T> p0 = psi[2 * n], p1 = psi[2 * n + 1];
-    const T sR = (t == nt - 1) ? T(-1) : T(1);
-    const T sL = (t == 0) ? T(-1) : T(1);
-    cx<T> t0, t1, t2, t3;
-    if (!DAG) {
-        t0 = sR * cmul(u0, a - b);
-        t1 = cmul(u1, c + cmuli(d));
-        t2 = sL * cmul(ul0, e + f);
-        t3 = cmul(ul1, g - cmuli(h));
-        o0 = mass * p0 - T(0.5) * (t0 + t1 + t2 + t3);
-        o1 = mass * p1 - T(0.5) * ((t2 - t0) + cmuli(t3 - t1));
-    } else {
-        t0 = sL * cmul(ul0, e - f);
-        t1 = cmul(ul1, g + cmuli(h));
-        t2 = sR * cmul(u0, a + b);
-        t3 = cmul(u1, c - cmuli(d));
-        o0 = mass * p0 - T(0.5) * (t0 + t1 + t2 + t3);
-        o1 = mass * p1 - T(0.5) * ((t2 - t0) + cmuli(t3 - t1));
-    }
+    o.r0 = x * nt + ((t + 1 == nt) ? 0 : t + 1);
+    o.r1 = ((x + 1 == nx) ? 0 : x + 1) * nt + t;
+    o.l0 = x * nt + ((t == 0) ? nt - 1 : t - 1);
+    o.l1 = ((x == 0) ? nx - 1 : x - 1) * nt + t;
+    o.u0 = U[2 * n];
+    o.u1 = U[2 * n + 1];
+    o.ul0 = cconj(U[2 * o.l0]);
+    o.ul1 = cconj(U[2 * o.l1 + 1]);
+    o.sR = (t == nt - 1) ? T(-1) : T(1);
+    o.sL = (t == 0) ? T(-1) : T(1);
+    return o;
 }
 
 template <typename T, bool DAG>
+__device__ __forceinline__ void dirac_site(const SiteOp<T>& L, const cx<T>* __restrict__ psi, int n, T mass,
+                                           cx<T>& o0, cx<T>& o1) {
+    const cx<T> a = psi[2 * L.r0], b = psi[2 * L.r0 + 1];
+    const cx<T> c = psi[2 * L.r1], d = psi[2 * L.r1 + 1];
+    const cx<T> e = psi[2 * L.l0], f = psi[2 * L.l0 + 1];
+    const cx<T> g = psi[2 * L.l1], h = psi[2 * L.l1 + 1];
+    const cx<T> p0 = psi[2 * n], p1 = psi[2 * n + 1];
+    cx<T> t0, t1, t2, t3;
+    if (!DAG) {
+        t0 = L.sR * cmul(L.u0, a - b);
+        t1 = cmul(L.u1, c + cmuli(d));
+        t2 = L.sL * cmul(L.ul0, e + f);
+        t3 = cmul(L.ul1, g - cmuli(h));
+    } else {
+        t0 = L.sL * cmul(L.ul0, e - f);
+        t1 = cmul(L.ul1, g + cmuli(h));
+        t2 = L.sR * cmul(L.u0, a + b);
+        t3 = cmul(L.u1, c - cmuli(d));
+    }
+    o0 = mass * p0 - T(0.5) * (t0 + t1 + t2 + t3);
+    o1 = mass * p1 - T(0.5) * ((t2 - t0) + cmuli(t3 - t1));
+}
+
+// One thread per site; the sources rhs = blockIdx.y, blockIdx.y + gridDim.y, ... share the
+// site's links, which are read from memory once per source group instead of once per
+// source.
+template <typename T, bool DAG>
 __global__ void __launch_bounds__(256) k_dirac(const cx<T>* __restrict__ U, const cx<T>* __restrict__ in,
-                                               cx<T>* __restrict__ out, int nx, int nt, T m0) {
+                                               cx<T>* __restrict__ out, int nx, int nt, T m0, int nrhs) {
     const int N = nx * nt;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= N) return;
-    const long long off = (long long)blockIdx.y * N * 2;
-    cx<T> o0, o1;
-    dirac_site<T, DAG>(U, in + off, n, nx, nt, m0 + T(2), o0, o1);
-    out[off + 2 * n] = o0;
-    out[off + 2 * n + 1] = o1;
+    const SiteOp<T> L = site_op<T>(U, n, nx, nt);
+    for (int rhs = blockIdx.y; rhs < nrhs; rhs += gridDim.y) {
+        const long long off = (long long)rhs * N * 2;
+        cx<T> o0, o1;
+        dirac_site<T, DAG>(L, in + off, n, m0 + T(2), o0, o1);
+        out[off + 2 * n] = o0;
+        out[off + 2 * n + 1] = o1;
+    }
 }
 
-// r = b - D x, and per-CTA partial sums of |r|^2 (deterministic second stage)
+// r = b - D x, and per-CTA partial sums of |r|^2 (deterministic second stage); sources
+// grouped per thread as in k_dirac.  Inactive sources (act[rhs] == 0) are skipped.
 template <typename T>
 __global__ void __launch_bounds__(256) k_residual(const cx<T>* __restrict__ U, const cx<T>* __restrict__ b,
                                                   long long bstride, const cx<T>* __restrict__ x,
                                                   cx<T>* __restrict__ r, int nx, int nt, T m0,
-                                                  double* __restrict__ partial, const int* __restrict__ act) {
+                                                  double* __restrict__ partial, const int* __restrict__ act,
+                                                  int nrhs) {
     __shared__ double red[8];
-    if (act && !act[blockIdx.y]) return;
     const int N = nx * nt;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    const long long off = (long long)blockIdx.y * N * 2;
-    const cx<T>* bb = b + (long long)blockIdx.y * bstride;
-    double nrm = 0;
-    if (n < N) {
-        cx<T> o0, o1;
-        dirac_site<T, false>(U, x + off, n, nx, nt, m0 + T(2), o0, o1);
-        cx<T> r0 = bb[2 * n] - o0, r1 = bb[2 * n + 1] - o1;
-        r[off + 2 * n] = r0;
-        r[off + 2 * n + 1] = r1;
-        nrm = (double)cnorm2(r0) + (double)cnorm2(r1);
+    SiteOp<T> L;
+    if (n < N) L = site_op<T>(U, n, nx, nt);
+    for (int rhs = blockIdx.y; rhs < nrhs; rhs += gridDim.y) {
+        if (act && !act[rhs]) continue;
+        const long long off = (long long)rhs * N * 2;
+        const cx<T>* bb = b + (long long)rhs * bstride;
+        double nrm = 0;
+        if (n < N) {
+            cx<T> o0, o1;
+            dirac_site<T, false>(L, x + off, n, m0 + T(2), o0, o1);
+            const cx<T> r0 = bb[2 * n] - o0, r1 = bb[2 * n + 1] - o1;
+            r[off + 2 * n] = r0;
+            r[off + 2 * n + 1] = r1;
+            nrm = (double)cnorm2(r0) + (double)cnorm2(r1);
+        }
+        if (partial) {
+            nrm = cta_sum(nrm, red);
+            if (threadIdx.x == 0) partial[(long long)rhs * gridDim.x + blockIdx.x] = nrm;
+        }
     }
-    nrm = cta_sum(nrm, red);
-    if (partial && threadIdx.x == 0) partial[(long long)blockIdx.y * gridDim.x + blockIdx.x] = nrm;
 }
 
 // out[rhs] = sum_k partial[rhs][k] in a fixed order
@@ -435,13 +465,20 @@ __global__ void k_d2bf(__nv_bfloat162* __restrict__ y, const double2* __restrict
 // ---------------------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------------------
+// Source groups of the stencil kernels: enough threads to fill the GPU (about 2^18), and
+// otherwise as few groups as possible so that the links stream from memory once per group.
+static int source_groups(int nsites, int nrhs) {
+    const int want = (262144 + nsites - 1) / nsites;
+    return std::max(1, std::min(nrhs, want));
+}
+
 template <typename T>
 void launch_dirac(const cx<T>* U, const cx<T>* in, cx<T>* out, int nx, int nt, int nrhs, T m0, int dagger,
                   cudaStream_t s) {
     count_launch(1);
-    dim3 grid((nx * nt + 255) / 256, nrhs);
-    if (dagger) k_dirac<T, true><<<grid, 256, 0, s>>>(U, in, out, nx, nt, m0);
-    else k_dirac<T, false><<<grid, 256, 0, s>>>(U, in, out, nx, nt, m0);
+    dim3 grid((nx * nt + 255) / 256, source_groups(nx * nt, nrhs));
+    if (dagger) k_dirac<T, true><<<grid, 256, 0, s>>>(U, in, out, nx, nt, m0, nrhs);
+    else k_dirac<T, false><<<grid, 256, 0, s>>>(U, in, out, nx, nt, m0, nrhs);
 }
 
 template <typename T>
@@ -449,8 +486,8 @@ void launch_residual(const cx<T>* U, const cx<T>* b, long long bstride, const cx
                      int nrhs, T m0, double* partial, double* norm2_out, const int* act, cudaStream_t s) {
     count_launch(norm2_out ? 2 : 1);
     const int nblk = (nx * nt + 255) / 256;
-    dim3 grid(nblk, nrhs);
-    k_residual<T><<<grid, 256, 0, s>>>(U, b, bstride, x, r, nx, nt, m0, norm2_out ? partial : nullptr, act);
+    dim3 grid(nblk, source_groups(nx * nt, nrhs));
+    k_residual<T><<<grid, 256, 0, s>>>(U, b, bstride, x, r, nx, nt, m0, norm2_out ? partial : nullptr, act, nrhs);
     if (norm2_out) k_sum_partials<<<nrhs, 256, 0, s>>>(partial, nblk, norm2_out);
 }
 
@@ -530,14 +567,78 @@ cudaError_t launch_sap0_lean(const cx<T>* U, const cx<T>* r, cx<T>* x, const int
     return cudaGetLastError();
 }
 
-// Blocks of 64 to 1024 sites with the reference's restart length 5 take the lean kernel
-// (sap_lean.cuh); any other shape or restart length takes the generic kernel above.
+// AMG_SAP_KERNEL=lean keeps FP32 solves on the lean kernel (A/B tests); AMG_SAP_SPT=2 puts
+// two sites on each thread of the paired-FP32 kernel (twice the threads) instead of four.
+static int g_sap0_f32 = -1, g_sap0_spt = -1;
+static int sap0_f32_enabled() {
+    if (g_sap0_f32 < 0) {
+        const char* e = getenv("AMG_SAP_KERNEL");
+        g_sap0_f32 = (e && (e[0] == 'g' || e[0] == 'l')) ? 0 : 1;
+        const char* t = getenv("AMG_SAP_SPT");
+        g_sap0_spt = (t && atoi(t) == 2) ? 2 : 4;
+    }
+    return g_sap0_f32;
+}
+
+template <int SPT, int NW>
+cudaError_t launch_sap0_f32(const float2* U, const float2* r, float2* x, const int* blocks, int ncol, int nrhs, int nx,
+                            int nt, int sbt, int sxe, int ste, float m0, int restarts, float tol, int* iters,
+                            const int* act, cudaStream_t s) {
+    const int bytes = sap0_f32_smem<5, SPT, NW>();
+    cudaError_t e = cudaFuncSetAttribute(k_sap0_f32<5, SPT, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+    dim3 grid(ncol, nrhs);
+    k_sap0_f32<5, SPT, NW><<<grid, 32 * NW, bytes, s>>>(U, r, x, blocks, ncol, nx, nt, sbt, sxe, ste, m0, restarts, tol,
+                                                        act, iters);
+    return cudaGetLastError();
+}
+
+// FP32 solves of 64- to 1024-site blocks take the paired-FP32 kernel.
+static cudaError_t launch_sap0_paired(const float2* U, const float2* r, float2* x, const int* blocks, int ncol,
+                                      int nrhs, int nx, int nt, int sbt, int sxe, int ste, float m0, int restarts,
+                                      float tol, int* iters, const int* act, cudaStream_t s, bool* done) {
+    *done = true;
+    const int S = sxe * ste;
+    if (g_sap0_spt == 2) {
+        switch (S) {
+            case 64: return launch_sap0_f32<2, 1>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
+            case 128: return launch_sap0_f32<2, 2>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
+            case 256: return launch_sap0_f32<2, 4>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
+            case 512: return launch_sap0_f32<2, 8>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
+            case 1024: return launch_sap0_f32<2, 16>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
+            default: break;
+        }
+    } else {
+        switch (S) {
+            case 64: return launch_sap0_f32<2, 1>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
+            case 128: return launch_sap0_f32<4, 1>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
+            case 256: return launch_sap0_f32<4, 2>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
+            case 512: return launch_sap0_f32<4, 4>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
+            case 1024: return launch_sap0_f32<4, 8>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
+            default: break;
+        }
+    }
+    *done = false;
+    return cudaSuccess;
+}
+
+// Blocks of 64 to 1024 sites with the reference's restart length 5 take the paired-FP32
+// kernel (sap_f32.cuh) in FP32 and the lean kernel (sap_lean.cuh) in FP64; any other shape
+// or restart length takes the generic kernel above.
 template <typename T>
 cudaError_t launch_sap0(const cx<T>* U, const cx<T>* r, cx<T>* x, const int* blocks, int ncol, int nrhs, int nx,
                         int nt, int sbt, int sxe, int ste, T m0, int m, int restarts, T tol, int use_smem,
                         cx<T>* gscratch, int* iters, const int* act, cudaStream_t s) {
     count_launch(1);
     const int S = sxe * ste;
+    if constexpr (std::is_same<T, float>::value) {
+        if (m == 5 && sap0_f32_enabled()) {
+            bool done = false;
+            const cudaError_t e = launch_sap0_paired(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts,
+                                                     tol, iters, act, s, &done);
+            if (done) return e;
+        }
+    }
     if (m == 5 && sap0_warp_enabled()) {
         switch (S) {
             case 64: return launch_sap0_lean<T, 2, 1>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);

@@ -1,0 +1,308 @@
+// FP32 SAP block solve on the fine level with paired (f32x2) arithmetic: the same solve as
+// k_sap0_lean (src/sap.cpp:44-62, GMRES_D_B include/sap.h:27-47, FGMRES::fgmres
+// src/fgmres.cpp:5-115 with x0 = b), restructured for sm_100's two-wide FP32 instructions.
+//
+// A site's two spin components travel together: in shared memory a basis vector is one
+// float4 per site (spin0.re, spin1.re, spin0.im, spin1.im), so a site moves with one 16-byte
+// access, and in registers a site is a pair of f32x2 values (re = (s0.re, s1.re), im =
+// (s0.im, s1.im)).  Every Gram-Schmidt dot, axpy, norm and solution update then works on
+// both spins with one paired instruction, and each basis vector is read from shared memory
+// once per Gram-Schmidt step (kept in registers across the reduction between the dot and
+// the axpy).  The block operator D_B is evaluated per site in scalar FP32 with the four
+// neighbour indices and the four hop links (sign and 1/2 folded in, zero outside the block)
+// set up once in registers, as in k_sap0_lean.
+#pragma once
+#include "common.cuh"
+#include "sap_lean.cuh"
+
+namespace amgb {
+
+// ---- two-wide FP32 arithmetic (PTX add/sub/mul/fma .rn.f32x2, sm_100 and later) ----------
+__device__ __forceinline__ float2 p_add(float2 a, float2 b) {
+    float2 r;
+    asm("{.reg .b64 a, b, d; mov.b64 a, {%2, %3}; mov.b64 b, {%4, %5}; add.rn.f32x2 d, a, b; mov.b64 {%0, %1}, d;}"
+        : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return r;
+}
+__device__ __forceinline__ float2 p_sub(float2 a, float2 b) {
+    float2 r;
+    asm("{.reg .b64 a, b, d; mov.b64 a, {%2, %3}; mov.b64 b, {%4, %5}; sub.rn.f32x2 d, a, b; mov.b64 {%0, %1}, d;}"
+        : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return r;
+}
+__device__ __forceinline__ float2 p_mul(float2 a, float2 b) {
+    float2 r;
+    asm("{.reg .b64 a, b, d; mov.b64 a, {%2, %3}; mov.b64 b, {%4, %5}; mul.rn.f32x2 d, a, b; mov.b64 {%0, %1}, d;}"
+        : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return r;
+}
+__device__ __forceinline__ float2 p_fma(float2 a, float2 b, float2 c) {
+    float2 r;
+    asm("{.reg .b64 a, b, c, d; mov.b64 a, {%2, %3}; mov.b64 b, {%4, %5}; mov.b64 c, {%6, %7};"
+        " fma.rn.f32x2 d, a, b, c; mov.b64 {%0, %1}, d;}"
+        : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+    return r;
+}
+__device__ __forceinline__ float2 p_bc(float a) { return make_float2(a, a); }
+
+// one site, both spins
+struct SiteP {
+    float2 re, im;
+};
+__device__ __forceinline__ SiteP site_ld(const float4* __restrict__ V, int m) {
+    const float4 q = V[m];
+    return {make_float2(q.x, q.y), make_float2(q.z, q.w)};
+}
+__device__ __forceinline__ void site_st(float4* __restrict__ V, int m, const SiteP& a) {
+    V[m] = make_float4(a.re.x, a.re.y, a.im.x, a.im.y);
+}
+// a global [N][2] complex64 site (s0.re, s0.im, s1.re, s1.im) as a SiteP
+__device__ __forceinline__ SiteP site_from_global(float4 g) { return {make_float2(g.x, g.z), make_float2(g.y, g.w)}; }
+
+template <int M, int SPT, int NW>
+__global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const float2* __restrict__ U, const float2* __restrict__ r,
+                                                          float2* __restrict__ xg, const int* __restrict__ blocks,
+                                                          int ncol, int nx, int nt, int sbt, int sxe, int ste, float m0,
+                                                          int restarts, float tol, const int* __restrict__ act,
+                                                          int* __restrict__ iters_out) {
+    constexpr int TPB = 32 * NW, S = TPB * SPT;
+    extern __shared__ __align__(16) unsigned char smraw_f[];
+    const int seg = blockIdx.x, rhs = blockIdx.y;
+    if (act && !act[rhs]) return;
+    float4* V = reinterpret_cast<float4*>(smraw_f);             // [M+1][S]
+    float2* H = reinterpret_cast<float2*>(V + (M + 1) * S);     // [M][M]
+    float2* gv = H + M * M;                                     // g[M+1]
+    float2* cn = gv + (M + 1);                                  // cn[M]
+    float2* sn = cn + M;                                        // sn[M]
+    float* part = reinterpret_cast<float*>(sn + M);             // [2][NW][2]
+    int buf = 0;
+    const int tid = threadIdx.x;
+    const int block = blocks[seg];
+    const int bxi = block / sbt, bti = block - bxi * sbt;
+    const int x0 = bxi * sxe, t0 = bti * ste;
+    const long long off = (long long)rhs * nx * nt * 2;
+    const float mass = m0 + 2.0f;
+
+    // per-site set-up: neighbour local indices and the folded hop links
+    int nb[SPT][4];
+    float2 lk[SPT][4];
+    int gs[SPT];
+#pragma unroll
+    for (int k = 0; k < SPT; k++) {
+        const int m = tid + TPB * k;
+        const int mx = m / ste, mt = m - mx * ste;
+        const int t = t0 + mt, x = x0 + mx;
+        gs[k] = x * nt + t;
+        const float sR = (t == nt - 1) ? -0.5f : 0.5f;
+        const float sL = (t == 0) ? -0.5f : 0.5f;
+        int q = -1;
+        if (mt + 1 < ste) q = m + 1; else if (ste == nt) q = mx * ste;
+        nb[k][0] = q < 0 ? m : q;
+        lk[k][0] = q < 0 ? czero<float>() : sR * U[2 * gs[k]];
+        q = -1;
+        if (mx + 1 < sxe) q = m + ste; else if (sxe == nx) q = mt;
+        nb[k][1] = q < 0 ? m : q;
+        lk[k][1] = q < 0 ? czero<float>() : 0.5f * U[2 * gs[k] + 1];
+        q = -1;
+        if (mt > 0) q = m - 1; else if (ste == nt) q = mx * ste + ste - 1;
+        nb[k][2] = q < 0 ? m : q;
+        lk[k][2] = q < 0 ? czero<float>() : sL * cconj(U[2 * (x * nt + ((t == 0) ? nt - 1 : t - 1))]);
+        q = -1;
+        if (mx > 0) q = m - ste; else if (sxe == nx) q = (sxe - 1) * ste + mt;
+        nb[k][3] = q < 0 ? m : q;
+        lk[k][3] = q < 0 ? czero<float>() : 0.5f * cconj(U[2 * (((x == 0) ? nx - 1 : x - 1) * nt + t) + 1]);
+    }
+
+    // w = D_B v for this thread's sites
+    auto apply = [&](const float4* __restrict__ v, SiteP (&w)[SPT]) {
+#pragma unroll
+        for (int k = 0; k < SPT; k++) {
+            const int m = tid + TPB * k;
+            const float4 c = v[m], a = v[nb[k][0]], b = v[nb[k][1]], e = v[nb[k][2]], g = v[nb[k][3]];
+            const float2 ta = cmul(lk[k][0], make_float2(a.x - a.y, a.z - a.w));   // (1 - sigma_0) forward t
+            const float2 tb = cmul(lk[k][1], make_float2(b.x - b.w, b.z + b.y));   // (1 - sigma_1) forward x
+            const float2 tc = cmul(lk[k][2], make_float2(e.x + e.y, e.z + e.w));   // (1 + sigma_0) backward t
+            const float2 td = cmul(lk[k][3], make_float2(g.x + g.w, g.z - g.y));   // (1 + sigma_1) backward x
+            const float w0r = mass * c.x - (ta.x + tb.x + tc.x + td.x);
+            const float w0i = mass * c.z - (ta.y + tb.y + tc.y + td.y);
+            const float w1r = mass * c.y - tc.x + ta.x + td.y - tb.y;
+            const float w1i = mass * c.w - tc.y + ta.y - td.x + tb.x;
+            w[k].re = make_float2(w0r, w1r);
+            w[k].im = make_float2(w0i, w1i);
+        }
+    };
+    auto norm2 = [&](const SiteP (&a)[SPT]) -> float {
+        float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int k = 0; k < SPT; k++) {
+            acc = p_fma(a[k].re, a[k].re, acc);
+            acc = p_fma(a[k].im, a[k].im, acc);
+        }
+        return lean_sum2<float, NW>(acc.x + acc.y, 0.f, part, buf).x;
+    };
+    auto store = [&](float4* Vd, const SiteP (&a)[SPT]) {
+#pragma unroll
+        for (int k = 0; k < SPT; k++) site_st(Vd, tid + TPB * k, a[k]);
+    };
+
+    const float4* rb4 = reinterpret_cast<const float4*>(r + off);
+    SiteP x[SPT], w[SPT];
+#pragma unroll
+    for (int k = 0; k < SPT; k++) x[k] = site_from_global(__ldg(&rb4[gs[k]]));
+    // r = b - A x0 (x0 = b)
+    store(V, x);
+    const float normb = sqrtf(norm2(x));
+    lean_sync<float, NW>();
+    apply(V, w);
+#pragma unroll
+    for (int k = 0; k < SPT; k++) {
+        w[k].re = p_sub(x[k].re, w[k].re);
+        w[k].im = p_sub(x[k].im, w[k].im);
+    }
+    float err = sqrtf(norm2(w));
+    int maxit = M;
+    int ret = restarts * M;
+    for (int kk = 0; kk < restarts; kk++) {
+        {
+            const float2 inv = p_bc(1.0f / err);
+#pragma unroll
+            for (int k = 0; k < SPT; k++) {
+                w[k].re = p_mul(inv, w[k].re);
+                w[k].im = p_mul(inv, w[k].im);
+            }
+            store(V, w);
+        }
+        if (tid == 0) gv[0] = make_float2(err, 0.f);
+        lean_sync<float, NW>();
+#pragma unroll
+        for (int j = 0; j < M; j++) {
+            apply(V + j * S, w);
+            float2 col[M + 1];
+            // modified Gram-Schmidt (src/fgmres.cpp:24-32), V_i read once per step
+#pragma unroll
+            for (int i = 0; i <= j; i++) {
+                SiteP vi[SPT];
+                float2 ar = make_float2(0.f, 0.f), ai = ar, an = ar;
+#pragma unroll
+                for (int k = 0; k < SPT; k++) {
+                    vi[k] = site_ld(V + i * S, tid + TPB * k);
+                    ar = p_fma(w[k].re, vi[k].re, ar);
+                    ar = p_fma(w[k].im, vi[k].im, ar);
+                    ai = p_fma(w[k].im, vi[k].re, ai);
+                    an = p_fma(w[k].re, vi[k].im, an);
+                }
+                const float2 h = lean_sum2<float, NW>(ar.x + ar.y, (ai.x + ai.y) - (an.x + an.y), part, buf);
+                col[i] = h;
+                const float2 nhx = p_bc(-h.x), hy = p_bc(h.y), nhy = p_bc(-h.y);
+#pragma unroll
+                for (int k = 0; k < SPT; k++) {
+                    w[k].re = p_fma(nhx, vi[k].re, w[k].re);
+                    w[k].re = p_fma(hy, vi[k].im, w[k].re);
+                    w[k].im = p_fma(nhx, vi[k].im, w[k].im);
+                    w[k].im = p_fma(nhy, vi[k].re, w[k].im);
+                }
+            }
+            const float hn = sqrtf(norm2(w));
+            if (hn > 0.f) {
+                const float2 inv = p_bc(1.0f / hn);
+                SiteP t[SPT];
+#pragma unroll
+                for (int k = 0; k < SPT; k++) {
+                    t[k].re = p_mul(inv, w[k].re);
+                    t[k].im = p_mul(inv, w[k].im);
+                }
+                store(V + (j + 1) * S, t);
+            }
+            // rotation(j) (src/fgmres.cpp:90-104): warp 0 computes it, lane 0 stores it
+            lean_sync<float, NW>();
+            if (tid < 32) {
+                col[j + 1] = make_float2(hn, 0.f);
+#pragma unroll
+                for (int i = 0; i < j; i++) {
+                    const float2 c = cn[i], s = sn[i];
+                    const float2 temp = cmulc(c, col[i]) + cmulc(s, col[i + 1]);
+                    col[i + 1] = cmul(c, col[i + 1]) - cmul(s, col[i]);
+                    col[i] = temp;
+                }
+                const float den = sqrtf(cnorm2(col[j]) + cnorm2(col[j + 1]));
+                const float2 snj = make_float2(col[j + 1].x / den, col[j + 1].y / den);
+                const float2 cnj = make_float2(col[j].x / den, col[j].y / den);
+                col[j] = cmulc(cnj, col[j]) + cmulc(snj, col[j + 1]);
+                const float2 gj = gv[j];
+                if (tid == 0) {
+#pragma unroll
+                    for (int i = 0; i <= j; i++) H[i * M + j] = col[i];
+                    sn[j] = snj;
+                    cn[j] = cnj;
+                    gv[j + 1] = -cmul(snj, gj);
+                    gv[j] = cmulc(cnj, gj);
+                }
+            }
+            lean_sync<float, NW>();
+            if (sqrtf(cnorm2(gv[j + 1])) < tol * normb) {
+                maxit = j + 1;
+                break;
+            }
+        }
+        // solve_upper_triangular (src/fgmres.cpp:107-115) and x += sum eta_j V_j
+        float2 eta[M];
+#pragma unroll
+        for (int i = M - 1; i >= 0; i--) {
+            if (i >= maxit) { eta[i] = czero<float>(); continue; }
+            float2 o = gv[i];
+#pragma unroll
+            for (int jj = i + 1; jj < M; jj++)
+                if (jj < maxit) o = o - cmul(H[i * M + jj], eta[jj]);
+            eta[i] = cdiv(o, H[i * M + i]);
+        }
+#pragma unroll
+        for (int jj = 0; jj < M; jj++) {
+            if (jj >= maxit) break;
+            const float2 ex = p_bc(eta[jj].x), ey = p_bc(eta[jj].y), ney = p_bc(-eta[jj].y);
+#pragma unroll
+            for (int k = 0; k < SPT; k++) {
+                const SiteP v = site_ld(V + jj * S, tid + TPB * k);
+                x[k].re = p_fma(ex, v.re, x[k].re);
+                x[k].re = p_fma(ney, v.im, x[k].re);
+                x[k].im = p_fma(ex, v.im, x[k].im);
+                x[k].im = p_fma(ey, v.re, x[k].im);
+            }
+        }
+        // true residual r = b - A x (x staged through V1)
+        lean_sync<float, NW>();
+        store(V + S, x);
+        lean_sync<float, NW>();
+        apply(V + S, w);
+#pragma unroll
+        for (int k = 0; k < SPT; k++) {
+            const SiteP b = site_from_global(__ldg(&rb4[gs[k]]));
+            w[k].re = p_sub(b.re, w[k].re);
+            w[k].im = p_sub(b.im, w[k].im);
+        }
+        err = sqrtf(norm2(w));
+        if (err < tol * normb) {
+            ret = kk * M + maxit;
+            break;
+        }
+        lean_sync<float, NW>();
+    }
+    float4* xo = reinterpret_cast<float4*>(xg + off);
+#pragma unroll
+    for (int k = 0; k < SPT; k++) {
+        float4 o = xo[gs[k]];
+        o.x += x[k].re.x;
+        o.y += x[k].im.x;
+        o.z += x[k].re.y;
+        o.w += x[k].im.y;
+        xo[gs[k]] = o;
+    }
+    if (iters_out && tid == 0) iters_out[rhs * ncol + seg] = ret;
+}
+
+template <int M, int SPT, int NW>
+inline int sap0_f32_smem() {
+    constexpr int S = 32 * NW * SPT;
+    return (M + 1) * S * 16 + (M * M + 3 * M + 1) * 8 + 2 * NW * 2 * 4 + 16;
+}
+
+}  // namespace amgb

@@ -40,6 +40,9 @@ CONFIGS = {
     "c32_l3_k_nit1": (32, [[0, 4, 4, 6, 2, 2], [1, 2, 2, 6, 2, 2]], 2.0, -0.1, 14, {"nit": 1}, False),
     "c64_l2_k": (64, [[0, 8, 8, 10, 4, 4]], 2.0, -0.1, 1, {}, False),
     "c64_l4_k": (64, [[0, 8, 8, 8, 4, 4], [1, 4, 4, 8, 4, 4], [2, 2, 2, 8, 2, 2]], 4.0, -0.05, 15, {}, False),
+    # SAP blocks of 32x32 and 16x32 sites (the block shapes of the 1024x1024 benchmark rows)
+    "c64_l3_sap1024": (64, [[0, 8, 8, 8, 2, 2], [1, 4, 4, 8, 2, 2]], 3.0, -0.1, 16, {}, False),
+    "c64_l2_sap512": (64, [[0, 8, 8, 8, 4, 2]], 4.0, -0.05, 17, {}, False),
 }
 
 # name: (ns, rows, beta, m0, seed); inputs: theta = gauge_angles(ns, ns, beta, seed),

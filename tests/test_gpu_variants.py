@@ -1,7 +1,10 @@
 """The alternative kernel paths give the reference's results too: the generic and the lean
 fine-level SAP block solvers, and the coarse engine on one CTA or on thread-block clusters
-of 4 and 16 CTAs.  Each variant runs in its own process (the choice is read from the
-environment once per process)."""
+of 4 and 16 CTAs, in FP64; and in the mixed form (FP32 cycle inside the FP64 outer
+FGMRES) the paired-FP32 SAP kernel with four or two sites per thread and the lean kernel.
+Each variant runs in its own process (the choice is read from the environment once per
+process).  Mixed-precision bars: FP64 true residual <= 1e-10, x within 1e-8 of the
+reference's, at most one outer iteration more than the reference."""
 import json
 import os
 import subprocess
@@ -21,10 +24,10 @@ from conftest import load_golden, rel
 from oracle import restatement as R
 from amg_schwingermodel_b200 import AMGContext
 out = {{}}
-for name in ("c32_l3_k", "c64_l4_k", "c64_l2_k"):
+for name in ("c32_l3_k", "c64_l4_k", "c64_l2_k", "c64_l3_sap1024", "c64_l2_sap512"):
     g = load_golden(name); m = g["meta"]; job = m["job"]
     ctx = AMGContext(m["ns"], m["nt"], m["rows"], m["m0"], cycle=job["cycle"], nu1=job["nu1"], nu2=job["nu2"],
-                     nit=job["nit"], sap_tv_iters=job["sap_tv_iters"], max_rhs=3)
+                     nit=job["nit"], sap_tv_iters=job["sap_tv_iters"], max_rhs=3, precision={prec})
     ctx.set_gauge(g["gauge"])
     for l, W in enumerate(R.reference_initial_test_vectors(R.read_parameters(m["ns"], m["nt"], m["rows"]))):
         ctx.set_initial_test_vectors(l, W)
@@ -42,15 +45,23 @@ print("RESULT" + json.dumps(out))
 """
 
 
-@pytest.mark.parametrize("sap,cluster", [("generic", "1"), ("lean", "1"), ("lean", "4"), ("lean", "16")])
-def test_variant_matches_reference(sap, cluster):
+@pytest.mark.parametrize("sap,cluster,prec", [
+    ("generic", "1", 0), ("lean", "1", 0), ("lean", "4", 0), ("lean", "16", 0),
+    ("paired", "16", 1), ("paired2", "16", 1), ("lean", "16", 1), ("paired", "4", 1)])
+def test_variant_matches_reference(sap, cluster, prec):
     env = dict(os.environ, AMG_SAP_KERNEL=sap, AMG_ENGINE_CLUSTER=cluster)
-    code = SCRIPT.format(root=str(ROOT), tests=str(ROOT / "tests"))
+    if sap == "paired2":
+        env["AMG_SAP_SPT"] = "2"
+    code = SCRIPT.format(root=str(ROOT), tests=str(ROOT / "tests"), prec=prec)
     p = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=600)
     assert p.returncode == 0, p.stderr[-3000:]
     res = json.loads(p.stdout.split("RESULT", 1)[1])
     for name, r in res.items():
-        assert r["it"] == r["ref_it"], (name, r)
+        if prec == 0:
+            assert r["it"] == r["ref_it"], (name, r)
+            assert r["batch_err"] < 1e-12, (name, r)
+        else:
+            assert r["it"] <= r["ref_it"] + 1, (name, r)
+            assert r["batch_err"] < 1e-10, (name, r)
         assert r["err"] < 1e-8, (name, r)
-        assert r["batch_err"] < 1e-12, (name, r)
         assert r["res"] < 1e-10, (name, r)
