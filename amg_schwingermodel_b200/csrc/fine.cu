@@ -182,6 +182,111 @@ __global__ void __launch_bounds__(256) k_restrict0m(const TW* __restrict__ W, co
     }
 }
 
+// Tiled multi-source form: CTA (split, block) walks its share of the aggregation block's
+// sites in tiles of kRtTile sites.  A tile's test vectors (converted to T) and sources are
+// staged in shared memory with coalesced loads, laid out [site][spin][test vector] and
+// [site][spin][source]; each thread then accumulates a 2 x 2 tile of outputs (two test
+// vectors x two sources, one spin) over the sites of its site group, reading two adjacent
+// pairs per site.  Site groups are summed in shared memory at the end; the partials have
+// the layout of k_restrict0m, so k_restrict0_sum finishes both.
+constexpr int kRtTile = 64;
+
+__host__ __device__ inline int rt_out_tiles(int ntest, int nrhs) { return ((ntest + 1) / 2) * 2 * ((nrhs + 1) / 2); }
+
+template <typename T>
+inline int rt_smem_bytes(int ntest, int nrhs) {
+    const int K2 = 2 * ((ntest + 1) / 2), R2 = 2 * ((nrhs + 1) / 2);
+    const int tiles = kRtTile * 2 * (K2 + R2);
+    const int red = rt_out_tiles(ntest, nrhs) * 4 * (256 / rt_out_tiles(ntest, nrhs));
+    return (tiles > red ? tiles : red) * (int)sizeof(cx<T>);
+}
+
+template <typename T, typename TW>
+__global__ void __launch_bounds__(256) k_restrict0t(const TW* __restrict__ W, const cx<T>* __restrict__ v,
+                                                    cx<T>* __restrict__ partial, int nx, int nt, int bt, int xe,
+                                                    int te, int nsplit, int ntest, int nrhs) {
+    extern __shared__ __align__(16) unsigned char smraw_t[];
+    const int N = nx * nt;
+    const int split = blockIdx.x, nc = blockIdx.y, nblk = gridDim.y;
+    const int bxi = nc / bt, bti = nc - bxi * bt;
+    const int spb = xe * te;
+    const int per = (spb + nsplit - 1) / nsplit;
+    const int q0 = split * per, q1 = min(spb, q0 + per);
+    const int KP = (ntest + 1) / 2, RP = (nrhs + 1) / 2, K2 = 2 * KP, R2 = 2 * RP;
+    const int OT = KP * 2 * RP;
+    const int G = blockDim.x / OT;
+    cx<T>* Ws = reinterpret_cast<cx<T>*>(smraw_t);   // [kRtTile][2][K2]
+    cx<T>* Vs = Ws + kRtTile * 2 * K2;               // [kRtTile][2][R2]
+    const int tid = threadIdx.x;
+    const bool active = tid < OT * G;
+    const int ot = tid % OT, grp = tid / OT;
+    const int kp = ot % KP, s = (ot / KP) & 1, rp = ot / (2 * KP);
+    cx<T> acc[2][2];
+#pragma unroll
+    for (int a = 0; a < 2; a++) { acc[a][0] = czero<T>(); acc[a][1] = czero<T>(); }
+
+    for (int qt = q0; qt < q1; qt += kRtTile) {
+        const int nq = min(kRtTile, q1 - qt);
+        __syncthreads();
+        for (int idx = tid; idx < nq * K2; idx += blockDim.x) {
+            const int k = idx / nq, qq = idx - k * nq;
+            const int q = qt + qq, mx = q / te, mt = q - mx * te;
+            const long long n = (long long)(bxi * xe + mx) * nt + (bti * te + mt);
+            cx<T> w0 = czero<T>(), w1 = czero<T>();
+            if (k < ntest) {
+                w0 = ccast<T>(load_cx(W + ((long long)k * N + n) * 2));
+                w1 = ccast<T>(load_cx(W + ((long long)k * N + n) * 2 + 1));
+            }
+            Ws[(qq * 2) * K2 + k] = w0;
+            Ws[(qq * 2 + 1) * K2 + k] = w1;
+        }
+        for (int idx = tid; idx < nq * R2; idx += blockDim.x) {
+            const int r = idx / nq, qq = idx - r * nq;
+            const int q = qt + qq, mx = q / te, mt = q - mx * te;
+            const long long n = (long long)(bxi * xe + mx) * nt + (bti * te + mt);
+            cx<T> p0 = czero<T>(), p1 = czero<T>();
+            if (r < nrhs) {
+                p0 = v[(long long)r * N * 2 + 2 * n];
+                p1 = v[(long long)r * N * 2 + 2 * n + 1];
+            }
+            Vs[(qq * 2) * R2 + r] = p0;
+            Vs[(qq * 2 + 1) * R2 + r] = p1;
+        }
+        __syncthreads();
+        if (active) {
+            for (int qq = grp; qq < nq; qq += G) {
+                const cx<T>* wp = Ws + (qq * 2 + s) * K2 + 2 * kp;
+                const cx<T>* vp = Vs + (qq * 2 + s) * R2 + 2 * rp;
+                const cx<T> wa = wp[0], wb = wp[1], va = vp[0], vb = vp[1];
+                cfmac(acc[0][0], wa, va);
+                cfmac(acc[0][1], wa, vb);
+                cfmac(acc[1][0], wb, va);
+                cfmac(acc[1][1], wb, vb);
+            }
+        }
+    }
+    // sum the site groups and write this split's partials
+    __syncthreads();
+    cx<T>* red = Ws;   // [G][OT][4]
+    if (active) {
+#pragma unroll
+        for (int a = 0; a < 2; a++) {
+            red[(grp * OT + ot) * 4 + 2 * a] = acc[a][0];
+            red[(grp * OT + ot) * 4 + 2 * a + 1] = acc[a][1];
+        }
+    }
+    __syncthreads();
+    for (int o = tid; o < OT * 4; o += blockDim.x) {
+        const int t = o >> 2, a = (o >> 1) & 1, b = o & 1;
+        cx<T> sum = czero<T>();
+        for (int g = 0; g < G; g++) sum += red[(g * OT + t) * 4 + 2 * a + b];
+        const int tk = t % KP, ts = (t / KP) & 1, tr = t / (2 * KP);
+        const int k = 2 * tk + a, r = 2 * tr + b;
+        if (k < ntest && r < nrhs)
+            partial[(((long long)r * nblk + nc) * nsplit + split) * (2 * ntest) + 2 * k + ts] = sum;
+    }
+}
+
 template <typename T>
 __global__ void k_restrict0_sum(const cx<T>* __restrict__ partial, cx<T>* __restrict__ out, int nblk, int nchunk,
                                 int K1) {
@@ -362,21 +467,22 @@ __global__ void __launch_bounds__(256) k_multiaxpy(double2* __restrict__ w, cons
 // partials are reduced by k_multidot_sum in a fixed order.  Sources with act[rhs] = 0 are
 // skipped (their partials are not written).
 template <int NV>
-__global__ void __launch_bounds__(256) k_axpy_dots(double2* __restrict__ w, const double2* __restrict__ V,
-                                                   long long len, long long vstride, int nv,
-                                                   const double2* __restrict__ h, int hstride, int nd,
-                                                   const int* __restrict__ act, double2* __restrict__ partial) {
+__global__ void __launch_bounds__(256, 2) k_axpy_dots(double2* __restrict__ w, const double2* __restrict__ V,
+                                                      long long len, long long vstride, int nv,
+                                                      const double2* __restrict__ h, int hstride, int nd,
+                                                      const int* __restrict__ act, double2* __restrict__ partial) {
     __shared__ double red[8][2 * (NV + 1)];
+    __shared__ double2 hk[NV];   // the axpy coefficients, read as broadcasts (fewer live registers)
     const int rhs = blockIdx.y;
     if (act && !act[rhs]) return;
     double2* ww = w + (long long)rhs * len;
     const double2* vb = V + (long long)rhs * len;
     double ax[NV + 1], ay[NV + 1];
-    double2 hk[NV];
 #pragma unroll
     for (int k = 0; k <= NV; k++) { ax[k] = 0; ay[k] = 0; }
-#pragma unroll
-    for (int k = 0; k < NV; k++) hk[k] = (h && k < nv) ? h[(long long)rhs * hstride + k] : make_double2(0, 0);
+    if (threadIdx.x < NV)
+        hk[threadIdx.x] = (h && (int)threadIdx.x < nv) ? h[(long long)rhs * hstride + threadIdx.x] : make_double2(0, 0);
+    __syncthreads();
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (long long)gridDim.x * blockDim.x) {
         double2 a = ww[e];
         if (h) {
@@ -531,6 +637,14 @@ void launch_restrict0(const TW* W, const cx<T>* v, cx<T>* out, cx<T>* partial, i
     count_launch(2);
     const int xe = nx / bx, te = nt / bt, nblk = bx * bt;
     dim3 grid(nchunk, nblk);
+    if (rt_out_tiles(ntest, nrhs) <= 256) {
+        const int bytes = rt_smem_bytes<T>(ntest, nrhs);
+        if (bytes > 48 * 1024) cudaFuncSetAttribute(k_restrict0t<T, TW>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        k_restrict0t<T, TW><<<grid, 256, bytes, s>>>(W, v, partial, nx, nt, bt, xe, te, nchunk, ntest, nrhs);
+        dim3 g2((nblk * 2 * ntest + 127) / 128, nrhs);
+        k_restrict0_sum<T><<<g2, 128, 0, s>>>(partial, out, nblk, nchunk, 2 * ntest);
+        return;
+    }
     const int thr = nrhs >= 8 ? 256 : 32 * nrhs;
     if (ntest <= 8) k_restrict0m<T, TW, 8><<<grid, thr, 0, s>>>(W, v, partial, nx, nt, bt, xe, te, nchunk, ntest, nrhs);
     else if (ntest <= 16) k_restrict0m<T, TW, 16><<<grid, thr, 0, s>>>(W, v, partial, nx, nt, bt, xe, te, nchunk, ntest, nrhs);

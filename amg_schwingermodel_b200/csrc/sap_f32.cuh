@@ -71,10 +71,7 @@ __global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const float2* __restric
     if (act && !act[rhs]) return;
     float4* V = reinterpret_cast<float4*>(smraw_f);             // [M+1][S]
     float2* H = reinterpret_cast<float2*>(V + (M + 1) * S);     // [M][M]
-    float2* gv = H + M * M;                                     // g[M+1]
-    float2* cn = gv + (M + 1);                                  // cn[M]
-    float2* sn = cn + M;                                        // sn[M]
-    float* part = reinterpret_cast<float*>(sn + M);             // [2][NW][2]
+    float* part = reinterpret_cast<float*>(H + M * M);          // [2][NW][2]
     int buf = 0;
     const int tid = threadIdx.x;
     const int block = blocks[seg];
@@ -172,7 +169,11 @@ __global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const float2* __restric
             }
             store(V, w);
         }
-        if (tid == 0) gv[0] = make_float2(err, 0.f);
+        // The Givens rotations run redundantly in every thread (the Hessenberg column is the
+        // same in all threads after the reductions), so an Arnoldi step needs one barrier,
+        // before the next operator application reads V_{j+1}; only H goes to shared memory.
+        float2 g[M + 1], cs[M], sns[M];
+        g[0] = make_float2(err, 0.f);
         lean_sync<float, NW>();
 #pragma unroll
         for (int j = 0; j < M; j++) {
@@ -213,33 +214,26 @@ __global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const float2* __restric
                 }
                 store(V + (j + 1) * S, t);
             }
-            // rotation(j) (src/fgmres.cpp:90-104): warp 0 computes it, lane 0 stores it
-            lean_sync<float, NW>();
-            if (tid < 32) {
-                col[j + 1] = make_float2(hn, 0.f);
+            // rotation(j) (src/fgmres.cpp:90-104)
+            col[j + 1] = make_float2(hn, 0.f);
 #pragma unroll
-                for (int i = 0; i < j; i++) {
-                    const float2 c = cn[i], s = sn[i];
-                    const float2 temp = cmulc(c, col[i]) + cmulc(s, col[i + 1]);
-                    col[i + 1] = cmul(c, col[i + 1]) - cmul(s, col[i]);
-                    col[i] = temp;
-                }
-                const float den = sqrtf(cnorm2(col[j]) + cnorm2(col[j + 1]));
-                const float2 snj = make_float2(col[j + 1].x / den, col[j + 1].y / den);
-                const float2 cnj = make_float2(col[j].x / den, col[j].y / den);
-                col[j] = cmulc(cnj, col[j]) + cmulc(snj, col[j + 1]);
-                const float2 gj = gv[j];
-                if (tid == 0) {
-#pragma unroll
-                    for (int i = 0; i <= j; i++) H[i * M + j] = col[i];
-                    sn[j] = snj;
-                    cn[j] = cnj;
-                    gv[j + 1] = -cmul(snj, gj);
-                    gv[j] = cmulc(cnj, gj);
-                }
+            for (int i = 0; i < j; i++) {
+                const float2 temp = cmulc(cs[i], col[i]) + cmulc(sns[i], col[i + 1]);
+                col[i + 1] = cmul(cs[i], col[i + 1]) - cmul(sns[i], col[i]);
+                col[i] = temp;
             }
+            const float den = sqrtf(cnorm2(col[j]) + cnorm2(col[j + 1]));
+            sns[j] = make_float2(col[j + 1].x / den, col[j + 1].y / den);
+            cs[j] = make_float2(col[j].x / den, col[j].y / den);
+            col[j] = cmulc(cs[j], col[j]) + cmulc(sns[j], col[j + 1]);
+            if (tid == 0) {
+#pragma unroll
+                for (int i = 0; i <= j; i++) H[i * M + j] = col[i];
+            }
+            g[j + 1] = -cmul(sns[j], g[j]);
+            g[j] = cmulc(cs[j], g[j]);
             lean_sync<float, NW>();
-            if (sqrtf(cnorm2(gv[j + 1])) < tol * normb) {
+            if (sqrtf(cnorm2(g[j + 1])) < tol * normb) {
                 maxit = j + 1;
                 break;
             }
@@ -249,7 +243,7 @@ __global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const float2* __restric
 #pragma unroll
         for (int i = M - 1; i >= 0; i--) {
             if (i >= maxit) { eta[i] = czero<float>(); continue; }
-            float2 o = gv[i];
+            float2 o = g[i];
 #pragma unroll
             for (int jj = i + 1; jj < M; jj++)
                 if (jj < maxit) o = o - cmul(H[i * M + jj], eta[jj]);
@@ -302,7 +296,7 @@ __global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const float2* __restric
 template <int M, int SPT, int NW>
 inline int sap0_f32_smem() {
     constexpr int S = 32 * NW * SPT;
-    return (M + 1) * S * 16 + (M * M + 3 * M + 1) * 8 + 2 * NW * 2 * 4 + 16;
+    return (M + 1) * S * 16 + M * M * 8 + 2 * NW * 2 * 4 + 16;
 }
 
 }  // namespace amgb
