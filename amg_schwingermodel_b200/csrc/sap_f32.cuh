@@ -59,6 +59,49 @@ __device__ __forceinline__ void site_st(float4* __restrict__ V, int m, const Sit
 // a global [N][2] complex64 site (s0.re, s0.im, s1.re, s1.im) as a SiteP
 __device__ __forceinline__ SiteP site_from_global(float4 g) { return {make_float2(g.x, g.z), make_float2(g.y, g.w)}; }
 
+// CTA sums with paired adds: warp shuffles, one barrier, then every thread adds the NW warp
+// partials (read two at a time) in warp order.  part is a double-buffered [2][NW] float2
+// array on a 16-byte boundary, so consecutive reductions need one barrier each.
+template <int NW>
+__device__ __forceinline__ float2 psum2(float2 a, float2* part, int& buf) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        float2 b;
+        b.x = __shfl_xor_sync(0xffffffffu, a.x, o);
+        b.y = __shfl_xor_sync(0xffffffffu, a.y, o);
+        a = p_add(a, b);
+    }
+    if (NW == 1) return a;
+    float2* p = part + buf * NW;
+    if ((threadIdx.x & 31) == 0) p[threadIdx.x >> 5] = a;
+    __syncthreads();
+    const float4* p4 = reinterpret_cast<const float4*>(p);
+    float4 q = p4[0];
+    float2 sum = p_add(make_float2(q.x, q.y), make_float2(q.z, q.w));
+#pragma unroll
+    for (int k = 1; k < NW / 2; k++) {
+        q = p4[k];
+        sum = p_add(sum, make_float2(q.x, q.y));
+        sum = p_add(sum, make_float2(q.z, q.w));
+    }
+    buf ^= 1;
+    return sum;
+}
+template <int NW>
+__device__ __forceinline__ float psum1(float a, float2* part, int& buf) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if (NW == 1) return a;
+    float* p = reinterpret_cast<float*>(part + buf * NW);
+    if ((threadIdx.x & 31) == 0) p[threadIdx.x >> 5] = a;
+    __syncthreads();
+    float sum = 0.f;
+#pragma unroll
+    for (int k = 0; k < NW; k++) sum += p[k];
+    buf ^= 1;
+    return sum;
+}
+
 template <int M, int SPT, int NW>
 __global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const float2* __restrict__ U, const float2* __restrict__ r,
                                                           float2* __restrict__ xg, const int* __restrict__ blocks,
@@ -71,7 +114,7 @@ __global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const float2* __restric
     if (act && !act[rhs]) return;
     float4* V = reinterpret_cast<float4*>(smraw_f);             // [M+1][S]
     float2* H = reinterpret_cast<float2*>(V + (M + 1) * S);     // [M][M]
-    float* part = reinterpret_cast<float*>(H + M * M);          // [2][NW][2]
+    float2* part = H + ((M * M + 1) & ~1);                      // [2][NW], 16-byte aligned
     int buf = 0;
     const int tid = threadIdx.x;
     const int block = blocks[seg];
@@ -135,7 +178,7 @@ __global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const float2* __restric
             acc = p_fma(a[k].re, a[k].re, acc);
             acc = p_fma(a[k].im, a[k].im, acc);
         }
-        return lean_sum2<float, NW>(acc.x + acc.y, 0.f, part, buf).x;
+        return psum1<NW>(acc.x + acc.y, part, buf);
     };
     auto store = [&](float4* Vd, const SiteP (&a)[SPT]) {
 #pragma unroll
@@ -192,7 +235,7 @@ __global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const float2* __restric
                     ai = p_fma(w[k].im, vi[k].re, ai);
                     an = p_fma(w[k].re, vi[k].im, an);
                 }
-                const float2 h = lean_sum2<float, NW>(ar.x + ar.y, (ai.x + ai.y) - (an.x + an.y), part, buf);
+                const float2 h = psum2<NW>(make_float2(ar.x + ar.y, (ai.x + ai.y) - (an.x + an.y)), part, buf);
                 col[i] = h;
                 const float2 nhx = p_bc(-h.x), hy = p_bc(h.y), nhy = p_bc(-h.y);
 #pragma unroll
@@ -262,7 +305,9 @@ __global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const float2* __restric
                 x[k].im = p_fma(ey, v.re, x[k].im);
             }
         }
-        // true residual r = b - A x (x staged through V1)
+        // true residual r = b - A x (x staged through V1).  After the last cycle it only
+        // decides the returned iteration count, so it is skipped when nobody reads that.
+        if (kk == restarts - 1 && !iters_out) break;
         lean_sync<float, NW>();
         store(V + S, x);
         lean_sync<float, NW>();
@@ -296,7 +341,7 @@ __global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const float2* __restric
 template <int M, int SPT, int NW>
 inline int sap0_f32_smem() {
     constexpr int S = 32 * NW * SPT;
-    return (M + 1) * S * 16 + M * M * 8 + 2 * NW * 2 * 4 + 16;
+    return (M + 1) * S * 16 + ((M * M + 1) & ~1) * 8 + 2 * NW * 8 + 16;
 }
 
 }  // namespace amgb

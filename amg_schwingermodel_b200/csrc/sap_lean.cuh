@@ -269,7 +269,9 @@ __global__ void __launch_bounds__(32 * NW, (sizeof(T) == 4 ? 16 : 8) / NW) k_sap
                 cfma(x[k][1], eta[jj], Vj[S + m]);
             }
         }
-        // true residual r = b - A x (x staged through V1, r into V0)
+        // true residual r = b - A x (x staged through V1, r into V0).  After the last cycle it
+        // only decides the returned iteration count, so it is skipped when nobody reads that.
+        if (kk == restarts - 1 && !iters_out) break;
         lean_sync<T, NW>();
         store(V + 2 * S, x);
         lean_sync<T, NW>();
