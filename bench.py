@@ -96,6 +96,8 @@ class ClockSampler:
 
 
 def dist_setup():
+    """One process per GPU (torchrun env).  NCCL between GPUs; gloo when CUDA is absent
+    (the multi-rank plumbing is tested that way on CPU)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -104,8 +106,10 @@ def dist_setup():
 
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
     return world, rank, local
 
 
@@ -116,13 +120,21 @@ def barrier(world):
 
 
 def max_over_ranks(v: float, world: int) -> float:
+    """The largest of the ranks' values (device times are reported as the max over ranks)."""
     if world == 1:
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_seeds(rank: int) -> tuple[int, int]:
+    """Seeds of the gauge field and the sources of one rank: every rank solves its own
+    configuration (replicas, no data exchanged)."""
+    return 1000 + rank, 2000 + rank
 
 
 def hierarchy_for_reference(ctx) -> dict:
@@ -163,8 +175,9 @@ def run_reference(args, world, rank):
     if not ref_runner.binary(NX, NT, len(ROWS) + 1).exists():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref binary for 1024x1024 L4 not built"}))
         return
-    U = gauge_field(NX, NT, BETA, 1000)
-    b0 = gaussian_spinor(NX * NT, 2, 2000)
+    gseed, bseed = replica_seeds(0)
+    U = gauge_field(NX, NT, BETA, gseed)
+    b0 = gaussian_spinor(NX * NT, 2, bseed)
     reps = args.warmup + args.steps
     t0 = time.time()
     out = ref_runner.run(NX, NT, ROWS, U, b0, m0=M0, solve=1, dump_hierarchy=0, dphi_reps=3,
@@ -197,8 +210,9 @@ def run_ours(args, world, rank, local):
     R = args.rhs
     prec = 1 if args.precision == "mixed" else 0
     N = NX * NT
-    U = gauge_field(NX, NT, BETA, 1000 + rank)
-    b_host = gaussian_spinor(N, 2, 2000 + rank, nrhs=R)
+    gseed, bseed = replica_seeds(rank)
+    U = gauge_field(NX, NT, BETA, gseed)
+    b_host = gaussian_spinor(N, 2, bseed, nrhs=R)
     # ---- the chosen form: mixed precision, R sources per solve
     ctx = AMGContext(NX, NT, ROWS, M0, precision=prec, max_rhs=R, device=local)
     ctx.set_gauge(U)
@@ -360,7 +374,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--rhs", type=int, default=16)
+    ap.add_argument("--rhs", type=int, default=32, help="sources per batched solve (one step)")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "f64"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--ref-iterations", type=int, default=11,
