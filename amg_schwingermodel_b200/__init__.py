@@ -17,7 +17,8 @@ import numpy as np
 from . import _lib
 from ._lib import AmgError, AmgParams, AmgSolveInfo, check, default_params, lib  # noqa: F401
 
-__all__ = ["AMGContext", "AmgError", "AmgParams", "default_params", "read_parameters", "dirac_apply_raw"]
+__all__ = ["AMGContext", "AmgError", "AmgParams", "default_params", "read_parameters", "dirac_apply_raw",
+           "solve_many"]
 
 
 def _cptr(a: np.ndarray):
@@ -49,6 +50,23 @@ def dirac_apply_raw(U_ptr: int, in_ptr: int, out_ptr: int, nx: int, nt: int, nrh
     """The stand-alone FP64 stencil on caller-owned device memory (raw device pointers)."""
     check(lib().amg_dirac_apply_raw(C.c_void_p(U_ptr), C.c_void_p(in_ptr), C.c_void_p(out_ptr), nx, nt, nrhs,
                                     float(m0), int(dagger), C.c_void_p(stream)), "amg_dirac_apply_raw")
+
+
+def solve_many(ctxs, bs):
+    """amg_solve_many: the solves of several contexts (any lattice sizes) driven together.
+    bs[i] is [N_i][2] or [nrhs_i][N_i][2]; returns (xs, infos) per context."""
+    n = len(ctxs)
+    bs = [_c128(b) for b in bs]
+    xs = [np.empty_like(b) for b in bs]
+    nrhs = (C.c_int * n)(*[1 if b.ndim == 2 else b.shape[0] for b in bs])
+    infos = [(AmgSolveInfo * nrhs[i])() for i in range(n)]
+    hs = (C.c_void_p * n)(*[c._h.value for c in ctxs])
+    bp = (C.c_void_p * n)(*[b.ctypes.data for b in bs])
+    xp = (C.c_void_p * n)(*[x.ctypes.data for x in xs])
+    ip = (C.c_void_p * n)(*[C.cast(i, C.c_void_p).value for i in infos])
+    check(lib().amg_solve_many(n, hs, bp, xp, nrhs, ip), "amg_solve_many")
+    return xs, [[dict(iterations=i.iterations, converged=bool(i.converged), rel_residual=i.rel_residual)
+                 for i in inf] for inf in infos]
 
 
 class AMGContext:

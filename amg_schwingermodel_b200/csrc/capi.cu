@@ -143,6 +143,30 @@ struct DevBuf {
     template <typename X> X* as() const { return reinterpret_cast<X*>(p); }
 };
 
+// page-locked host memory, so device-to-host copies of the outer FGMRES stay asynchronous
+struct PinnedBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    PinnedBuf() = default;
+    PinnedBuf(const PinnedBuf&) = delete;
+    PinnedBuf& operator=(const PinnedBuf&) = delete;
+    ~PinnedBuf() { if (p) cudaFreeHost(p); }
+    int alloc(size_t b) {
+        if (p && bytes >= b) return AMG_OK;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaMallocHost(&p, b);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            p = nullptr;
+            return fail(AMG_ERR_NOMEM, "cudaMallocHost(%zu) failed: %s", b, cudaGetErrorString(e));
+        }
+        bytes = b;
+        return AMG_OK;
+    }
+};
+
 // per-precision state of the fine-level cycle and the engine
 template <typename T>
 struct PrecSet {
@@ -178,6 +202,8 @@ struct amg_context {
     int gauge_set = 0, setup_done = 0;
     // outer FGMRES
     DevBuf V, Z, w, x, b, partial, dots, scal, masks, etab, vf, zf, sap_flags, norms;
+    PinnedBuf hpin;                // host staging of the outer FGMRES (dots, norms, masks)
+    cudaEvent_t ev_host = nullptr; // marks the end of each queued piece of the outer FGMRES
     int Rcap = 0;
     std::vector<double> history;
     double last_setup_ms = 0, last_solve_ms = 0;
@@ -582,138 +608,200 @@ int precondition(amg_context* c, const double2* v, double2* z, int R) {
 // classical Gram-Schmidt with one re-orthogonalisation on the device; the Hessenberg
 // rotations, the triangular solve and every control decision run on the host in FP64,
 // per source exactly as the reference (maxIt carried over restart cycles).
+//
+// The solve is a state machine: issue() queues device work on the context's stream that
+// ends with a device-to-host copy into pinned memory and an event; advance() runs once that
+// event has completed, does the host part and queues the next piece.  One solve drives it
+// to the end (outer_fgmres); amg_solve_many drives several contexts in turn, so the GPU
+// runs one context's kernels while the host handles another's Givens rotations.
 // ---------------------------------------------------------------------------------
-int outer_fgmres(amg_context* c, const double2* b, double2* x, int R, amg_solve_info* info) {
-    const amg_params& p = c->p;
-    const int m = p.outer_m;
-    const long long len = vlen0(c);
-    const long long vstride = (long long)R * len;
-    double2* V = c->V.as<double2>();
-    double2* Z = c->Z.as<double2>();
-    double2* w = c->w.as<double2>();
-    double* partial = c->partial.as<double>();
-    double2* dpart = c->partial.as<double2>();
-    double2* dots = c->dots.as<double2>();
-    double* scal = c->scal.as<double>();
-    int* act_d = c->masks.as<int>();
-    int* arn_d = act_d + c->Rcap;
-    int* wm_d = arn_d + c->Rcap;
-    int* nvr_d = wm_d + c->Rcap;
-    int* ro_d = nvr_d + c->Rcap;
-    double2* eta_d = c->etab.as<double2>();
-    const double2* U = c->d.U.as<double2>();
-    const int np = std::min<long long>(592, (len + 255) / 256);
+struct OuterSolve {
+    enum Phase { INIT, STEP, RESTART, DONE };
+    amg_context* c = nullptr;
+    const double2* b = nullptr;
+    double2* x = nullptr;
+    int R = 0;
+    amg_solve_info* info = nullptr;
+    int m = 0, np = 0;
+    long long len = 0, vstride = 0;
+    std::vector<cd> H, g, cn, sn, eta;
+    std::vector<double> err, normb;
+    std::vector<int> maxit, act, arn, iters;
+    int k = 0, j = 0;
+    Phase phase = DONE;
+    int rc = AMG_OK;
+    // pinned host staging (views into c->hpin)
+    double* h_norm = nullptr;      // [2R]
+    double2* h_dots = nullptr;     // [R * (2m + 3)]
+    int* h_ro = nullptr;           // [R]
+    int* h_mask = nullptr;         // [2R]  act, arn
+    double* h_scal = nullptr;      // [R]
+    double2* h_eta = nullptr;      // [R * m]
+    int* h_nvr = nullptr;          // [R]
 
-    std::vector<cd> H((size_t)R * (m + 1) * m), g((size_t)R * (m + 1)), cn((size_t)R * m), sn((size_t)R * m),
-        eta((size_t)R * m);
-    std::vector<double> err(R), normb(R);
-    std::vector<int> maxit(R, m), act(R, 1), arn(R, 0), iters(R, p.outer_restarts * m);
-    std::vector<double> hbuf(2 * (size_t)R * (m + 2) * 3 + 2 * R);
-    c->history.clear();
+    int* act_d() const { return c->masks.as<int>(); }
+    int* arn_d() const { return act_d() + c->Rcap; }
+    int* wm_d() const { return arn_d() + c->Rcap; }
+    int* nvr_d() const { return wm_d() + c->Rcap; }
+    int* ro_d() const { return nvr_d() + c->Rcap; }
 
-    // x = x0 = 0; r = b - D x into V0
-    CK(cudaMemsetAsync(x, 0, (size_t)R * len * sizeof(double2), c->stream));
-    double* n2 = c->norms.as<double>();
-    launch_residual<double>(U, b, len, x, V, c->nx, c->nt, R, c->m0, partial, n2, nullptr, c->stream);
-    launch_norm2<double>(b, len, len, R, partial, n2 + c->Rcap, c->stream);
-    std::vector<double> hn(2 * R);
-    CK(cudaMemcpyAsync(hn.data(), n2, R * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaMemcpyAsync(hn.data() + R, n2 + c->Rcap, R * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    for (int r = 0; r < R; r++) { err[r] = std::sqrt(hn[r]); normb[r] = std::sqrt(hn[R + r]); }
-    std::vector<double> sc(R);
-    std::vector<int> hmask(4 * (size_t)R);
-
-    auto upload_masks = [&]() -> int {
-        for (int r = 0; r < R; r++) { hmask[r] = act[r]; hmask[R + r] = arn[r]; }
-        CK(cudaMemcpyAsync(act_d, hmask.data(), R * sizeof(int), cudaMemcpyHostToDevice, c->stream));
-        CK(cudaMemcpyAsync(arn_d, hmask.data() + R, R * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    int init(amg_context* c_, const double2* b_, double2* x_, int R_, amg_solve_info* info_) {
+        c = c_; b = b_; x = x_; R = R_; info = info_;
+        const amg_params& p = c->p;
+        m = p.outer_m;
+        len = vlen0(c);
+        vstride = (long long)R * len;
+        np = (int)std::min<long long>(592, (len + 255) / 256);
+        H.assign((size_t)R * (m + 1) * m, cd(0));
+        g.assign((size_t)R * (m + 1), cd(0));
+        cn.assign((size_t)R * m, cd(0));
+        sn.assign((size_t)R * m, cd(0));
+        eta.assign((size_t)R * m, cd(0));
+        err.assign(R, 0);
+        normb.assign(R, 0);
+        maxit.assign(R, m);
+        act.assign(R, 1);
+        arn.assign(R, 0);
+        iters.assign(R, p.outer_restarts * m);
+        char* hp = static_cast<char*>(c->hpin.p);
+        auto take = [&](size_t bytes) { char* q = hp; hp += (bytes + 15) & ~size_t(15); return q; };
+        h_norm = reinterpret_cast<double*>(take(2 * R * sizeof(double)));
+        h_dots = reinterpret_cast<double2*>(take((size_t)R * (2 * m + 3) * sizeof(double2)));
+        h_ro = reinterpret_cast<int*>(take(R * sizeof(int)));
+        h_mask = reinterpret_cast<int*>(take(2 * R * sizeof(int)));
+        h_scal = reinterpret_cast<double*>(take(R * sizeof(double)));
+        h_eta = reinterpret_cast<double2*>(take((size_t)R * m * sizeof(double2)));
+        h_nvr = reinterpret_cast<int*>(take(R * sizeof(int)));
+        c->history.clear();
+        // x = x0 = 0; r = b - D x into V0; |r|^2 and |b|^2 to the host
+        double2* V = c->V.as<double2>();
+        double* n2 = c->norms.as<double>();
+        double* partial = c->partial.as<double>();
+        CK(cudaMemsetAsync(x, 0, (size_t)R * len * sizeof(double2), c->stream));
+        launch_residual<double>(c->d.U.as<double2>(), b, len, x, V, c->nx, c->nt, R, c->m0, partial, n2, nullptr,
+                                c->stream);
+        launch_norm2<double>(b, len, len, R, partial, n2 + c->Rcap, c->stream);
+        CK(cudaMemcpyAsync(h_norm, n2, R * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(h_norm + R, n2 + c->Rcap, R * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaEventRecord(c->ev_host, c->stream));
+        phase = INIT;
         return AMG_OK;
-    };
+    }
 
-    for (int k = 0; k < p.outer_restarts; k++) {
+    int upload_masks() {
+        for (int r = 0; r < R; r++) { h_mask[r] = act[r]; h_mask[R + r] = arn[r]; }
+        CK(cudaMemcpyAsync(act_d(), h_mask, R * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(arn_d(), h_mask + R, R * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+        return AMG_OK;
+    }
+
+    // a new restart cycle: V0 = r / |r| for the active sources, then Arnoldi step 0
+    int begin_cycle() {
         bool any = false;
-        for (int r = 0; r < R; r++) any |= act[r];
-        if (!any) break;
+        for (int r = 0; r < R; r++) any |= act[r] != 0;
+        if (!any || k >= c->p.outer_restarts) return finish();
         for (int r = 0; r < R; r++) {
             arn[r] = act[r];
-            sc[r] = act[r] ? 1.0 / err[r] : 0.0;
+            h_scal[r] = act[r] ? 1.0 / err[r] : 0.0;
             if (act[r]) g[(size_t)r * (m + 1)] = cd(err[r], 0);
         }
         CKR(upload_masks());
-        CK(cudaMemcpyAsync(scal, sc.data(), R * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-        launch_scale(V, V, len, scal, act_d, R, c->stream);
-        for (int j = 0; j < m; j++) {
-            bool anyarn = false;
-            for (int r = 0; r < R; r++) anyarn |= arn[r];
-            if (!anyarn) break;
-            double2* Vj = V + (long long)j * vstride;
-            double2* Zj = Z + (long long)j * vstride;
-            CKR(precondition(c, Vj, Zj, R));
-            {
-                ProfScope ps_(c, AMG_PROF_FINE_OP, (double)c->N * (2.0 + 4.0 * R) * sizeof(double2));
-                launch_dirac<double>(U, Zj, w, c->nx, c->nt, R, c->m0, 0, c->stream);
-            }
-            const int nv = j + 1;
-            double2* d1 = dots;
-            double2* d2 = dots + (size_t)R * (nv + 1);
-            double2* d3 = d2 + (size_t)R * (nv + 1);
-            {
-                // classical Gram-Schmidt, re-orthogonalised only where the first pass cancelled
-                ProfScope ps_(c, AMG_PROF_BLAS, (double)R * len * sizeof(double2) * (2.0 * (nv + 1) + 4.0));
-                launch_multidot(w, V, len, vstride, nv, R, dpart, np, d1, arn_d, c->stream);
-                launch_axpy_multidot(w, V, len, vstride, nv, d1, nv + 1, nv, arn_d, R, dpart, np, d2, c->stream);
-                k_reorth_flag<<<1, 256, 0, c->stream>>>(d1, d2, nv, arn_d, ro_d, R);
-                launch_axpy_multidot(w, V, len, vstride, nv, d2, nv + 1, 0, ro_d, R, dpart, np, d3, c->stream);
-                k_inv_norm2<<<1, 256, 0, c->stream>>>(d2, d3, ro_d, nv, scal, arn_d, wm_d, R);
-                count_launch(2);
-                launch_scale(V + (long long)(j + 1) * vstride, w, len, scal, wm_d, R, c->stream);
-            }
-            std::vector<double2> hd((size_t)R * (2 * (nv + 1) + 1));
-            std::vector<int> ro(R);
-            CK(cudaMemcpyAsync(hd.data(), dots, hd.size() * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
-            CK(cudaMemcpyAsync(ro.data(), ro_d, R * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-            CK(cudaStreamSynchronize(c->stream));
-            for (int r = 0; r < R; r++) {
-                if (!arn[r]) continue;
-                cd* Hr = &H[(size_t)r * (m + 1) * m];
-                cd* cnr = &cn[(size_t)r * m];
-                cd* snr = &sn[(size_t)r * m];
-                cd* gr = &g[(size_t)r * (m + 1)];
-                for (int i = 0; i <= j; i++) {
-                    const double2 a = hd[(size_t)r * (nv + 1) + i];
-                    const double2 bq = hd[(size_t)R * (nv + 1) + (size_t)r * (nv + 1) + i];
-                    Hr[i * m + j] = ro[r] ? cd(a.x + bq.x, a.y + bq.y) : cd(a.x, a.y);
-                }
-                const double hn2 = ro[r] ? hd[(size_t)2 * R * (nv + 1) + r].x
-                                         : hd[(size_t)R * (nv + 1) + (size_t)r * (nv + 1) + nv].x;
-                Hr[(j + 1) * m + j] = cd(std::sqrt(hn2), 0);
-                // rotation(j) (src/fgmres.cpp:90-104)
-                for (int i = 0; i < j; i++) {
-                    cd temp = std::conj(cnr[i]) * Hr[i * m + j] + std::conj(snr[i]) * Hr[(i + 1) * m + j];
-                    Hr[(i + 1) * m + j] = -snr[i] * Hr[i * m + j] + cnr[i] * Hr[(i + 1) * m + j];
-                    Hr[i * m + j] = temp;
-                }
-                cd den = std::sqrt(std::conj(Hr[j * m + j]) * Hr[j * m + j] +
-                                   std::conj(Hr[(j + 1) * m + j]) * Hr[(j + 1) * m + j]);
-                snr[j] = Hr[(j + 1) * m + j] / den;
-                cnr[j] = Hr[j * m + j] / den;
-                Hr[j * m + j] = std::conj(cnr[j]) * Hr[j * m + j] + std::conj(snr[j]) * Hr[(j + 1) * m + j];
-                Hr[(j + 1) * m + j] = 0.0;
-                gr[j + 1] = -snr[j] * gr[j];
-                gr[j] = std::conj(cnr[j]) * gr[j];
-                if (r == 0) c->history.push_back(std::abs(gr[j + 1]));
-                if (std::abs(gr[j + 1]) < p.outer_tol * normb[r]) {
-                    maxit[r] = j + 1;
-                    arn[r] = 0;
-                }
-            }
-            CKR(upload_masks());
+        CK(cudaMemcpyAsync(c->scal.p, h_scal, R * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        double2* V = c->V.as<double2>();
+        launch_scale(V, V, len, c->scal.as<double>(), act_d(), R, c->stream);
+        j = 0;
+        return issue_step();
+    }
+
+    // Arnoldi step j on the device: Z_j = M V_j, w = D Z_j, CGS2 against V_0..V_j,
+    // V_{j+1} = w / |w|; the Hessenberg column goes to the host
+    int issue_step() {
+        double2* V = c->V.as<double2>();
+        double2* Z = c->Z.as<double2>();
+        double2* w = c->w.as<double2>();
+        double2* dpart = c->partial.as<double2>();
+        double2* dots = c->dots.as<double2>();
+        double2* Vj = V + (long long)j * vstride;
+        double2* Zj = Z + (long long)j * vstride;
+        CKR(precondition(c, Vj, Zj, R));
+        {
+            ProfScope ps_(c, AMG_PROF_FINE_OP, (double)c->N * (2.0 + 4.0 * R) * sizeof(double2));
+            launch_dirac<double>(c->d.U.as<double2>(), Zj, w, c->nx, c->nt, R, c->m0, 0, c->stream);
         }
-        // solve_upper_triangular (src/fgmres.cpp:107-115) and x += sum eta_j Z_j
-        std::vector<double2> etah((size_t)R * m);
-        std::vector<int> nvr(R, 0);
+        const int nv = j + 1;
+        double2* d1 = dots;
+        double2* d2 = dots + (size_t)R * (nv + 1);
+        double2* d3 = d2 + (size_t)R * (nv + 1);
+        {
+            // classical Gram-Schmidt, re-orthogonalised only where the first pass cancelled
+            ProfScope ps_(c, AMG_PROF_BLAS, (double)R * len * sizeof(double2) * (2.0 * (nv + 1) + 4.0));
+            launch_multidot(w, V, len, vstride, nv, R, dpart, np, d1, arn_d(), c->stream);
+            launch_axpy_multidot(w, V, len, vstride, nv, d1, nv + 1, nv, arn_d(), R, dpart, np, d2, c->stream);
+            k_reorth_flag<<<1, 256, 0, c->stream>>>(d1, d2, nv, arn_d(), ro_d(), R);
+            launch_axpy_multidot(w, V, len, vstride, nv, d2, nv + 1, 0, ro_d(), R, dpart, np, d3, c->stream);
+            k_inv_norm2<<<1, 256, 0, c->stream>>>(d2, d3, ro_d(), nv, c->scal.as<double>(), arn_d(), wm_d(), R);
+            count_launch(2);
+            launch_scale(V + (long long)(j + 1) * vstride, w, len, c->scal.as<double>(), wm_d(), R, c->stream);
+        }
+        CK(cudaMemcpyAsync(h_dots, dots, (size_t)R * (2 * (nv + 1) + 1) * sizeof(double2), cudaMemcpyDeviceToHost,
+                           c->stream));
+        CK(cudaMemcpyAsync(h_ro, ro_d(), R * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaEventRecord(c->ev_host, c->stream));
+        phase = STEP;
+        return AMG_OK;
+    }
+
+    // the host part of Arnoldi step j: Hessenberg column, rotation(j) (src/fgmres.cpp:90-104)
+    int finish_step() {
+        const int nv = j + 1;
+        const double2* hd = h_dots;
         for (int r = 0; r < R; r++) {
+            if (!arn[r]) continue;
+            cd* Hr = &H[(size_t)r * (m + 1) * m];
+            cd* cnr = &cn[(size_t)r * m];
+            cd* snr = &sn[(size_t)r * m];
+            cd* gr = &g[(size_t)r * (m + 1)];
+            for (int i = 0; i <= j; i++) {
+                const double2 a = hd[(size_t)r * (nv + 1) + i];
+                const double2 bq = hd[(size_t)R * (nv + 1) + (size_t)r * (nv + 1) + i];
+                Hr[i * m + j] = h_ro[r] ? cd(a.x + bq.x, a.y + bq.y) : cd(a.x, a.y);
+            }
+            const double hn2 = h_ro[r] ? hd[(size_t)2 * R * (nv + 1) + r].x
+                                       : hd[(size_t)R * (nv + 1) + (size_t)r * (nv + 1) + nv].x;
+            Hr[(j + 1) * m + j] = cd(std::sqrt(hn2), 0);
+            for (int i = 0; i < j; i++) {
+                cd temp = std::conj(cnr[i]) * Hr[i * m + j] + std::conj(snr[i]) * Hr[(i + 1) * m + j];
+                Hr[(i + 1) * m + j] = -snr[i] * Hr[i * m + j] + cnr[i] * Hr[(i + 1) * m + j];
+                Hr[i * m + j] = temp;
+            }
+            cd den = std::sqrt(std::conj(Hr[j * m + j]) * Hr[j * m + j] +
+                               std::conj(Hr[(j + 1) * m + j]) * Hr[(j + 1) * m + j]);
+            snr[j] = Hr[(j + 1) * m + j] / den;
+            cnr[j] = Hr[j * m + j] / den;
+            Hr[j * m + j] = std::conj(cnr[j]) * Hr[j * m + j] + std::conj(snr[j]) * Hr[(j + 1) * m + j];
+            Hr[(j + 1) * m + j] = 0.0;
+            gr[j + 1] = -snr[j] * gr[j];
+            gr[j] = std::conj(cnr[j]) * gr[j];
+            if (r == 0) c->history.push_back(std::abs(gr[j + 1]));
+            if (std::abs(gr[j + 1]) < c->p.outer_tol * normb[r]) {
+                maxit[r] = j + 1;
+                arn[r] = 0;
+            }
+        }
+        CKR(upload_masks());
+        bool anyarn = false;
+        for (int r = 0; r < R; r++) anyarn |= arn[r] != 0;
+        if (anyarn && j + 1 < m) {
+            j++;
+            return issue_step();
+        }
+        return end_cycle();
+    }
+
+    // solve_upper_triangular (src/fgmres.cpp:107-115), x += sum eta_j Z_j, true residual
+    int end_cycle() {
+        for (int r = 0; r < R; r++) {
+            h_nvr[r] = 0;
             if (!act[r]) continue;
             const cd* Hr = &H[(size_t)r * (m + 1) * m];
             const cd* gr = &g[(size_t)r * (m + 1)];
@@ -724,36 +812,73 @@ int outer_fgmres(amg_context* c, const double2* b, double2* x, int R, amg_solve_
                 for (int jj = i + 1; jj < n; jj++) er[i] -= Hr[i * m + jj] * er[jj];
                 er[i] /= Hr[i * m + i];
             }
-            for (int i = 0; i < n; i++) etah[(size_t)r * m + i] = make_double2(er[i].real(), er[i].imag());
-            nvr[r] = n;
+            for (int i = 0; i < m; i++) h_eta[(size_t)r * m + i] = i < n ? make_double2(er[i].real(), er[i].imag())
+                                                                        : make_double2(0, 0);
+            h_nvr[r] = n;
         }
-        CK(cudaMemcpyAsync(eta_d, etah.data(), etah.size() * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
-        CK(cudaMemcpyAsync(nvr_d, nvr.data(), R * sizeof(int), cudaMemcpyHostToDevice, c->stream));
-        launch_multiaxpy_add(x, Z, len, vstride, m, eta_d, m, nvr_d, act_d, R, c->stream);
-        // true residual into V0
-        launch_residual<double>(U, b, len, x, V, c->nx, c->nt, R, c->m0, partial, n2, act_d, c->stream);
-        CK(cudaMemcpyAsync(hn.data(), n2, R * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaStreamSynchronize(c->stream));
-        for (int r = 0; r < R; r++) {
-            if (!act[r]) continue;
-            err[r] = std::sqrt(hn[r]);
-            if (err[r] < p.outer_tol * normb[r]) {
-                iters[r] = k * m + maxit[r];
-                act[r] = 0;
+        double2* eta_d = c->etab.as<double2>();
+        CK(cudaMemcpyAsync(eta_d, h_eta, (size_t)R * m * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(nvr_d(), h_nvr, R * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+        launch_multiaxpy_add(x, c->Z.as<double2>(), len, vstride, m, eta_d, m, nvr_d(), act_d(), R, c->stream);
+        double* n2 = c->norms.as<double>();
+        launch_residual<double>(c->d.U.as<double2>(), b, len, x, c->V.as<double2>(), c->nx, c->nt, R, c->m0,
+                                c->partial.as<double>(), n2, act_d(), c->stream);
+        CK(cudaMemcpyAsync(h_norm, n2, R * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaEventRecord(c->ev_host, c->stream));
+        phase = RESTART;
+        return AMG_OK;
+    }
+
+    int finish() {
+        CKL();
+        prof_harvest(c);
+        if (info)
+            for (int r = 0; r < R; r++) {
+                info[r].iterations = iters[r];
+                info[r].rel_residual = normb[r] > 0 ? err[r] / normb[r] : err[r];
+                info[r].converged = err[r] < c->p.outer_tol * normb[r];
             }
+        rc = AMG_OK;
+        for (int r = 0; r < R; r++)
+            if (act[r]) rc = AMG_NOT_CONVERGED;
+        phase = DONE;
+        return AMG_OK;
+    }
+
+    // called once the event of the queued piece has completed
+    int advance() {
+        switch (phase) {
+            case INIT:
+                for (int r = 0; r < R; r++) { err[r] = std::sqrt(h_norm[r]); normb[r] = std::sqrt(h_norm[R + r]); }
+                k = 0;
+                return begin_cycle();
+            case STEP:
+                return finish_step();
+            case RESTART:
+                for (int r = 0; r < R; r++) {
+                    if (!act[r]) continue;
+                    err[r] = std::sqrt(h_norm[r]);
+                    if (err[r] < c->p.outer_tol * normb[r]) {
+                        iters[r] = k * m + maxit[r];
+                        act[r] = 0;
+                    }
+                }
+                k++;
+                return begin_cycle();
+            default:
+                return AMG_OK;
         }
     }
-    CKL();
-    prof_harvest(c);
-    if (info)
-        for (int r = 0; r < R; r++) {
-            info[r].iterations = iters[r];
-            info[r].rel_residual = normb[r] > 0 ? err[r] / normb[r] : err[r];
-            info[r].converged = err[r] < p.outer_tol * normb[r];
-        }
-    for (int r = 0; r < R; r++)
-        if (act[r]) return AMG_NOT_CONVERGED;
-    return AMG_OK;
+};
+
+int outer_fgmres(amg_context* c, const double2* b, double2* x, int R, amg_solve_info* info) {
+    OuterSolve s;
+    CKR(s.init(c, b, x, R, info));
+    while (s.phase != OuterSolve::DONE) {
+        CK(cudaEventSynchronize(c->ev_host));
+        CKR(s.advance());
+    }
+    return s.rc;
 }
 
 int ensure_capacity(amg_context* c, int R) {
@@ -774,6 +899,8 @@ int ensure_capacity(amg_context* c, int R) {
     CKR(c->etab.alloc((size_t)Rn * m * sizeof(double2)));
     CKR(c->sap_flags.alloc((size_t)2 * Rn * sizeof(int)));
     CKR(c->norms.alloc((size_t)2 * Rn * sizeof(double)));
+    CKR(c->hpin.alloc((size_t)Rn * (2 * sizeof(double) + (2 * m + 3) * sizeof(double2) + 4 * sizeof(int) +
+                                     sizeof(double) + m * sizeof(double2)) + 8 * 16));
     c->Rcap = Rn;
     CKR(alloc_fine<double>(c, c->d, Rn));
     if (c->p.precision == AMG_PREC_MIXED) {
@@ -1082,7 +1209,8 @@ int amg_create(amg_ctx* out, int nx, int nt, int levels, const int* rows, double
     int rc = AMG_OK;
     auto bail = [&](int r) { delete c; return r; };
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess)
+        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_host, cudaEventDisableTiming) != cudaSuccess)
         return bail(fail(AMG_ERR_CUDA, "stream/event creation failed"));
     const long long len = vlen0(c);
     if ((rc = c->d.U.alloc((size_t)len * sizeof(double2))) < 0) return bail(rc);
@@ -1105,6 +1233,7 @@ int amg_destroy(amg_ctx c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->ev_host) cudaEventDestroy(c->ev_host);
     cudaStream_t s = c->stream;
     delete c;
     if (s) cudaStreamDestroy(s);
@@ -1427,6 +1556,105 @@ int amg_solve(amg_ctx c, const double* b, double* x, int nrhs, amg_solve_info* i
     if (rc < 0) return rc;
     CK(cudaMemcpyAsync(x, c->x.p, (size_t)n * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    return rc;
+}
+
+namespace {
+// capacity and engines of a context for nrhs sources (amg_solve_dev's preamble)
+int prepare_solve(amg_ctx c, int nrhs) {
+    CKR(check_ready(c, 0, true));
+    if (nrhs < 1) return fail(AMG_ERR_INVALID, "nrhs must be >= 1");
+    CKR(select_device(c));
+    if (nrhs > c->Rcap) {
+        CKR(ensure_capacity(c, nrhs));
+        CKR(build_engine<double>(c, c->d, std::max(c->d.eng_cap, nrhs)));
+        if (c->p.precision == AMG_PREC_MIXED) CKR(build_engine<float>(c, c->f, std::max(c->f.eng_cap, nrhs)));
+    }
+    return AMG_OK;
+}
+
+// several contexts' outer FGMRES solves driven in turn (see OuterSolve)
+int solve_many(int count, const amg_ctx* ctx, const double2* const* b, double2* const* x, const int* nrhs,
+               amg_solve_info* const* info) {
+    std::vector<OuterSolve> S(count);
+    for (int i = 0; i < count; i++) {
+        CKR(select_device(ctx[i]));
+        CK(cudaEventRecord(ctx[i]->ev0, ctx[i]->stream));
+        CKR(S[i].init(ctx[i], b[i], x[i], nrhs[i], info ? info[i] : nullptr));
+    }
+    for (bool busy = true; busy;) {
+        busy = false;
+        for (int i = 0; i < count; i++) {
+            if (S[i].phase == OuterSolve::DONE) continue;
+            busy = true;
+            CKR(select_device(ctx[i]));
+            CK(cudaEventSynchronize(ctx[i]->ev_host));
+            CKR(S[i].advance());
+        }
+    }
+    int rc = AMG_OK;
+    for (int i = 0; i < count; i++) {
+        amg_ctx c = ctx[i];
+        CKR(select_device(c));
+        CK(cudaEventRecord(c->ev1, c->stream));
+        CK(cudaEventSynchronize(c->ev1));
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+        c->last_solve_ms = ms;
+        int flags = 0;
+        CK(cudaMemcpy(&flags, c->d.eh.flags, sizeof(int), cudaMemcpyDeviceToHost));
+        if (flags) return fail(AMG_ERR_UNSUPPORTED, "engine of context %d reported flags %d", i, flags);
+        if (S[i].rc == AMG_NOT_CONVERGED) rc = AMG_NOT_CONVERGED;
+    }
+    return rc;
+}
+
+int check_many(int count, const amg_ctx* ctx, const void* const* b, void* const* x, const int* nrhs) {
+    if (count < 1 || !ctx || !b || !x || !nrhs) return fail(AMG_ERR_INVALID, "bad argument");
+    for (int i = 0; i < count; i++) {
+        if (!b[i] || !x[i]) return fail(AMG_ERR_INVALID, "null vector for context %d", i);
+        for (int k = 0; k < i; k++)
+            if (ctx[k] == ctx[i]) return fail(AMG_ERR_INVALID, "context %d appears twice", i);
+        CKR(prepare_solve(ctx[i], nrhs[i]));
+    }
+    return AMG_OK;
+}
+}  // namespace
+
+int amg_solve_many_dev(int count, const amg_ctx* ctx, const void* const* b_dev, void* const* x_dev, const int* nrhs,
+                       amg_solve_info* const* info) {
+    CKR(check_many(count, ctx, b_dev, x_dev, nrhs));
+    std::vector<const double2*> b(count);
+    std::vector<double2*> x(count);
+    for (int i = 0; i < count; i++) {
+        b[i] = static_cast<const double2*>(b_dev[i]);
+        x[i] = static_cast<double2*>(x_dev[i]);
+    }
+    return solve_many(count, ctx, b.data(), x.data(), nrhs, info);
+}
+
+int amg_solve_many(int count, const amg_ctx* ctx, const double* const* b, double* const* x, const int* nrhs,
+                   amg_solve_info* const* info) {
+    CKR(check_many(count, ctx, reinterpret_cast<const void* const*>(b), reinterpret_cast<void* const*>(x), nrhs));
+    std::vector<const double2*> bd(count);
+    std::vector<double2*> xd(count);
+    for (int i = 0; i < count; i++) {
+        amg_ctx c = ctx[i];
+        CKR(select_device(c));
+        const long long n = (long long)nrhs[i] * vlen0(c);
+        CK(cudaMemcpyAsync(c->b.p, b[i], (size_t)n * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+        bd[i] = c->b.as<double2>();
+        xd[i] = c->x.as<double2>();
+    }
+    const int rc = solve_many(count, ctx, bd.data(), xd.data(), nrhs, info);
+    if (rc < 0) return rc;
+    for (int i = 0; i < count; i++) {
+        amg_ctx c = ctx[i];
+        CKR(select_device(c));
+        const long long n = (long long)nrhs[i] * vlen0(c);
+        CK(cudaMemcpyAsync(x[i], c->x.p, (size_t)n * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
     return rc;
 }
 

@@ -182,6 +182,17 @@ AMG_API int amg_kcycle_fgmres(amg_ctx ctx, int level, const double* b, double* x
 AMG_API int amg_solve(amg_ctx ctx, const double* b, double* x, int nrhs, amg_solve_info* info);
 /* Same on device arrays (no host copies). */
 AMG_API int amg_solve_dev(amg_ctx ctx, const void* b_dev, void* x_dev, int nrhs, amg_solve_info* info);
+/* Solves on several contexts at once (uneven lattice sizes, different gauge fields): the
+ * outer FGMRES of every context advances in turn, each on its context's stream, so one
+ * context's kernels run while the host does another's Givens rotations.  Context i solves
+ * nrhs[i] sources b[i] -> x[i] ([nrhs][N_i][2] complex128; device pointers for _dev);
+ * info[i] (optional, or info == NULL) receives nrhs[i] results.  Every context appears at
+ * most once.  Same results as amg_solve on each context alone.  No reference counterpart:
+ * the reference solves one configuration per run (src/main.cpp:130). */
+AMG_API int amg_solve_many(int count, const amg_ctx* ctx, const double* const* b, double* const* x, const int* nrhs,
+                           amg_solve_info* const* info);
+AMG_API int amg_solve_many_dev(int count, const amg_ctx* ctx, const void* const* b_dev, void* const* x_dev,
+                               const int* nrhs, amg_solve_info* const* info);
 /* Residual history of source 0 of the last solve: |g_{j+1}| per Arnoldi step
  * (the reference's Residuals_FGMRES_*.res, src/fgmres.cpp:45, :70-79). */
 AMG_API int amg_residual_history(amg_ctx ctx, double* out, int max_len, int* len);
