@@ -9,6 +9,7 @@
 #include "kernels.h"
 #include "sap_lean.cuh"
 #include "sap_f32.cuh"
+#include "sap_ca.cuh"
 
 namespace amgb {
 
@@ -683,15 +684,34 @@ cudaError_t launch_sap0_lean(const cx<T>* U, const cx<T>* r, cx<T>* x, const int
 
 // AMG_SAP_KERNEL=lean keeps FP32 solves on the lean kernel (A/B tests); AMG_SAP_SPT=2 puts
 // two sites on each thread of the paired-FP32 kernel (twice the threads) instead of four.
-static int g_sap0_f32 = -1, g_sap0_spt = -1;
+// AMG_SAP_KERNEL=ca selects the communication-avoiding FP32 kernel (sap_ca.cuh) instead of
+// the paired-FP32 MGS kernel: it executes about a third fewer instructions, but its
+// per-step small dense algebra sits on one warp's critical path and the two measure within
+// a few percent of each other on B200, so the MGS form (the reference's arithmetic) stays
+// the default.
+static int g_sap0_f32 = -1, g_sap0_spt = -1, g_sap0_ca = -1;
 static int sap0_f32_enabled() {
     if (g_sap0_f32 < 0) {
         const char* e = getenv("AMG_SAP_KERNEL");
         g_sap0_f32 = (e && (e[0] == 'g' || e[0] == 'l')) ? 0 : 1;
+        g_sap0_ca = (e && e[0] == 'c') ? 1 : 0;
         const char* t = getenv("AMG_SAP_SPT");
         g_sap0_spt = (t && atoi(t) == 2) ? 2 : 4;
     }
     return g_sap0_f32;
+}
+
+template <int SPT, int NW>
+cudaError_t launch_sap0_ca(const float2* U, const float2* r, float2* x, const int* blocks, int ncol, int nrhs, int nx,
+                           int nt, int sbt, int sxe, int ste, float m0, int restarts, float tol, int* iters,
+                           const int* act, cudaStream_t s) {
+    const int bytes = sap0_ca_smem<SPT, NW>();
+    cudaError_t e = cudaFuncSetAttribute(k_sap0_ca<SPT, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+    dim3 grid(ncol, nrhs);
+    k_sap0_ca<SPT, NW><<<grid, 32 * NW, bytes, s>>>(U, r, x, blocks, ncol, nx, nt, sbt, sxe, ste, m0, restarts, tol, act,
+                                                    iters);
+    return cudaGetLastError();
 }
 
 template <int SPT, int NW>
@@ -713,6 +733,16 @@ static cudaError_t launch_sap0_paired(const float2* U, const float2* r, float2* 
                                       float tol, int* iters, const int* act, cudaStream_t s, bool* done) {
     *done = true;
     const int S = sxe * ste;
+    if (g_sap0_ca) {
+        switch (S) {
+            case 64: return launch_sap0_ca<2, 1>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
+            case 128: return launch_sap0_ca<4, 1>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
+            case 256: return launch_sap0_ca<4, 2>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
+            case 512: return launch_sap0_ca<4, 4>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
+            case 1024: return launch_sap0_ca<4, 8>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
+            default: break;
+        }
+    }
     if (g_sap0_spt == 2) {
         switch (S) {
             case 64: return launch_sap0_f32<2, 1>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
