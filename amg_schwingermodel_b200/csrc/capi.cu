@@ -8,6 +8,8 @@
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <map>
+#include <tuple>
 #include <random>
 #include <string>
 #include <vector>
@@ -215,7 +217,18 @@ struct amg_context {
     struct Pending { int slot; cudaEvent_t a, b; double bytes; };
     std::vector<Pending> prof_pending;
     std::vector<cudaEvent_t> ev_pool;
+    // the preconditioner (one K- or V-cycle from the fine level) as CUDA graphs, one per
+    // (precision path, sources, input, output); built on a key's second use, replayed after
+    struct GraphEntry { int uses = 0; cudaGraphExec_t exec = nullptr; long long launches = 0; };
+    std::map<std::tuple<int, int, const void*, void*>, GraphEntry> graphs;
+    int graphs_off = 0;            // capture failed once: run eagerly from then on
+    void drop_graphs() {
+        for (auto& kv : graphs)
+            if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+        graphs.clear();
+    }
     ~amg_context() {
+        drop_graphs();
         for (auto& p : prof_pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
         for (auto e : ev_pool) cudaEventDestroy(e);
     }
@@ -314,6 +327,7 @@ int engine_cluster_limit() {
 // ---------------------------------------------------------------------------------
 template <typename T>
 int build_engine(amg_context* c, PrecSet<T>& ps, int nsrc) {
+    c->drop_graphs();   // captured cycles hold the old engine arguments
     const amg_params& p = c->p;
     EngArgs<T>& a = ps.eh;
     memset(&a, 0, sizeof a);
@@ -586,17 +600,65 @@ int fine_cycle(amg_context* c, PrecSet<T>& ps, const cx<T>* eta, cx<T>* psi, int
 }
 
 // FGMRES_AMG::preconditioner (include/amg.h:134-144): out = 0, then one cycle
+// AMG_GRAPHS=0 runs the cycles eagerly (A/B tests)
+int graphs_enabled() {
+    static int on = -1;
+    if (on < 0) {
+        const char* e = getenv("AMG_GRAPHS");
+        on = (e && e[0] == '0') ? 0 : 1;
+    }
+    return on;
+}
+
+// Runs body() (launches on c->stream only, no host synchronisation) through the graph cache
+// entry `key`: eagerly on its first use (lazy allocations and attributes happen then),
+// captured into a graph on the second, replayed afterwards.  Profiling runs eagerly.
+template <class Body>
+int run_graph(amg_context* c, const std::tuple<int, int, const void*, void*>& key, Body&& body) {
+    if (!graphs_enabled() || c->graphs_off || c->prof_on) return body();
+    amg_context::GraphEntry& e = c->graphs[key];
+    if (e.exec) {
+        count_launch((int)e.launches);
+        CK(cudaGraphLaunch(e.exec, c->stream));
+        return AMG_OK;
+    }
+    if (e.uses++ == 0) return body();
+    const long long l0 = amg_launch_count();
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
+    const int rc = body();
+    cudaGraph_t g = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(c->stream, &g);
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t ei = (rc >= 0 && ec == cudaSuccess && g) ? cudaGraphInstantiate(&exec, g, 0) : cudaErrorUnknown;
+    if (g) cudaGraphDestroy(g);
+    if (rc < 0 || ec != cudaSuccess || ei != cudaSuccess) {
+        // capture did not work here: fall back to eager launches for this context
+        cudaGetLastError();
+        c->graphs_off = 1;
+        if (rc < 0) return rc;
+        return body();
+    }
+    e.exec = exec;
+    e.launches = amg_launch_count() - l0;
+    CK(cudaGraphLaunch(e.exec, c->stream));
+    return AMG_OK;
+}
+
 int precondition(amg_context* c, const double2* v, double2* z, int R) {
     const long long len = vlen0(c);
     if (c->p.precision == AMG_PREC_F64) {
-        CK(cudaMemsetAsync(z, 0, (size_t)R * len * sizeof(double2), c->stream));
-        return fine_cycle<double>(c, c->d, v, z, R, true);
+        return run_graph(c, std::make_tuple(0, R, (const void*)v, (void*)z), [&]() -> int {
+            CK(cudaMemsetAsync(z, 0, (size_t)R * len * sizeof(double2), c->stream));
+            return fine_cycle<double>(c, c->d, v, z, R, true);
+        });
     }
     float2* vf = c->vf.as<float2>();
     float2* zf = c->zf.as<float2>();
     launch_d2f(vf, v, R * len, c->stream);
-    CK(cudaMemsetAsync(zf, 0, (size_t)R * len * sizeof(float2), c->stream));
-    CKR(fine_cycle<float>(c, c->f, vf, zf, R, true));
+    CKR(run_graph(c, std::make_tuple(1, R, (const void*)vf, (void*)zf), [&]() -> int {
+        CK(cudaMemsetAsync(zf, 0, (size_t)R * len * sizeof(float2), c->stream));
+        return fine_cycle<float>(c, c->f, vf, zf, R, true);
+    }));
     launch_f2d(z, zf, R * len, c->stream);
     CKL();
     return AMG_OK;
@@ -883,6 +945,7 @@ int outer_fgmres(amg_context* c, const double2* b, double2* x, int R, amg_solve_
 
 int ensure_capacity(amg_context* c, int R) {
     if (R <= c->Rcap && c->V.p) return AMG_OK;
+    c->drop_graphs();
     const int Rn = std::max(R, c->Rcap);
     const long long len = vlen0(c);
     const int m = c->p.outer_m;
@@ -988,6 +1051,7 @@ int build_mixed(amg_context* c) {
 }
 
 int do_setup(amg_context* c) {
+    c->drop_graphs();
     if (!c->gauge_set) return fail(AMG_ERR_STATE, "set the gauge field before the set-up");
     const amg_params& p = c->p;
     const int L = c->L;
@@ -1250,6 +1314,7 @@ int amg_set_mass(amg_ctx c, double m0) {
     if (!c) return fail(AMG_ERR_INVALID, "null context");
     c->m0 = m0;
     c->setup_done = 0;
+    c->drop_graphs();
     return AMG_OK;
 }
 
@@ -1257,6 +1322,7 @@ int amg_set_cycle(amg_ctx c, int cycle) {
     if (!c) return fail(AMG_ERR_INVALID, "null context");
     if (cycle != AMG_CYCLE_K && cycle != AMG_CYCLE_V) return fail(AMG_ERR_INVALID, "cycle must be AMG_CYCLE_K or AMG_CYCLE_V");
     c->p.cycle = cycle;
+    c->drop_graphs();
     return AMG_OK;
 }
 
@@ -1275,6 +1341,7 @@ int amg_set_gauge(amg_ctx c, const double* U) {
     CK(cudaStreamSynchronize(c->stream));
     c->gauge_set = 1;
     c->setup_done = 0;
+    c->drop_graphs();
     return AMG_OK;
 }
 
