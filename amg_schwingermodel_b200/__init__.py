@@ -269,6 +269,14 @@ class AMGContext:
         check(lib().amg_force_dev(self._h, C.c_void_p(lam_ptr), C.c_void_p(x_ptr), nrhs, C.c_void_p(F_ptr)),
               "amg_force_dev")
 
+    def autotune_info(self) -> dict:
+        """The autotuner's choice (amg_autotune_info)."""
+        o = np.zeros(4, dtype=np.int32)
+        check(lib().amg_autotune_info(self._h, _cptr(o)), "amg_autotune_info")
+        names = {-1: "default", 0: "generic", 1: "lean", 2: "paired_f32", 3: "ca_f32"}
+        return dict(tuned=bool(o[0]), sap_kernel=names.get(int(o[1]), str(o[1])), engine_cluster=int(o[2]),
+                    tuned_cycle_us=int(o[3]))
+
     def residual_history(self) -> np.ndarray:
         n = C.c_int(0)
         check(lib().amg_residual_history(self._h, None, 0, C.byref(n)), "amg_residual_history")

@@ -32,7 +32,7 @@ class AmgParams(C.Structure):
         ("sap_tol", C.c_double), ("kcycle_m", C.c_int), ("kcycle_restarts", C.c_int), ("kcycle_tol", C.c_double),
         ("coarse_m", C.c_int), ("coarse_restarts", C.c_int), ("coarse_tol", C.c_double), ("outer_m", C.c_int),
         ("outer_restarts", C.c_int), ("outer_tol", C.c_double), ("precision", C.c_int), ("max_rhs", C.c_int),
-        ("tv_seed", C.c_ulonglong),
+        ("tv_seed", C.c_ulonglong), ("autotune", C.c_int),
     ]
 
 
@@ -91,6 +91,7 @@ SIGNATURES = {
     "amg_force": (_I, [_P, _P, _P, _I, _P]),
     "amg_force_dev": (_I, [_P, _P, _P, _I, _P]),
     "amg_last_timings": (_I, [_P, C.POINTER(_D), C.POINTER(_D)]),
+    "amg_autotune_info": (_I, [_P, _P]),
     "amg_profile": (_I, [_P, _I]),
     "amg_profile_query": (_I, [_P, _I, C.POINTER(_D), C.POINTER(C.c_longlong), C.POINTER(_D)]),
     "amg_launch_count": (C.c_longlong, []),

@@ -182,6 +182,7 @@ struct PrecSet {
     int eng_smem = 0, eng_cap = 0;
     int max_cluster = 1;             // largest engine cluster the slabs are sized for
     int cluster_cache[17] = {0};     // engine_max_clusters(c) + 1, 0 = not queried
+    int cluster_pick = 0;            // the autotuner's cluster size (0: largest single-wave size)
     DevBuf r0, eta1, psi1, rpart, sap_r, sap_scratch;
     int ready = 0;
 };
@@ -222,6 +223,9 @@ struct amg_context {
     struct GraphEntry { int uses = 0; cudaGraphExec_t exec = nullptr; long long launches = 0; };
     std::map<std::tuple<int, int, const void*, void*>, GraphEntry> graphs;
     int graphs_off = 0;            // capture failed once: run eagerly from then on
+    // autotuner state: the fine SAP kernel variant (-1: default) and whether it ran
+    int sap_variant = -1, tuned = 0;
+    double tuned_us = 0;
     void drop_graphs() {
         for (auto& kv : graphs)
             if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
@@ -432,6 +436,7 @@ int build_engine(amg_context* c, PrecSet<T>& ps, int nsrc) {
 // once, so one launch serves every source in a single wave.
 template <typename T>
 int pick_cluster(PrecSet<T>& ps, int nsrc) {
+    if (ps.cluster_pick > 0 && ps.cluster_pick <= ps.max_cluster) return ps.cluster_pick;
     for (int cs = ps.max_cluster; cs > 1; cs >>= 1) {
         if (!ps.cluster_cache[cs]) ps.cluster_cache[cs] = engine_max_clusters<T>(cs, ps.eng_smem) + 1;
         if (ps.cluster_cache[cs] - 1 >= nsrc) return cs;
@@ -544,7 +549,7 @@ int fine_sap(amg_context* c, PrecSet<T>& ps, const cx<T>* v, long long vstride, 
                 ProfScope ps_(c, AMG_PROF_SAP, (double)h.ncol * S * (2.0 + 6.0 * R) * sizeof(cx<T>));
                 CK(launch_sap0<T>(U, r, x, colour == 0 ? d_red : d_black, h.ncol, R, c->nx, c->nt, h.sbt, h.sxe,
                                   h.ste, m0, p.sap_gmres_m, p.sap_gmres_restarts, (T)p.sap_gmres_tol, use_smem,
-                                  scratch, nullptr, act, c->stream));
+                                  scratch, nullptr, act, c->stream, c->sap_variant));
             }
             const bool last = (colour == 1) && (it == nu - 1);
             if (last && !need_ret) break;
@@ -662,6 +667,65 @@ int precondition(amg_context* c, const double2* v, double2* z, int R) {
     launch_f2d(z, zf, R * len, c->stream);
     CKL();
     return AMG_OK;
+}
+
+// ---------------------------------------------------------------------------------
+// Autotuner: on a context's first solve, time one preconditioner application (the first
+// Krylov vector, R sources) for every fine SAP kernel variant that applies (FP32: paired,
+// communication-avoiding, lean; FP64: lean) and every engine cluster size the device can
+// schedule, and keep the fastest.  An environment override (AMG_SAP_KERNEL,
+// AMG_ENGINE_CLUSTER) fixes that dimension instead.
+// ---------------------------------------------------------------------------------
+int autotune(amg_context* c, const double2* v, double2* z, int R) {
+    c->tuned = 1;
+    if (!c->p.autotune) return AMG_OK;
+    const bool mixed = c->p.precision == AMG_PREC_MIXED;
+    std::vector<int> variants{-1};
+    if (!getenv("AMG_SAP_KERNEL") && mixed)
+        variants = {SAP_VARIANT_PAIRED, SAP_VARIANT_CA, SAP_VARIANT_LEAN};
+    int* pick = mixed ? &c->f.cluster_pick : &c->d.cluster_pick;
+    const int maxc = mixed ? c->f.max_cluster : c->d.max_cluster;
+    const int smem = mixed ? c->f.eng_smem : c->d.eng_smem;
+    std::vector<int> clusters{0};
+    if (!getenv("AMG_ENGINE_CLUSTER")) {
+        clusters.clear();
+        for (int cs = maxc; cs >= 1; cs >>= 1) {
+            const int n = cs == 1 ? 1 : (mixed ? engine_max_clusters<float>(cs, smem) : engine_max_clusters<double>(cs, smem));
+            if (n > 0) clusters.push_back(cs);
+        }
+        if (clusters.empty()) clusters.push_back(0);
+    }
+    const int graphs_was = c->graphs_off;
+    c->graphs_off = 1;
+    cudaEvent_t a = nullptr, b = nullptr;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    float best = 1e30f;
+    int bv = -1, bc = 0;
+    int rc = AMG_OK;
+    for (int vv : variants) {
+        for (int cs : clusters) {
+            c->sap_variant = vv;
+            *pick = cs;
+            if ((rc = precondition(c, v, z, R)) < 0) break;   // warm-up (attributes, lazy buffers)
+            cudaEventRecord(a, c->stream);
+            if ((rc = precondition(c, v, z, R)) < 0) break;
+            cudaEventRecord(b, c->stream);
+            cudaEventSynchronize(b);
+            float ms = 0;
+            cudaEventElapsedTime(&ms, a, b);
+            if (ms < best) { best = ms; bv = vv; bc = cs; }
+        }
+        if (rc < 0) break;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    c->graphs_off = graphs_was;
+    c->sap_variant = bv;
+    *pick = bc;
+    c->tuned_us = best < 1e29f ? 1e3 * best : 0;
+    c->drop_graphs();
+    return rc;
 }
 
 // ---------------------------------------------------------------------------------
@@ -785,6 +849,7 @@ struct OuterSolve {
         double2* dots = c->dots.as<double2>();
         double2* Vj = V + (long long)j * vstride;
         double2* Zj = Z + (long long)j * vstride;
+        if (!c->tuned && !c->prof_on) CKR(autotune(c, Vj, Zj, R));
         CKR(precondition(c, Vj, Zj, R));
         {
             ProfScope ps_(c, AMG_PROF_FINE_OP, (double)c->N * (2.0 + 4.0 * R) * sizeof(double2));
@@ -1227,6 +1292,7 @@ void amg_params_default(amg_params* p) {
     p->precision = AMG_PREC_F64;
     p->max_rhs = 1;
     p->tv_seed = 0;
+    p->autotune = 1;
 }
 
 int amg_read_parameters(const char* path, int* rows, int max_rows, int* nrows) {
@@ -1828,6 +1894,16 @@ int amg_profile_query(amg_ctx c, int slot, double* ms, long long* launches, doub
     if (ms) *ms = c->prof[slot].ms;
     if (launches) *launches = c->prof[slot].n;
     if (bytes) *bytes = c->prof[slot].bytes;
+    return AMG_OK;
+}
+
+int amg_autotune_info(amg_ctx c, int* out) {
+    if (!c || !out) return fail(AMG_ERR_INVALID, "null argument");
+    const bool mixed = c->p.precision == AMG_PREC_MIXED;
+    out[0] = c->tuned;
+    out[1] = c->sap_variant;
+    out[2] = mixed ? c->f.cluster_pick : c->d.cluster_pick;
+    out[3] = (int)c->tuned_us;
     return AMG_OK;
 }
 

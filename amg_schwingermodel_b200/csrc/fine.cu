@@ -730,10 +730,10 @@ cudaError_t launch_sap0_f32(const float2* U, const float2* r, float2* x, const i
 // FP32 solves of 64- to 1024-site blocks take the paired-FP32 kernel.
 static cudaError_t launch_sap0_paired(const float2* U, const float2* r, float2* x, const int* blocks, int ncol,
                                       int nrhs, int nx, int nt, int sbt, int sxe, int ste, float m0, int restarts,
-                                      float tol, int* iters, const int* act, cudaStream_t s, bool* done) {
+                                      float tol, int* iters, const int* act, cudaStream_t s, bool* done, bool ca) {
     *done = true;
     const int S = sxe * ste;
-    if (g_sap0_ca) {
+    if (ca) {
         switch (S) {
             case 64: return launch_sap0_ca<2, 1>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
             case 128: return launch_sap0_ca<4, 1>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
@@ -772,18 +772,25 @@ static cudaError_t launch_sap0_paired(const float2* U, const float2* r, float2* 
 template <typename T>
 cudaError_t launch_sap0(const cx<T>* U, const cx<T>* r, cx<T>* x, const int* blocks, int ncol, int nrhs, int nx,
                         int nt, int sbt, int sxe, int ste, T m0, int m, int restarts, T tol, int use_smem,
-                        cx<T>* gscratch, int* iters, const int* act, cudaStream_t s) {
+                        cx<T>* gscratch, int* iters, const int* act, cudaStream_t s, int variant) {
     count_launch(1);
     const int S = sxe * ste;
+    // variant: SAP_VARIANT_* (a context's tuned choice) or -1 for the environment's default
+    int v = variant;
+    if (v < 0) {
+        const int f32 = sap0_f32_enabled();
+        v = !sap0_warp_enabled() ? SAP_VARIANT_GENERIC : (f32 ? (g_sap0_ca ? SAP_VARIANT_CA : SAP_VARIANT_PAIRED)
+                                                               : SAP_VARIANT_LEAN);
+    }
     if constexpr (std::is_same<T, float>::value) {
-        if (m == 5 && sap0_f32_enabled()) {
+        if (m == 5 && (v == SAP_VARIANT_PAIRED || v == SAP_VARIANT_CA)) {
             bool done = false;
             const cudaError_t e = launch_sap0_paired(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts,
-                                                     tol, iters, act, s, &done);
+                                                     tol, iters, act, s, &done, v == SAP_VARIANT_CA);
             if (done) return e;
         }
     }
-    if (m == 5 && sap0_warp_enabled()) {
+    if (m == 5 && v != SAP_VARIANT_GENERIC) {
         switch (S) {
             case 64: return launch_sap0_lean<T, 2, 1>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
             case 128: return launch_sap0_lean<T, 4, 1>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
@@ -925,7 +932,7 @@ void launch_force(const double2* U, const double2* lam, const double2* x, double
     template void launch_norm2<T>(const cx<T>*, long long, long long, int, double*, double*, cudaStream_t);      \
     template int sap0_smem_bytes<T>(int, int, int);                                                              \
     template cudaError_t launch_sap0<T>(const cx<T>*, const cx<T>*, cx<T>*, const int*, int, int, int, int, int, \
-                                        int, int, T, int, int, T, int, cx<T>*, int*, const int*, cudaStream_t);
+                                        int, int, T, int, int, T, int, cx<T>*, int*, const int*, cudaStream_t, int);
 INST(double)
 INST(float)
 template void launch_restrict0<double, double2>(const double2*, const cx<double>*, cx<double>*, cx<double>*, int,

@@ -32,10 +32,13 @@ template <typename T>
 int sap0_smem_bytes(int S, int m, int use_smem);
 int sap0_warp_enabled();
 void set_sap0_warp(int on);
+// fine-level SAP block solvers: generic (any block), lean (MGS, one CTA per block), paired
+// (FP32 MGS with two-wide arithmetic), ca (FP32 communication-avoiding GMRES)
+enum { SAP_VARIANT_GENERIC = 0, SAP_VARIANT_LEAN = 1, SAP_VARIANT_PAIRED = 2, SAP_VARIANT_CA = 3 };
 template <typename T>
 cudaError_t launch_sap0(const cx<T>* U, const cx<T>* r, cx<T>* x, const int* blocks, int ncol, int nrhs, int nx,
                         int nt, int sbt, int sxe, int ste, T m0, int m, int restarts, T tol, int use_smem,
-                        cx<T>* gscratch, int* iters, const int* act, cudaStream_t s);
+                        cx<T>* gscratch, int* iters, const int* act, cudaStream_t s, int variant = -1);
 void launch_multidot(const double2* w, const double2* V, long long len, long long vstride, int nv, int nrhs,
                      double2* partial, int nparts, double2* out, const int* act, cudaStream_t s);
 void launch_axpy_multidot(double2* w, const double2* V, long long len, long long vstride, int nv, const double2* h,

@@ -244,6 +244,7 @@ def run_ours(args, world, rank, local):
     resid = max(i["rel_residual"] for i in infos)
     converged = all(i["converged"] for i in infos)
     x_chosen = x_dev.cpu().numpy().view(np.complex128).reshape(R, N, 2)
+    tuned = ctx.autotune_info()
 
     # ---- per-kernel-class device time inside the same kind of step (profiled pass)
     ctx.profile(True)
@@ -345,7 +346,8 @@ def run_ours(args, world, rank, local):
             "vs_baseline": None, "dtype": "f32+bf16 inner, f64 outer" if prec else "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "lattice": [NX, NT], "levels": 4, "rows": ROWS, "nrhs_per_step": R,
                        "precision": args.precision, "beta": BETA, "m0": M0, "tol": TOL,
-                       "l2": "working set > L2 (126 MB)", "parallelism": f"replicas x{world}"},
+                       "l2": "working set > L2 (126 MB)", "parallelism": f"replicas x{world}",
+                       "autotune": tuned},
             "iterations": iters, "max_rel_residual": resid, "converged": converged,
             "err_vs_fp64": err_vs_fp64,
             "setup_s": setup_ms / 1e3,

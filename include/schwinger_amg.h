@@ -73,6 +73,9 @@ typedef struct amg_params {
     int precision;             /* AMG_PREC_F64 or AMG_PREC_MIXED */
     int max_rhs;               /* largest number of sources per solve call (buffers) */
     unsigned long long tv_seed;/* 0: the reference's draw (mt19937(50), src/amg.cpp:8-16) */
+    int autotune;              /* 1 (default): the first solve of a context times the fine SAP
+                                  kernel variants and the coarse-engine cluster sizes on its own
+                                  data and keeps the fastest; 0: fixed defaults */
 } amg_params;
 
 /* Per-source result of a solve. */
@@ -235,6 +238,10 @@ AMG_API long long amg_launch_count(void);
 AMG_API void* amg_get_stream(amg_ctx ctx);
 /* Device milliseconds of the last amg_setup / solve call (CUDA events). */
 AMG_API int amg_last_timings(amg_ctx ctx, double* setup_ms, double* solve_ms);
+/* The autotuner's choice: out[0] = 1 once tuned, out[1] = fine SAP kernel (0 generic,
+ * 1 lean, 2 paired FP32, 3 communication-avoiding FP32; -1 default), out[2] = engine cluster
+ * size (0 default), out[3] = the tuned preconditioner time in microseconds. */
+AMG_API int amg_autotune_info(amg_ctx ctx, int* out4);
 
 #ifdef __cplusplus
 }

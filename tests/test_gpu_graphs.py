@@ -26,7 +26,7 @@ out = {{}}
 for name in ("c32_l3_k", "c64_l3_sap1024"):
     g = load_golden(name); m = g["meta"]
     for prec in (0, 1):
-        ctx = AMGContext(m["ns"], m["nt"], m["rows"], m["m0"], precision=prec, max_rhs=2)
+        ctx = AMGContext(m["ns"], m["nt"], m["rows"], m["m0"], precision=prec, max_rhs=2, autotune=0)
         ctx.set_gauge(g["gauge"])
         ctx.setup()
         b = np.stack([g["rhs"], g["probe_l0"]])
