@@ -204,7 +204,7 @@ struct amg_context {
     std::vector<int> have_init;
     int gauge_set = 0, setup_done = 0;
     // outer FGMRES
-    DevBuf V, Z, w, x, b, partial, dots, scal, masks, etab, vf, zf, sap_flags, norms;
+    DevBuf V, Z, w, x, b, partial, dots, scal, masks, etab, vf, zf, vd, zd, sap_flags, norms;
     PinnedBuf hpin;                // host staging of the outer FGMRES (dots, norms, masks)
     cudaEvent_t ev_host = nullptr; // marks the end of each queued piece of the outer FGMRES
     int Rcap = 0;
@@ -652,10 +652,16 @@ int run_graph(amg_context* c, const std::tuple<int, int, const void*, void*>& ke
 int precondition(amg_context* c, const double2* v, double2* z, int R) {
     const long long len = vlen0(c);
     if (c->p.precision == AMG_PREC_F64) {
-        return run_graph(c, std::make_tuple(0, R, (const void*)v, (void*)z), [&]() -> int {
-            CK(cudaMemsetAsync(z, 0, (size_t)R * len * sizeof(double2), c->stream));
-            return fine_cycle<double>(c, c->d, v, z, R, true);
-        });
+        // staged through fixed buffers, so one graph serves every Krylov slot
+        double2* vs = c->vd.as<double2>();
+        double2* zs = c->zd.as<double2>();
+        CK(cudaMemcpyAsync(vs, v, (size_t)R * len * sizeof(double2), cudaMemcpyDeviceToDevice, c->stream));
+        CKR(run_graph(c, std::make_tuple(0, R, (const void*)vs, (void*)zs), [&]() -> int {
+            CK(cudaMemsetAsync(zs, 0, (size_t)R * len * sizeof(double2), c->stream));
+            return fine_cycle<double>(c, c->d, vs, zs, R, true);
+        }));
+        CK(cudaMemcpyAsync(z, zs, (size_t)R * len * sizeof(double2), cudaMemcpyDeviceToDevice, c->stream));
+        return AMG_OK;
     }
     float2* vf = c->vf.as<float2>();
     float2* zf = c->zf.as<float2>();
@@ -1031,6 +1037,10 @@ int ensure_capacity(amg_context* c, int R) {
                                      sizeof(double) + m * sizeof(double2)) + 8 * 16));
     c->Rcap = Rn;
     CKR(alloc_fine<double>(c, c->d, Rn));
+    if (c->p.precision == AMG_PREC_F64) {
+        CKR(c->vd.alloc((size_t)Rn * len * sizeof(double2)));
+        CKR(c->zd.alloc((size_t)Rn * len * sizeof(double2)));
+    }
     if (c->p.precision == AMG_PREC_MIXED) {
         CKR(c->vf.alloc((size_t)Rn * len * sizeof(float2)));
         CKR(c->zf.alloc((size_t)Rn * len * sizeof(float2)));

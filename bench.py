@@ -274,7 +274,8 @@ def run_ours(args, world, rank, local):
     setup64_ms = ctx64.setup()
     b1 = b_dev[0:1].contiguous()
     x1 = torch.empty_like(b1)
-    info64 = ctx64.solve_dev(b1.data_ptr(), x1.data_ptr(), 1)
+    for _ in range(max(2, args.warmup)):
+        info64 = ctx64.solve_dev(b1.data_ptr(), x1.data_ptr(), 1)
     torch.cuda.synchronize()
     s64 = torch.cuda.ExternalStream(ctx64.stream())
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -287,6 +288,7 @@ def run_ours(args, world, rank, local):
     ms64 = max_over_ranks(f0.elapsed_time(f1), world)
     fp64_value = world * n64 / (ms64 / 1e3)
     x64 = x1.cpu().numpy().view(np.complex128).reshape(N, 2)
+    tuned64 = ctx64.autotune_info()
     err_vs_fp64 = float(np.linalg.norm(x_chosen[0] - x64) / np.linalg.norm(x64))
     hierarchy = hierarchy_for_reference(ctx64) if (rank == 0 and world == 1 and not args.no_cpu) else None
     ctx64.close()
@@ -352,7 +354,8 @@ def run_ours(args, world, rank, local):
             "err_vs_fp64": err_vs_fp64,
             "setup_s": setup_ms / 1e3,
             "fp64_dropin": {"value": fp64_value, "unit": UNIT, "iterations": info64[0]["iterations"],
-                            "rel_residual": info64[0]["rel_residual"], "setup_s": setup64_ms / 1e3},
+                            "rel_residual": info64[0]["rel_residual"], "setup_s": setup64_ms / 1e3,
+                            "autotune": tuned64},
             "speedup_vs_fp64_dropin": value / fp64_value,
             "dapply": {"gbs": d_gbs, "frac": d_gbs / hbm, "peak_gbs": hbm, "peak": peak_kind,
                        "ms_per_launch": d_ms, "nrhs": nd, "bytes_per_launch": d_bytes},
