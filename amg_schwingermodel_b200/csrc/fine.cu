@@ -197,7 +197,7 @@ __host__ __device__ inline int rt_out_tiles(int ntest, int nrhs) { return ((ntes
 template <typename T>
 inline int rt_smem_bytes(int ntest, int nrhs) {
     const int K2 = 2 * ((ntest + 1) / 2), R2 = 2 * ((nrhs + 1) / 2);
-    const int tiles = kRtTile * 2 * (K2 + R2);
+    const int tiles = kRtTile * (2 * K2 + 1 + 2 * R2 + 1);
     const int red = rt_out_tiles(ntest, nrhs) * 4 * (256 / rt_out_tiles(ntest, nrhs));
     return (tiles > red ? tiles : red) * (int)sizeof(cx<T>);
 }
@@ -216,8 +216,11 @@ __global__ void __launch_bounds__(256) k_restrict0t(const TW* __restrict__ W, co
     const int KP = (ntest + 1) / 2, RP = (nrhs + 1) / 2, K2 = 2 * KP, R2 = 2 * RP;
     const int OT = KP * 2 * RP;
     const int G = blockDim.x / OT;
-    cx<T>* Ws = reinterpret_cast<cx<T>*>(smraw_t);   // [kRtTile][2][K2]
-    cx<T>* Vs = Ws + kRtTile * 2 * K2;               // [kRtTile][2][R2]
+    cx<T>* Ws = reinterpret_cast<cx<T>*>(smraw_t);   // [kRtTile][2 * K2 + 1]
+    // a site's row holds both spins plus one pad element, so the staging stores of
+    // consecutive sites (one per thread) fall in different banks
+    const int WR = 2 * K2 + 1, VR = 2 * R2 + 1;
+    cx<T>* Vs = Ws + kRtTile * WR;                   // [kRtTile][2 * R2 + 1]
     const int tid = threadIdx.x;
     const bool active = tid < OT * G;
     const int ot = tid % OT, grp = tid / OT;
@@ -238,8 +241,8 @@ __global__ void __launch_bounds__(256) k_restrict0t(const TW* __restrict__ W, co
                 w0 = ccast<T>(load_cx(W + ((long long)k * N + n) * 2));
                 w1 = ccast<T>(load_cx(W + ((long long)k * N + n) * 2 + 1));
             }
-            Ws[(qq * 2) * K2 + k] = w0;
-            Ws[(qq * 2 + 1) * K2 + k] = w1;
+            Ws[qq * WR + k] = w0;
+            Ws[qq * WR + K2 + k] = w1;
         }
         for (int idx = tid; idx < nq * R2; idx += blockDim.x) {
             const int r = idx / nq, qq = idx - r * nq;
@@ -250,14 +253,14 @@ __global__ void __launch_bounds__(256) k_restrict0t(const TW* __restrict__ W, co
                 p0 = v[(long long)r * N * 2 + 2 * n];
                 p1 = v[(long long)r * N * 2 + 2 * n + 1];
             }
-            Vs[(qq * 2) * R2 + r] = p0;
-            Vs[(qq * 2 + 1) * R2 + r] = p1;
+            Vs[qq * VR + r] = p0;
+            Vs[qq * VR + R2 + r] = p1;
         }
         __syncthreads();
         if (active) {
             for (int qq = grp; qq < nq; qq += G) {
-                const cx<T>* wp = Ws + (qq * 2 + s) * K2 + 2 * kp;
-                const cx<T>* vp = Vs + (qq * 2 + s) * R2 + 2 * rp;
+                const cx<T>* wp = Ws + qq * WR + s * K2 + 2 * kp;
+                const cx<T>* vp = Vs + qq * VR + s * R2 + 2 * rp;
                 const cx<T> wa = wp[0], wb = wp[1], va = vp[0], vb = vp[1];
                 cfmac(acc[0][0], wa, va);
                 cfmac(acc[0][1], wa, vb);
