@@ -470,8 +470,10 @@ __global__ void __launch_bounds__(256) k_multiaxpy(double2* __restrict__ w, cons
 // with the accumulators in registers (NV bounds nv and nd at compile time); per-CTA
 // partials are reduced by k_multidot_sum in a fixed order.  Sources with act[rhs] = 0 are
 // skipped (their partials are not written).
+// Up to 8 vectors two CTAs per SM fit; more vectors keep their loaded elements in registers
+// at one CTA per SM (the loads of 8 warps x 13 vectors still cover the HBM latency).
 template <int NV>
-__global__ void __launch_bounds__(256, 2) k_axpy_dots(double2* __restrict__ w, const double2* __restrict__ V,
+__global__ void __launch_bounds__(256, (NV <= 8 ? 2 : 1)) k_axpy_dots(double2* __restrict__ w, const double2* __restrict__ V,
                                                       long long len, long long vstride, int nv,
                                                       const double2* __restrict__ h, int hstride, int nd,
                                                       const int* __restrict__ act, double2* __restrict__ partial) {
@@ -487,15 +489,19 @@ __global__ void __launch_bounds__(256, 2) k_axpy_dots(double2* __restrict__ w, c
     if (threadIdx.x < NV)
         hk[threadIdx.x] = (h && (int)threadIdx.x < nv) ? h[(long long)rhs * hstride + threadIdx.x] : make_double2(0, 0);
     __syncthreads();
+    const int nload = (h && nv > nd) ? nv : nd;
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (long long)gridDim.x * blockDim.x) {
         double2 a = ww[e];
+        // every V_k element is loaded once and kept for both the update and the dots
+        double2 bk[NV];
+#pragma unroll
+        for (int k = 0; k < NV; k++) bk[k] = k < nload ? vb[(long long)k * vstride + e] : make_double2(0, 0);
         if (h) {
 #pragma unroll
             for (int k = 0; k < NV; k++) {
                 if (k < nv) {
-                    const double2 b = vb[(long long)k * vstride + e];
-                    a.x -= hk[k].x * b.x - hk[k].y * b.y;
-                    a.y -= hk[k].x * b.y + hk[k].y * b.x;
+                    a.x -= hk[k].x * bk[k].x - hk[k].y * bk[k].y;
+                    a.y -= hk[k].x * bk[k].y + hk[k].y * bk[k].x;
                 }
             }
             ww[e] = a;
@@ -503,9 +509,8 @@ __global__ void __launch_bounds__(256, 2) k_axpy_dots(double2* __restrict__ w, c
 #pragma unroll
         for (int k = 0; k < NV; k++) {
             if (k < nd) {
-                const double2 b = vb[(long long)k * vstride + e];
-                ax[k] += a.x * b.x + a.y * b.y;
-                ay[k] += a.y * b.x - a.x * b.y;
+                ax[k] += a.x * bk[k].x + a.y * bk[k].y;
+                ay[k] += a.y * bk[k].x - a.x * bk[k].y;
             }
         }
         ax[NV] += a.x * a.x + a.y * a.y;

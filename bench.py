@@ -32,6 +32,10 @@ sys.path.insert(0, str(ROOT))
 
 NX = NT = 1024
 ROWS = [[0, 8, 8, 16, 32, 32], [1, 4, 4, 16, 4, 4], [2, 2, 2, 16, 2, 2]]
+# DRAM bytes (read + write) of one fine SAP launch per (block, source) it solves, from an ncu
+# capture of this workload at 2 sources (profiles/k_sap0_f32_1024x1024_r2.md: 42.20 MB for
+# 512 blocks x 2 sources); the traffic grows with the blocks x sources a launch solves.
+SAP_DRAM_BYTES_PER_BLOCK_SOURCE = 42.197504e6 / 1024
 BETA, M0, TOL = 4.0, -0.05, 1e-10
 METRIC = "1024^2 solves/s at FP64 resid <=1e-10: mixed+batched vs FP64 GPU; D-apply GB/s"
 UNIT = "solves/s"
@@ -323,6 +327,8 @@ def run_ours(args, world, rank, local):
     per_launch_bytes = pd["bytes"] / max(pd["launches"], 1)
     achieved = per_launch_bytes / (per_launch_ms * 1e-3) / 1e9 if per_launch_ms > 0 else 0.0
     tot_prof = sum(v["ms"] for v in prof.values())
+    ncol = ROWS[0][4] * ROWS[0][5] // 2
+    sap_traffic = SAP_DRAM_BYTES_PER_BLOCK_SOURCE * ncol * R
 
     # ---- CPU baseline: the reference's own outer iteration on this workload (rank 0, N = 1)
     cpu = None
@@ -360,7 +366,9 @@ def run_ours(args, world, rank, local):
             "dapply": {"gbs": d_gbs, "frac": d_gbs / hbm, "peak_gbs": hbm, "peak": peak_kind,
                        "ms_per_launch": d_ms, "nrhs": nd, "bytes_per_launch": d_bytes},
             "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "traffic": None, "peak_kind": peak_kind,
+                         "frac": achieved / hbm, "traffic": sap_traffic if dom == "sap" else None,
+                         "traffic_source": "ncu capture at 2 sources, scaled by blocks x sources" if dom == "sap" else None,
+                         "peak_kind": peak_kind,
                          "share_of_step": pd["ms"] / tot_prof if tot_prof else None,
                          "bytes_per_launch": per_launch_bytes, "ms_per_launch": per_launch_ms},
             "kernels": prof,
