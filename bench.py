@@ -390,7 +390,7 @@ def main():
     ap.add_argument("--rhs", type=int, default=32, help="sources per batched solve (one step)")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "f64"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
-    ap.add_argument("--ref-iterations", type=int, default=11,
+    ap.add_argument("--ref-iterations", type=int, default=10,
                     help="outer iterations of the reference algorithm on this workload (FP64 drop-in count)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
