@@ -677,9 +677,9 @@ int precondition(amg_context* c, const double2* v, double2* z, int R) {
 
 // ---------------------------------------------------------------------------------
 // Autotuner: on a context's first solve, time one preconditioner application (the first
-// Krylov vector, R sources) for every fine SAP kernel variant that applies (FP32: paired,
-// communication-avoiding, lean; FP64: lean) and every engine cluster size the device can
-// schedule, and keep the fastest.  An environment override (AMG_SAP_KERNEL,
+// Krylov vector, R sources) for every fine SAP kernel variant that applies (FP32: paired
+// MGS, paired CGS, communication-avoiding, lean; FP64: lean) and every engine cluster size
+// the device can schedule, and keep the fastest.  An environment override (AMG_SAP_KERNEL,
 // AMG_ENGINE_CLUSTER) fixes that dimension instead.
 // ---------------------------------------------------------------------------------
 int autotune(amg_context* c, const double2* v, double2* z, int R) {
@@ -688,7 +688,7 @@ int autotune(amg_context* c, const double2* v, double2* z, int R) {
     const bool mixed = c->p.precision == AMG_PREC_MIXED;
     std::vector<int> variants{-1};
     if (!getenv("AMG_SAP_KERNEL") && mixed)
-        variants = {SAP_VARIANT_PAIRED, SAP_VARIANT_CA, SAP_VARIANT_LEAN};
+        variants = {SAP_VARIANT_PAIRED, SAP_VARIANT_CGS, SAP_VARIANT_CA, SAP_VARIANT_LEAN};
     int* pick = mixed ? &c->f.cluster_pick : &c->d.cluster_pick;
     const int maxc = mixed ? c->f.max_cluster : c->d.max_cluster;
     const int smem = mixed ? c->f.eng_smem : c->d.eng_smem;

@@ -4,6 +4,7 @@
 //
 // Layout: psi[rhs][n][spin] complex (double2 or float2), n = x*Nt + t; U[n][mu].
 #include <cstdlib>
+#include <cstring>
 #include <type_traits>
 
 #include "kernels.h"
@@ -634,7 +635,7 @@ static int g_sap0_warp = -1;
 int sap0_warp_enabled() {
     if (g_sap0_warp < 0) {
         const char* e = getenv("AMG_SAP_KERNEL");
-        g_sap0_warp = (e && e[0] == 'g') ? 0 : 1;
+        g_sap0_warp = (e && !strcmp(e, "generic")) ? 0 : 1;
     }
     return g_sap0_warp;
 }
@@ -696,13 +697,14 @@ cudaError_t launch_sap0_lean(const cx<T>* U, const cx<T>* r, cx<T>* x, const int
 // the paired-FP32 MGS kernel: it executes about a third fewer instructions, but its
 // per-step small dense algebra sits on one warp's critical path and the two measure within
 // a few percent of each other on B200, so the MGS form (the reference's arithmetic) stays
-// the default.
-static int g_sap0_f32 = -1, g_sap0_spt = -1, g_sap0_ca = -1;
+// the default.  AMG_SAP_KERNEL=cgs selects the paired kernel with classical Gram-Schmidt
+// (one reduction per Arnoldi step instead of j + 2, a second projection on cancellation).
+static int g_sap0_f32 = -1, g_sap0_spt = -1, g_sap0_f32_variant = -1;
 static int sap0_f32_enabled() {
     if (g_sap0_f32 < 0) {
         const char* e = getenv("AMG_SAP_KERNEL");
-        g_sap0_f32 = (e && (e[0] == 'g' || e[0] == 'l')) ? 0 : 1;
-        g_sap0_ca = (e && e[0] == 'c') ? 1 : 0;
+        g_sap0_f32 = (e && (!strcmp(e, "generic") || !strcmp(e, "lean"))) ? 0 : 1;
+        g_sap0_f32_variant = !e ? 0 : !strcmp(e, "ca") ? SAP_VARIANT_CA : !strcmp(e, "cgs") ? SAP_VARIANT_CGS : 0;
         const char* t = getenv("AMG_SAP_SPT");
         g_sap0_spt = (t && atoi(t) == 2) ? 2 : 4;
     }
@@ -722,26 +724,36 @@ cudaError_t launch_sap0_ca(const float2* U, const float2* r, float2* x, const in
     return cudaGetLastError();
 }
 
-template <int SPT, int NW>
+template <int SPT, int NW, bool CGS = false>
 cudaError_t launch_sap0_f32(const float2* U, const float2* r, float2* x, const int* blocks, int ncol, int nrhs, int nx,
                             int nt, int sbt, int sxe, int ste, float m0, int restarts, float tol, int* iters,
                             const int* act, cudaStream_t s) {
-    const int bytes = sap0_f32_smem<5, SPT, NW>();
-    cudaError_t e = cudaFuncSetAttribute(k_sap0_f32<5, SPT, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    const int bytes = sap0_f32_smem<5, SPT, NW, CGS>();
+    cudaError_t e = cudaFuncSetAttribute(k_sap0_f32<5, SPT, NW, CGS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e != cudaSuccess) return e;
     dim3 grid(ncol, nrhs);
-    k_sap0_f32<5, SPT, NW><<<grid, 32 * NW, bytes, s>>>(U, r, x, blocks, ncol, nx, nt, sbt, sxe, ste, m0, restarts, tol,
-                                                        act, iters);
+    k_sap0_f32<5, SPT, NW, CGS><<<grid, 32 * NW, bytes, s>>>(U, r, x, blocks, ncol, nx, nt, sbt, sxe, ste, m0, restarts,
+                                                             tol, act, iters);
     return cudaGetLastError();
 }
 
 // FP32 solves of 64- to 1024-site blocks take the paired-FP32 kernel.
 static cudaError_t launch_sap0_paired(const float2* U, const float2* r, float2* x, const int* blocks, int ncol,
                                       int nrhs, int nx, int nt, int sbt, int sxe, int ste, float m0, int restarts,
-                                      float tol, int* iters, const int* act, cudaStream_t s, bool* done, bool ca) {
+                                      float tol, int* iters, const int* act, cudaStream_t s, bool* done, int v) {
     *done = true;
     const int S = sxe * ste;
-    if (ca) {
+    if (v == SAP_VARIANT_CGS) {
+        switch (S) {
+            case 64: return launch_sap0_f32<2, 1, true>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
+            case 128: return launch_sap0_f32<4, 1, true>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
+            case 256: return launch_sap0_f32<4, 2, true>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
+            case 512: return launch_sap0_f32<4, 4, true>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
+            case 1024: return launch_sap0_f32<4, 8, true>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
+            default: break;
+        }
+    }
+    if (v == SAP_VARIANT_CA) {
         switch (S) {
             case 64: return launch_sap0_ca<2, 1>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
             case 128: return launch_sap0_ca<4, 1>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
@@ -787,14 +799,14 @@ cudaError_t launch_sap0(const cx<T>* U, const cx<T>* r, cx<T>* x, const int* blo
     int v = variant;
     if (v < 0) {
         const int f32 = sap0_f32_enabled();
-        v = !sap0_warp_enabled() ? SAP_VARIANT_GENERIC : (f32 ? (g_sap0_ca ? SAP_VARIANT_CA : SAP_VARIANT_PAIRED)
+        v = !sap0_warp_enabled() ? SAP_VARIANT_GENERIC : (f32 ? (g_sap0_f32_variant ? g_sap0_f32_variant : SAP_VARIANT_PAIRED)
                                                                : SAP_VARIANT_LEAN);
     }
     if constexpr (std::is_same<T, float>::value) {
-        if (m == 5 && (v == SAP_VARIANT_PAIRED || v == SAP_VARIANT_CA)) {
+        if (m == 5 && (v == SAP_VARIANT_PAIRED || v == SAP_VARIANT_CA || v == SAP_VARIANT_CGS)) {
             bool done = false;
             const cudaError_t e = launch_sap0_paired(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts,
-                                                     tol, iters, act, s, &done, v == SAP_VARIANT_CA);
+                                                     tol, iters, act, s, &done, v);
             if (done) return e;
         }
     }

@@ -33,8 +33,9 @@ int sap0_smem_bytes(int S, int m, int use_smem);
 int sap0_warp_enabled();
 void set_sap0_warp(int on);
 // fine-level SAP block solvers: generic (any block), lean (MGS, one CTA per block), paired
-// (FP32 MGS with two-wide arithmetic), ca (FP32 communication-avoiding GMRES)
-enum { SAP_VARIANT_GENERIC = 0, SAP_VARIANT_LEAN = 1, SAP_VARIANT_PAIRED = 2, SAP_VARIANT_CA = 3 };
+// (FP32 MGS with two-wide arithmetic), ca (FP32 communication-avoiding GMRES), cgs (the
+// paired kernel with classical Gram-Schmidt and re-orthogonalisation on demand)
+enum { SAP_VARIANT_GENERIC = 0, SAP_VARIANT_LEAN = 1, SAP_VARIANT_PAIRED = 2, SAP_VARIANT_CA = 3, SAP_VARIANT_CGS = 4 };
 template <typename T>
 cudaError_t launch_sap0(const cx<T>* U, const cx<T>* r, cx<T>* x, const int* blocks, int ncol, int nrhs, int nx,
                         int nt, int sbt, int sxe, int ste, T m0, int m, int restarts, T tol, int use_smem,

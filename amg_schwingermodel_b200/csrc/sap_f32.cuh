@@ -60,9 +60,10 @@ __device__ __forceinline__ void site_st(float4* __restrict__ V, int m, const Sit
 __device__ __forceinline__ SiteP site_from_global(float4 g) { return {make_float2(g.x, g.z), make_float2(g.y, g.w)}; }
 
 // CTA sums with paired adds: warp shuffles, one barrier, then every thread adds the NW warp
-// partials (read two at a time) in warp order.  part is a double-buffered [2][NW] float2
-// array on a 16-byte boundary, so consecutive reductions need one barrier each.
-template <int NW>
+// partials (read two at a time) in warp order.  part holds two buffers of STR float2 each
+// (STR >= NW, a multiple of 2) on a 16-byte boundary, so consecutive reductions need one
+// barrier each.
+template <int NW, int STR = NW>
 __device__ __forceinline__ float2 psum2(float2 a, float2* part, int& buf) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -72,7 +73,7 @@ __device__ __forceinline__ float2 psum2(float2 a, float2* part, int& buf) {
         a = p_add(a, b);
     }
     if (NW == 1) return a;
-    float2* p = part + buf * NW;
+    float2* p = part + buf * STR;
     if ((threadIdx.x & 31) == 0) p[threadIdx.x >> 5] = a;
     __syncthreads();
     const float4* p4 = reinterpret_cast<const float4*>(p);
@@ -87,12 +88,12 @@ __device__ __forceinline__ float2 psum2(float2 a, float2* part, int& buf) {
     buf ^= 1;
     return sum;
 }
-template <int NW>
+template <int NW, int STR = NW>
 __device__ __forceinline__ float psum1(float a, float2* part, int& buf) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
     if (NW == 1) return a;
-    float* p = reinterpret_cast<float*>(part + buf * NW);
+    float* p = reinterpret_cast<float*>(part + buf * STR);
     if ((threadIdx.x & 31) == 0) p[threadIdx.x >> 5] = a;
     __syncthreads();
     float sum = 0.f;
@@ -102,19 +103,69 @@ __device__ __forceinline__ float psum1(float a, float2* part, int& buf) {
     return sum;
 }
 
-template <int M, int SPT, int NW>
+// CTA sums of the first n of K complex values per thread (n is a constant once the caller's
+// loops are unrolled), every thread receiving the same sums; one barrier for all n.  A buffer
+// of part holds the values one after another, each as its NW warp partials ([K][NW] float2,
+// read two warps at a time), and the two buffers are STR float2 apart as in psum2.  The xor
+// butterfly adds the same pair in both lanes of every exchange, so with one warp every lane
+// already holds the same sums.
+template <int NW, int STR, int K>
+__device__ __forceinline__ void psum_n(float2 (&v)[K], int n, float2* part, int& buf) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+        for (int q = 0; q < K; q++) {
+            if (q < n) {
+                float2 b;
+                b.x = __shfl_xor_sync(0xffffffffu, v[q].x, o);
+                b.y = __shfl_xor_sync(0xffffffffu, v[q].y, o);
+                v[q] = p_add(v[q], b);
+            }
+        }
+    }
+    if (NW == 1) return;
+    float2* p = part + buf * STR;
+    if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+        for (int q = 0; q < K; q++)
+            if (q < n) p[q * NW + (threadIdx.x >> 5)] = v[q];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < K; q++) {
+        if (q < n) {
+            const float4* p4 = reinterpret_cast<const float4*>(p + q * NW);
+            float4 t = p4[0];
+            float2 sum = p_add(make_float2(t.x, t.y), make_float2(t.z, t.w));
+#pragma unroll
+            for (int k = 1; k < NW / 2; k++) {
+                t = p4[k];
+                sum = p_add(sum, make_float2(t.x, t.y));
+                sum = p_add(sum, make_float2(t.z, t.w));
+            }
+            v[q] = sum;
+        }
+    }
+    buf ^= 1;
+}
+
+template <int M, int SPT, int NW, bool CGS = false>
 __global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const float2* __restrict__ U, const float2* __restrict__ r,
                                                           float2* __restrict__ xg, const int* __restrict__ blocks,
                                                           int ncol, int nx, int nt, int sbt, int sxe, int ste, float m0,
                                                           int restarts, float tol, const int* __restrict__ act,
                                                           int* __restrict__ iters_out) {
     constexpr int TPB = 32 * NW, S = TPB * SPT;
+    // reduction buffer stride (float2): the batched Gram-Schmidt reduction holds up to M + 2
+    // values per warp
+    constexpr int PST = CGS ? NW * (M + 2) : NW;
     extern __shared__ __align__(16) unsigned char smraw_f[];
     const int seg = blockIdx.x, rhs = blockIdx.y;
     if (act && !act[rhs]) return;
     float4* V = reinterpret_cast<float4*>(smraw_f);             // [M+1][S]
     float2* H = reinterpret_cast<float2*>(V + (M + 1) * S);     // [M][M]
-    float2* part = H + ((M * M + 1) & ~1);                      // [2][NW], 16-byte aligned
+    float2* part = H + ((M * M + 1) & ~1);                      // [2][PST], 16-byte aligned
+    float2* hcor = part + 2 * PST;                               // [M]: second-projection column
     int buf = 0;
     const int tid = threadIdx.x;
     const int block = blocks[seg];
@@ -178,33 +229,84 @@ __global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const float2* __restric
             acc = p_fma(a[k].re, a[k].re, acc);
             acc = p_fma(a[k].im, a[k].im, acc);
         }
-        return psum1<NW>(acc.x + acc.y, part, buf);
+        return psum1<NW, PST>(acc.x + acc.y, part, buf);
     };
     auto store = [&](float4* Vd, const SiteP (&a)[SPT]) {
 #pragma unroll
         for (int k = 0; k < SPT; k++) site_st(Vd, tid + TPB * k, a[k]);
     };
+    // this thread's parts of <V_i, w> for i <= j (d[i]) and of |w|^2 (d[j + 1].x)
+    auto dots = [&](int j, const SiteP (&w)[SPT], float2 (&d)[M + 2]) {
+        float2 nw = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int k = 0; k < SPT; k++) {
+            nw = p_fma(w[k].re, w[k].re, nw);
+            nw = p_fma(w[k].im, w[k].im, nw);
+        }
+#pragma unroll
+        for (int i = 0; i <= M; i++) {
+            if (i <= j) {
+                float2 ar = make_float2(0.f, 0.f), ai = ar, an = ar;
+#pragma unroll
+                for (int k = 0; k < SPT; k++) {
+                    const SiteP vi = site_ld(V + i * S, tid + TPB * k);
+                    ar = p_fma(w[k].re, vi.re, ar);
+                    ar = p_fma(w[k].im, vi.im, ar);
+                    ai = p_fma(w[k].im, vi.re, ai);
+                    an = p_fma(w[k].re, vi.im, an);
+                }
+                d[i] = make_float2(ar.x + ar.y, (ai.x + ai.y) - (an.x + an.y));
+            }
+        }
+        d[j + 1] = make_float2(nw.x + nw.y, 0.f);
+    };
+    // w -= sum_{i <= j} h_i V_i
+    auto project = [&](int j, const float2 (&h)[M + 2], SiteP (&w)[SPT]) {
+#pragma unroll
+        for (int i = 0; i <= M; i++) {
+            if (i <= j) {
+                const float2 nhx = p_bc(-h[i].x), hy = p_bc(h[i].y), nhy = p_bc(-h[i].y);
+#pragma unroll
+                for (int k = 0; k < SPT; k++) {
+                    const SiteP vi = site_ld(V + i * S, tid + TPB * k);
+                    w[k].re = p_fma(nhx, vi.re, w[k].re);
+                    w[k].re = p_fma(hy, vi.im, w[k].re);
+                    w[k].im = p_fma(nhx, vi.im, w[k].im);
+                    w[k].im = p_fma(nhy, vi.re, w[k].im);
+                }
+            }
+        }
+    };
 
     const float4* rb4 = reinterpret_cast<const float4*>(r + off);
-    SiteP x[SPT], w[SPT];
+    // The iterate x lives in basis slot M, which the Arnoldi process never needs (the update
+    // uses V_0..V_{M-1} and each cycle restarts from the true residual), so it holds no
+    // registers during the Arnoldi steps and the residual's operator reads it in place.
+    float4* X = V + M * S;
+    SiteP w[SPT];
+    float normb;
+    {
+        // r = b - A x0 (x0 = b)
+        SiteP b[SPT];
 #pragma unroll
-    for (int k = 0; k < SPT; k++) x[k] = site_from_global(__ldg(&rb4[gs[k]]));
-    // r = b - A x0 (x0 = b)
-    store(V, x);
-    const float normb = sqrtf(norm2(x));
-    lean_sync<float, NW>();
-    apply(V, w);
+        for (int k = 0; k < SPT; k++) b[k] = site_from_global(__ldg(&rb4[gs[k]]));
+        store(X, b);
+        normb = sqrtf(norm2(b));
+        lean_sync<float, NW>();
+        apply(X, w);
 #pragma unroll
-    for (int k = 0; k < SPT; k++) {
-        w[k].re = p_sub(x[k].re, w[k].re);
-        w[k].im = p_sub(x[k].im, w[k].im);
+        for (int k = 0; k < SPT; k++) {
+            w[k].re = p_sub(b[k].re, w[k].re);
+            w[k].im = p_sub(b[k].im, w[k].im);
+        }
     }
-    float err = sqrtf(norm2(w));
+    float err2 = norm2(w), rerr = rsqrtf(err2), err = err2 * rerr;
+    const float tolb2 = (tol * normb) * (tol * normb);   // the exit test on |g_{j+1}|^2
     int maxit = M;
     int ret = restarts * M;
     for (int kk = 0; kk < restarts; kk++) {
         {
-            const float2 inv = p_bc(1.0f / err);
+            const float2 inv = p_bc(rerr);
 #pragma unroll
             for (int k = 0; k < SPT; k++) {
                 w[k].re = p_mul(inv, w[k].re);
@@ -222,33 +324,97 @@ __global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const float2* __restric
         for (int j = 0; j < M; j++) {
             apply(V + j * S, w);
             float2 col[M + 1];
-            // modified Gram-Schmidt (src/fgmres.cpp:24-32), V_i read once per step
+            float hn2;
+            if constexpr (CGS) {
+                // classical Gram-Schmidt: the j + 1 dots and |w|^2 in one reduction and the
+                // norm of the projected w by Pythagoras, so one barrier per step instead of
+                // j + 2; the same Hessenberg column as the modified form in exact
+                // arithmetic.  When the projection cancels below 1/8 of |w| (the
+                // re-orthogonalisation test of Daniel, Gragg, Kaufman and Stewart, Math.
+                // Comp. 30 (1976), with eta = 1/8) w is projected once more and its norm
+                // taken directly, which keeps the Pythagorean norm accurate to ~64 ulp and
+                // bounds the loss of orthogonality per step by 8x.  On 32x32 Wilson blocks
+                // the ratio stays near 0.6 (min 0.45), so the second projection is the rare
+                // path; it goes one basis vector at a time, which needs fewer registers than
+                // a second batched pass.
+                float2 d[M + 2];
+                dots(j, w, d);
+                psum_n<NW, PST>(d, j + 2, part, buf);
+                float hs = 0.f;
 #pragma unroll
-            for (int i = 0; i <= j; i++) {
-                SiteP vi[SPT];
-                float2 ar = make_float2(0.f, 0.f), ai = ar, an = ar;
-#pragma unroll
-                for (int k = 0; k < SPT; k++) {
-                    vi[k] = site_ld(V + i * S, tid + TPB * k);
-                    ar = p_fma(w[k].re, vi[k].re, ar);
-                    ar = p_fma(w[k].im, vi[k].im, ar);
-                    ai = p_fma(w[k].im, vi[k].re, ai);
-                    an = p_fma(w[k].re, vi[k].im, an);
+                for (int i = 0; i <= j; i++) {
+                    col[i] = d[i];
+                    hs += cnorm2(d[i]);
                 }
-                const float2 h = psum2<NW>(make_float2(ar.x + ar.y, (ai.x + ai.y) - (an.x + an.y)), part, buf);
-                col[i] = h;
-                const float2 nhx = p_bc(-h.x), hy = p_bc(h.y), nhy = p_bc(-h.y);
+                const float ww = d[j + 1].x;
+                hn2 = ww - hs;
+                project(j, d, w);
+                if (hn2 < ww * (1.0f / 64.0f)) {
+                    // second projection, one basis vector at a time in a loop that is not
+                    // unrolled (the rare path stays small); thread 0 passes the corrections
+                    // to the column through shared memory, ordered by the norm's barrier
+#pragma unroll 1
+                    for (int i = 0; i <= j; i++) {
+                        const float4* Vi = V + i * S;
+                        float2 ar = make_float2(0.f, 0.f), ai = ar, an = ar;
 #pragma unroll
-                for (int k = 0; k < SPT; k++) {
-                    w[k].re = p_fma(nhx, vi[k].re, w[k].re);
-                    w[k].re = p_fma(hy, vi[k].im, w[k].re);
-                    w[k].im = p_fma(nhx, vi[k].im, w[k].im);
-                    w[k].im = p_fma(nhy, vi[k].re, w[k].im);
+                        for (int k = 0; k < SPT; k++) {
+                            const SiteP vi = site_ld(Vi, tid + TPB * k);
+                            ar = p_fma(w[k].re, vi.re, ar);
+                            ar = p_fma(w[k].im, vi.im, ar);
+                            ai = p_fma(w[k].im, vi.re, ai);
+                            an = p_fma(w[k].re, vi.im, an);
+                        }
+                        const float2 h = psum2<NW, PST>(make_float2(ar.x + ar.y, (ai.x + ai.y) - (an.x + an.y)), part, buf);
+                        if (tid == 0) hcor[i] = h;
+                        const float2 nhx = p_bc(-h.x), hy = p_bc(h.y), nhy = p_bc(-h.y);
+#pragma unroll
+                        for (int k = 0; k < SPT; k++) {
+                            const SiteP vi = site_ld(Vi, tid + TPB * k);
+                            w[k].re = p_fma(nhx, vi.re, w[k].re);
+                            w[k].re = p_fma(hy, vi.im, w[k].re);
+                            w[k].im = p_fma(nhx, vi.im, w[k].im);
+                            w[k].im = p_fma(nhy, vi.re, w[k].im);
+                        }
+                    }
+                    hn2 = norm2(w);
+                    if (NW == 1) __syncwarp();
+#pragma unroll
+                    for (int i = 0; i <= j; i++) col[i] = col[i] + hcor[i];
                 }
+                hn2 = fmaxf(hn2, 0.f);
+            } else {
+                // modified Gram-Schmidt (src/fgmres.cpp:24-32), V_i read once per step
+#pragma unroll
+                for (int i = 0; i <= j; i++) {
+                    SiteP vi[SPT];
+                    float2 ar = make_float2(0.f, 0.f), ai = ar, an = ar;
+#pragma unroll
+                    for (int k = 0; k < SPT; k++) {
+                        vi[k] = site_ld(V + i * S, tid + TPB * k);
+                        ar = p_fma(w[k].re, vi[k].re, ar);
+                        ar = p_fma(w[k].im, vi[k].im, ar);
+                        ai = p_fma(w[k].im, vi[k].re, ai);
+                        an = p_fma(w[k].re, vi[k].im, an);
+                    }
+                    const float2 h = psum2<NW, PST>(make_float2(ar.x + ar.y, (ai.x + ai.y) - (an.x + an.y)), part, buf);
+                    col[i] = h;
+                    const float2 nhx = p_bc(-h.x), hy = p_bc(h.y), nhy = p_bc(-h.y);
+#pragma unroll
+                    for (int k = 0; k < SPT; k++) {
+                        w[k].re = p_fma(nhx, vi[k].re, w[k].re);
+                        w[k].re = p_fma(hy, vi[k].im, w[k].re);
+                        w[k].im = p_fma(nhx, vi[k].im, w[k].im);
+                        w[k].im = p_fma(nhy, vi[k].re, w[k].im);
+                    }
+                }
+                hn2 = norm2(w);
             }
-            const float hn = sqrtf(norm2(w));
-            if (hn > 0.f) {
-                const float2 inv = p_bc(1.0f / hn);
+            // 1/|w| and |w| from one reciprocal square root
+            const float rhn = rsqrtf(hn2);
+            const float hn = hn2 > 0.f ? hn2 * rhn : 0.f;
+            if (j + 1 < M && hn2 > 0.f) {
+                const float2 inv = p_bc(rhn);
                 SiteP t[SPT];
 #pragma unroll
                 for (int k = 0; k < SPT; k++) {
@@ -265,9 +431,9 @@ __global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const float2* __restric
                 col[i + 1] = cmul(cs[i], col[i + 1]) - cmul(sns[i], col[i]);
                 col[i] = temp;
             }
-            const float den = sqrtf(cnorm2(col[j]) + cnorm2(col[j + 1]));
-            sns[j] = make_float2(col[j + 1].x / den, col[j + 1].y / den);
-            cs[j] = make_float2(col[j].x / den, col[j].y / den);
+            const float rden = rsqrtf(cnorm2(col[j]) + cnorm2(col[j + 1]));
+            sns[j] = make_float2(col[j + 1].x * rden, col[j + 1].y * rden);
+            cs[j] = make_float2(col[j].x * rden, col[j].y * rden);
             col[j] = cmulc(cs[j], col[j]) + cmulc(sns[j], col[j + 1]);
             if (tid == 0) {
 #pragma unroll
@@ -276,7 +442,7 @@ __global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const float2* __restric
             g[j + 1] = -cmul(sns[j], g[j]);
             g[j] = cmulc(cs[j], g[j]);
             lean_sync<float, NW>();
-            if (sqrtf(cnorm2(g[j + 1])) < tol * normb) {
+            if (cnorm2(g[j + 1]) < tolb2) {
                 maxit = j + 1;
                 break;
             }
@@ -292,34 +458,40 @@ __global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const float2* __restric
                 if (jj < maxit) o = o - cmul(H[i * M + jj], eta[jj]);
             eta[i] = cdiv(o, H[i * M + i]);
         }
+        {
+            SiteP x[SPT];
 #pragma unroll
-        for (int jj = 0; jj < M; jj++) {
-            if (jj >= maxit) break;
-            const float2 ex = p_bc(eta[jj].x), ey = p_bc(eta[jj].y), ney = p_bc(-eta[jj].y);
+            for (int k = 0; k < SPT; k++) x[k] = site_ld(X, tid + TPB * k);
 #pragma unroll
-            for (int k = 0; k < SPT; k++) {
-                const SiteP v = site_ld(V + jj * S, tid + TPB * k);
-                x[k].re = p_fma(ex, v.re, x[k].re);
-                x[k].re = p_fma(ney, v.im, x[k].re);
-                x[k].im = p_fma(ex, v.im, x[k].im);
-                x[k].im = p_fma(ey, v.re, x[k].im);
+            for (int jj = 0; jj < M; jj++) {
+                if (jj >= maxit) break;
+                const float2 ex = p_bc(eta[jj].x), ey = p_bc(eta[jj].y), ney = p_bc(-eta[jj].y);
+#pragma unroll
+                for (int k = 0; k < SPT; k++) {
+                    const SiteP v = site_ld(V + jj * S, tid + TPB * k);
+                    x[k].re = p_fma(ex, v.re, x[k].re);
+                    x[k].re = p_fma(ney, v.im, x[k].re);
+                    x[k].im = p_fma(ex, v.im, x[k].im);
+                    x[k].im = p_fma(ey, v.re, x[k].im);
+                }
             }
+            store(X, x);
         }
-        // true residual r = b - A x (x staged through V1).  After the last cycle it only
-        // decides the returned iteration count, so it is skipped when nobody reads that.
+        // true residual r = b - A x.  After the last cycle it only decides the returned
+        // iteration count, so it is skipped when nobody reads that.
         if (kk == restarts - 1 && !iters_out) break;
         lean_sync<float, NW>();
-        store(V + S, x);
-        lean_sync<float, NW>();
-        apply(V + S, w);
+        apply(X, w);
 #pragma unroll
         for (int k = 0; k < SPT; k++) {
             const SiteP b = site_from_global(__ldg(&rb4[gs[k]]));
             w[k].re = p_sub(b.re, w[k].re);
             w[k].im = p_sub(b.im, w[k].im);
         }
-        err = sqrtf(norm2(w));
-        if (err < tol * normb) {
+        err2 = norm2(w);
+        rerr = rsqrtf(err2);
+        err = err2 * rerr;
+        if (err2 < tolb2) {
             ret = kk * M + maxit;
             break;
         }
@@ -328,20 +500,21 @@ __global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const float2* __restric
     float4* xo = reinterpret_cast<float4*>(xg + off);
 #pragma unroll
     for (int k = 0; k < SPT; k++) {
+        const SiteP xk = site_ld(X, tid + TPB * k);
         float4 o = xo[gs[k]];
-        o.x += x[k].re.x;
-        o.y += x[k].im.x;
-        o.z += x[k].re.y;
-        o.w += x[k].im.y;
+        o.x += xk.re.x;
+        o.y += xk.im.x;
+        o.z += xk.re.y;
+        o.w += xk.im.y;
         xo[gs[k]] = o;
     }
     if (iters_out && tid == 0) iters_out[rhs * ncol + seg] = ret;
 }
 
-template <int M, int SPT, int NW>
+template <int M, int SPT, int NW, bool CGS = false>
 inline int sap0_f32_smem() {
     constexpr int S = 32 * NW * SPT;
-    return (M + 1) * S * 16 + ((M * M + 1) & ~1) * 8 + 2 * NW * 8 + 16;
+    return (M + 1) * S * 16 + ((M * M + 1) & ~1) * 8 + 2 * (CGS ? NW * (M + 2) : NW) * 8 + M * 8 + 16;
 }
 
 }  // namespace amgb
