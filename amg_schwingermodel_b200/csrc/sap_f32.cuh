@@ -205,11 +205,14 @@ __global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const float2* __restric
     }
 
     // w = D_B v for this thread's sites
-    auto apply = [&](const float4* __restrict__ v, SiteP (&w)[SPT]) {
+    // (cw: the thread's own sites of v are also in w, so only the neighbours come from
+    // shared memory)
+    auto apply = [&](const float4* __restrict__ v, SiteP (&w)[SPT], bool cw) {
 #pragma unroll
         for (int k = 0; k < SPT; k++) {
             const int m = tid + TPB * k;
-            const float4 c = v[m], a = v[nb[k][0]], b = v[nb[k][1]], e = v[nb[k][2]], g = v[nb[k][3]];
+            const float4 c = cw ? make_float4(w[k].re.x, w[k].re.y, w[k].im.x, w[k].im.y) : v[m];
+            const float4 a = v[nb[k][0]], b = v[nb[k][1]], e = v[nb[k][2]], g = v[nb[k][3]];
             const float2 ta = cmul(lk[k][0], make_float2(a.x - a.y, a.z - a.w));   // (1 - sigma_0) forward t
             const float2 tb = cmul(lk[k][1], make_float2(b.x - b.w, b.z + b.y));   // (1 - sigma_1) forward x
             const float2 tc = cmul(lk[k][2], make_float2(e.x + e.y, e.z + e.w));   // (1 + sigma_0) backward t
@@ -293,7 +296,7 @@ __global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const float2* __restric
         store(X, b);
         normb = sqrtf(norm2(b));
         lean_sync<float, NW>();
-        apply(X, w);
+        apply(X, w, false);
 #pragma unroll
         for (int k = 0; k < SPT; k++) {
             w[k].re = p_sub(b[k].re, w[k].re);
@@ -322,7 +325,7 @@ __global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const float2* __restric
         lean_sync<float, NW>();
 #pragma unroll
         for (int j = 0; j < M; j++) {
-            apply(V + j * S, w);
+            apply(V + j * S, w, true);   // w holds V_j
             float2 col[M + 1];
             float hn2;
             if constexpr (CGS) {
@@ -415,13 +418,12 @@ __global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const float2* __restric
             const float hn = hn2 > 0.f ? hn2 * rhn : 0.f;
             if (j + 1 < M && hn2 > 0.f) {
                 const float2 inv = p_bc(rhn);
-                SiteP t[SPT];
 #pragma unroll
                 for (int k = 0; k < SPT; k++) {
-                    t[k].re = p_mul(inv, w[k].re);
-                    t[k].im = p_mul(inv, w[k].im);
+                    w[k].re = p_mul(inv, w[k].re);
+                    w[k].im = p_mul(inv, w[k].im);
                 }
-                store(V + (j + 1) * S, t);
+                store(V + (j + 1) * S, w);
             }
             // rotation(j) (src/fgmres.cpp:90-104)
             col[j + 1] = make_float2(hn, 0.f);
@@ -481,7 +483,7 @@ __global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const float2* __restric
         // iteration count, so it is skipped when nobody reads that.
         if (kk == restarts - 1 && !iters_out) break;
         lean_sync<float, NW>();
-        apply(X, w);
+        apply(X, w, false);
 #pragma unroll
         for (int k = 0; k < SPT; k++) {
             const SiteP b = site_from_global(__ldg(&rb4[gs[k]]));
