@@ -149,6 +149,12 @@ __device__ __forceinline__ void psum_n(float2 (&v)[K], int n, float2* part, int&
     buf ^= 1;
 }
 
+// float2 stride between the two reduction buffers: the batched classical Gram-Schmidt
+// reduction holds up to M + 2 values per warp, the modified form 2 (the last projection's dot
+// and |w|^2)
+template <int M, int NW, bool CGS>
+constexpr int sap0_f32_pst() { return CGS ? NW * (M + 2) : NW * 2; }
+
 template <int M, int SPT, int NW, bool CGS = false>
 __global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const float2* __restrict__ U, const float2* __restrict__ r,
                                                           float2* __restrict__ xg, const int* __restrict__ blocks,
@@ -156,9 +162,7 @@ __global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const float2* __restric
                                                           int restarts, float tol, const int* __restrict__ act,
                                                           int* __restrict__ iters_out) {
     constexpr int TPB = 32 * NW, S = TPB * SPT;
-    // reduction buffer stride (float2): the batched Gram-Schmidt reduction holds up to M + 2
-    // values per warp
-    constexpr int PST = CGS ? NW * (M + 2) : NW;
+    constexpr int PST = sap0_f32_pst<M, NW, CGS>();
     extern __shared__ __align__(16) unsigned char smraw_f[];
     const int seg = blockIdx.x, rhs = blockIdx.y;
     if (act && !act[rhs]) return;
@@ -387,11 +391,15 @@ __global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const float2* __restric
                 }
                 hn2 = fmaxf(hn2, 0.f);
             } else {
-                // modified Gram-Schmidt (src/fgmres.cpp:24-32), V_i read once per step
+                // modified Gram-Schmidt (src/fgmres.cpp:24-32), V_i read once per step.  The
+                // last projection's reduction also carries |w|^2, and |w - h_j V_j|^2 =
+                // |w|^2 - |h_j|^2 (w is already orthogonal to V_0..V_{j-1}) saves the norm's
+                // own reduction; when it cancels below 1/8 of |w| the norm is taken directly.
+                float ww = 0.f;
 #pragma unroll
                 for (int i = 0; i <= j; i++) {
                     SiteP vi[SPT];
-                    float2 ar = make_float2(0.f, 0.f), ai = ar, an = ar;
+                    float2 ar = make_float2(0.f, 0.f), ai = ar, an = ar, nw = ar;
 #pragma unroll
                     for (int k = 0; k < SPT; k++) {
                         vi[k] = site_ld(V + i * S, tid + TPB * k);
@@ -399,8 +407,21 @@ __global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const float2* __restric
                         ar = p_fma(w[k].im, vi[k].im, ar);
                         ai = p_fma(w[k].im, vi[k].re, ai);
                         an = p_fma(w[k].re, vi[k].im, an);
+                        if (i == j) {
+                            nw = p_fma(w[k].re, w[k].re, nw);
+                            nw = p_fma(w[k].im, w[k].im, nw);
+                        }
                     }
-                    const float2 h = psum2<NW, PST>(make_float2(ar.x + ar.y, (ai.x + ai.y) - (an.x + an.y)), part, buf);
+                    float2 h;
+                    if (i == j) {
+                        float2 d[2] = {make_float2(ar.x + ar.y, (ai.x + ai.y) - (an.x + an.y)),
+                                       make_float2(nw.x + nw.y, 0.f)};
+                        psum_n<NW, PST>(d, 2, part, buf);
+                        h = d[0];
+                        ww = d[1].x;
+                    } else {
+                        h = psum2<NW, PST>(make_float2(ar.x + ar.y, (ai.x + ai.y) - (an.x + an.y)), part, buf);
+                    }
                     col[i] = h;
                     const float2 nhx = p_bc(-h.x), hy = p_bc(h.y), nhy = p_bc(-h.y);
 #pragma unroll
@@ -411,7 +432,8 @@ __global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const float2* __restric
                         w[k].im = p_fma(nhy, vi[k].re, w[k].im);
                     }
                 }
-                hn2 = norm2(w);
+                hn2 = ww - cnorm2(col[j]);
+                if (hn2 < ww * (1.0f / 64.0f)) hn2 = norm2(w);
             }
             // 1/|w| and |w| from one reciprocal square root
             const float rhn = rsqrtf(hn2);
@@ -516,7 +538,8 @@ __global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const float2* __restric
 template <int M, int SPT, int NW, bool CGS = false>
 inline int sap0_f32_smem() {
     constexpr int S = 32 * NW * SPT;
-    return (M + 1) * S * 16 + ((M * M + 1) & ~1) * 8 + 2 * (CGS ? NW * (M + 2) : NW) * 8 + M * 8 + 16;
+    // V [M+1][S] float4, H [M][M] float2 (even count), part [2][PST] float2, hcor [M] float2
+    return (M + 1) * S * 16 + ((M * M + 1) & ~1) * 8 + 2 * sap0_f32_pst<M, NW, CGS>() * 8 + M * 8 + 16;
 }
 
 }  // namespace amgb
