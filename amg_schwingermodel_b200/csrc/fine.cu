@@ -743,6 +743,14 @@ static cudaError_t launch_sap0_paired(const float2* U, const float2* r, float2* 
                                       float tol, int* iters, const int* act, cudaStream_t s, bool* done, int v) {
     *done = true;
     const int S = sxe * ste;
+    // the paired kernel gives each thread a run of SPT consecutive t sites (SPT = 2 for 64-site
+    // blocks or the MGS form with AMG_SAP_SPT=2, else 4), so the block's t extent must be a
+    // multiple of it
+    const int spt = (S == 64 || (v != SAP_VARIANT_CGS && g_sap0_spt == 2)) ? 2 : 4;
+    if (v != SAP_VARIANT_CA && ste % spt != 0) {
+        *done = false;
+        return cudaSuccess;
+    }
     if (v == SAP_VARIANT_CGS) {
         switch (S) {
             case 64: return launch_sap0_f32<2, 1, true>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);

@@ -178,13 +178,20 @@ __global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const float2* __restric
     const long long off = (long long)rhs * nx * nt * 2;
     const float mass = m0 + 2.0f;
 
-    // per-site set-up: neighbour local indices and the folded hop links
-    int nb[SPT][4];
+    // Thread tid owns the SPT consecutive sites m = SPT*tid + k (k = 0..SPT-1) of one t row
+    // (the dispatcher guarantees SPT | ste), and site m lives at shared index
+    // sidx(m) = (m % SPT)*TPB + m / SPT, so a warp's accesses to "site k of every thread" are
+    // contiguous.  A site's t neighbours are then the thread's own registers except at the
+    // ends of its run, and only the x neighbours and those two come from shared memory.
+    // Per-site set-up: the shared indices of those neighbours and the folded hop links.
+    auto sidx = [&](int q) { return (q % SPT) * TPB + q / SPT; };
+    int nbt[2];          // t-1 neighbour of site 0, t+1 neighbour of site SPT-1
+    int nbx[SPT][2];     // x+1, x-1 neighbours
     float2 lk[SPT][4];
     int gs[SPT];
 #pragma unroll
     for (int k = 0; k < SPT; k++) {
-        const int m = tid + TPB * k;
+        const int m = SPT * tid + k;
         const int mx = m / ste, mt = m - mx * ste;
         const int t = t0 + mt, x = x0 + mx;
         gs[k] = x * nt + t;
@@ -192,31 +199,42 @@ __global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const float2* __restric
         const float sL = (t == 0) ? -0.5f : 0.5f;
         int q = -1;
         if (mt + 1 < ste) q = m + 1; else if (ste == nt) q = mx * ste;
-        nb[k][0] = q < 0 ? m : q;
+        if (k == SPT - 1) nbt[1] = sidx(q < 0 ? m : q);
         lk[k][0] = q < 0 ? czero<float>() : sR * U[2 * gs[k]];
         q = -1;
         if (mx + 1 < sxe) q = m + ste; else if (sxe == nx) q = mt;
-        nb[k][1] = q < 0 ? m : q;
+        nbx[k][0] = sidx(q < 0 ? m : q);
         lk[k][1] = q < 0 ? czero<float>() : 0.5f * U[2 * gs[k] + 1];
         q = -1;
         if (mt > 0) q = m - 1; else if (ste == nt) q = mx * ste + ste - 1;
-        nb[k][2] = q < 0 ? m : q;
+        if (k == 0) nbt[0] = sidx(q < 0 ? m : q);
         lk[k][2] = q < 0 ? czero<float>() : sL * cconj(U[2 * (x * nt + ((t == 0) ? nt - 1 : t - 1))]);
         q = -1;
         if (mx > 0) q = m - ste; else if (sxe == nx) q = (sxe - 1) * ste + mt;
-        nb[k][3] = q < 0 ? m : q;
+        nbx[k][1] = sidx(q < 0 ? m : q);
         lk[k][3] = q < 0 ? czero<float>() : 0.5f * cconj(U[2 * (((x == 0) ? nx - 1 : x - 1) * nt + t) + 1]);
     }
 
     // w = D_B v for this thread's sites
-    // (cw: the thread's own sites of v are also in w, so only the neighbours come from
-    // shared memory)
+    // (cw: the thread's own sites of v are also in w, so the t neighbours inside the run come
+    // from registers; the sites are done in order and each keeps its old value for the next)
     auto apply = [&](const float4* __restrict__ v, SiteP (&w)[SPT], bool cw) {
+        float4 prev = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
         for (int k = 0; k < SPT; k++) {
-            const int m = tid + TPB * k;
-            const float4 c = cw ? make_float4(w[k].re.x, w[k].re.y, w[k].im.x, w[k].im.y) : v[m];
-            const float4 a = v[nb[k][0]], b = v[nb[k][1]], e = v[nb[k][2]], g = v[nb[k][3]];
+            const int mi = tid + TPB * k;
+            float4 c, a, e;
+            if (cw) {
+                c = make_float4(w[k].re.x, w[k].re.y, w[k].im.x, w[k].im.y);
+                a = (k < SPT - 1) ? make_float4(w[k + 1].re.x, w[k + 1].re.y, w[k + 1].im.x, w[k + 1].im.y) : v[nbt[1]];
+                e = (k > 0) ? prev : v[nbt[0]];
+                prev = c;
+            } else {
+                c = v[mi];
+                a = (k < SPT - 1) ? v[mi + TPB] : v[nbt[1]];
+                e = (k > 0) ? v[mi - TPB] : v[nbt[0]];
+            }
+            const float4 b = v[nbx[k][0]], g = v[nbx[k][1]];
             const float2 ta = cmul(lk[k][0], make_float2(a.x - a.y, a.z - a.w));   // (1 - sigma_0) forward t
             const float2 tb = cmul(lk[k][1], make_float2(b.x - b.w, b.z + b.y));   // (1 - sigma_1) forward x
             const float2 tc = cmul(lk[k][2], make_float2(e.x + e.y, e.z + e.w));   // (1 + sigma_0) backward t
