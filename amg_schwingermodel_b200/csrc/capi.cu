@@ -305,15 +305,27 @@ __global__ void k_reorth_flag(const double2* d1, const double2* d2, int nv, cons
     if (i >= R) return;
     flag[i] = (arn[i] && d2[i * (nv + 1) + nv].x < 0.5 * d1[i * (nv + 1) + nv].x) ? 1 : 0;
 }
-// scale[r] = 1/|w_final|, wmask[r] = arn[r] && |w_final| > 0, |w_final|^2 from pass 2 or pass 3
-__global__ void k_inv_norm2(const double2* d2, const double2* d3, const int* flag, int nv, double* scale,
-                            const int* arn, int* wmask, int R) {
+// |w_final|^2 of source r from the second pass: d2[r][nv] = |w'|^2 and, where a third pass
+// projects again (flag), minus its coefficients' |d2[r][k]|^2 (Pythagoras; they are the
+// small re-orthogonalisation corrections, so nothing cancels)
+__host__ __device__ inline double final_norm2(const double2* d2r, int nv, int proj) {
+    double v = d2r[nv].x;
+    if (proj)
+        for (int k = 0; k < nv; k++) v -= d2r[k].x * d2r[k].x + d2r[k].y * d2r[k].y;
+    return v > 0 ? v : 0.0;
+}
+// scale[r] = 1/|w_final|, wmask[r] = arn[r] && |w_final| > 0, split into pmask (projected
+// again on the way into V_{j+1}) and smask (only scaled)
+__global__ void k_inv_norm2(const double2* d2, const int* flag, int nv, double* scale, const int* arn, int* wmask,
+                            int* pmask, int* smask, int R) {
     const int i = threadIdx.x;
     if (i >= R) return;
-    const double v = flag[i] ? d3[i].x : d2[i * (nv + 1) + nv].x;
-    const double h = sqrt(v);
+    const double h = sqrt(final_norm2(d2 + (size_t)i * (nv + 1), nv, flag[i]));
     scale[i] = h > 0 ? 1.0 / h : 0.0;
-    wmask[i] = (arn[i] && h > 0) ? 1 : 0;
+    const int wm = (arn[i] && h > 0) ? 1 : 0;
+    wmask[i] = wm;
+    pmask[i] = wm && flag[i];
+    smask[i] = wm && !flag[i];
 }
 
 int ensure_capacity(amg_context* c, int R);
@@ -776,6 +788,8 @@ struct OuterSolve {
     int* wm_d() const { return arn_d() + c->Rcap; }
     int* nvr_d() const { return wm_d() + c->Rcap; }
     int* ro_d() const { return nvr_d() + c->Rcap; }
+    int* pm_d() const { return ro_d() + c->Rcap; }   // wm && ro: projected again into V_{j+1}
+    int* sm_d() const { return pm_d() + c->Rcap; }   // wm && !ro: only scaled into V_{j+1}
 
     int init(amg_context* c_, const double2* b_, double2* x_, int R_, amg_solve_info* info_) {
         c = c_; b = b_; x = x_; R = R_; info = info_;
@@ -864,19 +878,22 @@ struct OuterSolve {
         const int nv = j + 1;
         double2* d1 = dots;
         double2* d2 = dots + (size_t)R * (nv + 1);
-        double2* d3 = d2 + (size_t)R * (nv + 1);
         {
-            // classical Gram-Schmidt, re-orthogonalised only where the first pass cancelled
-            ProfScope ps_(c, AMG_PROF_BLAS, (double)R * len * sizeof(double2) * (2.0 * (nv + 1) + 4.0));
+            // classical Gram-Schmidt, re-orthogonalised only where the first pass cancelled; the
+            // second projection and the normalisation are one pass writing V_{j+1}
+            ProfScope ps_(c, AMG_PROF_BLAS, (double)R * len * sizeof(double2) * (3.0 * nv + 5.0));
             launch_multidot(w, V, len, vstride, nv, R, dpart, np, d1, arn_d(), c->stream);
             launch_axpy_multidot(w, V, len, vstride, nv, d1, nv + 1, nv, arn_d(), R, dpart, np, d2, c->stream);
             k_reorth_flag<<<1, 256, 0, c->stream>>>(d1, d2, nv, arn_d(), ro_d(), R);
-            launch_axpy_multidot(w, V, len, vstride, nv, d2, nv + 1, 0, ro_d(), R, dpart, np, d3, c->stream);
-            k_inv_norm2<<<1, 256, 0, c->stream>>>(d2, d3, ro_d(), nv, c->scal.as<double>(), arn_d(), wm_d(), R);
+            k_inv_norm2<<<1, 256, 0, c->stream>>>(d2, ro_d(), nv, c->scal.as<double>(), arn_d(), wm_d(), pm_d(),
+                                                  sm_d(), R);
             count_launch(2);
-            launch_scale(V + (long long)(j + 1) * vstride, w, len, c->scal.as<double>(), wm_d(), R, c->stream);
+            double2* Vn = V + (long long)(j + 1) * vstride;
+            launch_axpy_scale_to(Vn, w, V, len, vstride, nv, d2, nv + 1, c->scal.as<double>(), pm_d(), R, dpart, np,
+                                 c->stream);
+            launch_scale(Vn, w, len, c->scal.as<double>(), sm_d(), R, c->stream);
         }
-        CK(cudaMemcpyAsync(h_dots, dots, (size_t)R * (2 * (nv + 1) + 1) * sizeof(double2), cudaMemcpyDeviceToHost,
+        CK(cudaMemcpyAsync(h_dots, dots, (size_t)R * 2 * (nv + 1) * sizeof(double2), cudaMemcpyDeviceToHost,
                            c->stream));
         CK(cudaMemcpyAsync(h_ro, ro_d(), R * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
         CK(cudaEventRecord(c->ev_host, c->stream));
@@ -899,8 +916,7 @@ struct OuterSolve {
                 const double2 bq = hd[(size_t)R * (nv + 1) + (size_t)r * (nv + 1) + i];
                 Hr[i * m + j] = h_ro[r] ? cd(a.x + bq.x, a.y + bq.y) : cd(a.x, a.y);
             }
-            const double hn2 = h_ro[r] ? hd[(size_t)2 * R * (nv + 1) + r].x
-                                       : hd[(size_t)R * (nv + 1) + (size_t)r * (nv + 1) + nv].x;
+            const double hn2 = final_norm2(hd + (size_t)R * (nv + 1) + (size_t)r * (nv + 1), nv, h_ro[r]);
             Hr[(j + 1) * m + j] = cd(std::sqrt(hn2), 0);
             for (int i = 0; i < j; i++) {
                 cd temp = std::conj(cnr[i]) * Hr[i * m + j] + std::conj(snr[i]) * Hr[(i + 1) * m + j];
@@ -1029,7 +1045,7 @@ int ensure_capacity(amg_context* c, int R) {
     CKR(c->partial.alloc(np * Rn * 24 * sizeof(double2)));
     CKR(c->dots.alloc((size_t)Rn * 3 * 24 * sizeof(double2)));
     CKR(c->scal.alloc((size_t)Rn * sizeof(double)));
-    CKR(c->masks.alloc((size_t)5 * Rn * sizeof(int)));
+    CKR(c->masks.alloc((size_t)7 * Rn * sizeof(int)));
     CKR(c->etab.alloc((size_t)Rn * m * sizeof(double2)));
     CKR(c->sap_flags.alloc((size_t)2 * Rn * sizeof(int)));
     CKR(c->norms.alloc((size_t)2 * Rn * sizeof(double)));

@@ -466,7 +466,8 @@ __global__ void __launch_bounds__(256) k_multiaxpy(double2* __restrict__ w, cons
 }
 
 // One pass over w and the basis V_0..V_{nv-1} of every source (FP64):
-//   w -= sum_k h[k] V_k            (skipped when h is null)
+//   w -= sum_k h[k] V_k            (skipped when h is null; with y given, the result goes to
+//                                   y scaled by sc[rhs] and w is left as it was)
 //   partial[k] = sum_e w[e] conj(V_k[e]) for k < nd, and |w|^2 at k = nd
 // with the accumulators in registers (NV bounds nv and nd at compile time); per-CTA
 // partials are reduced by k_multidot_sum in a fixed order.  Sources with act[rhs] = 0 are
@@ -477,7 +478,8 @@ template <int NV>
 __global__ void __launch_bounds__(256, (NV <= 8 ? 2 : 1)) k_axpy_dots(double2* __restrict__ w, const double2* __restrict__ V,
                                                       long long len, long long vstride, int nv,
                                                       const double2* __restrict__ h, int hstride, int nd,
-                                                      const int* __restrict__ act, double2* __restrict__ partial) {
+                                                      const int* __restrict__ act, double2* __restrict__ partial,
+                                                      double2* __restrict__ y, const double* __restrict__ sc) {
     __shared__ double red[8][2 * (NV + 1)];
     __shared__ double2 hk[NV];   // the axpy coefficients, read as broadcasts (fewer live registers)
     const int rhs = blockIdx.y;
@@ -491,6 +493,8 @@ __global__ void __launch_bounds__(256, (NV <= 8 ? 2 : 1)) k_axpy_dots(double2* _
         hk[threadIdx.x] = (h && (int)threadIdx.x < nv) ? h[(long long)rhs * hstride + threadIdx.x] : make_double2(0, 0);
     __syncthreads();
     const int nload = (h && nv > nd) ? nv : nd;
+    const double f = y ? sc[rhs] : 1.0;
+    double2* yy = y ? y + (long long)rhs * len : nullptr;
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (long long)gridDim.x * blockDim.x) {
         double2 a = ww[e];
         // every V_k element is loaded once and kept for both the update and the dots
@@ -505,7 +509,8 @@ __global__ void __launch_bounds__(256, (NV <= 8 ? 2 : 1)) k_axpy_dots(double2* _
                     a.y -= hk[k].x * bk[k].y + hk[k].y * bk[k].x;
                 }
             }
-            ww[e] = a;
+            if (yy) yy[e] = make_double2(f * a.x, f * a.y);
+            else ww[e] = a;
         }
 #pragma unroll
         for (int k = 0; k < NV; k++) {
@@ -839,9 +844,10 @@ cudaError_t launch_sap0(const cx<T>* U, const cx<T>* r, cx<T>* x, const int* blo
 
 template <int NV>
 static void axpy_dots_nv(double2* w, const double2* V, long long len, long long vstride, int nv, const double2* h,
-                         int hstride, int nd, const int* act, int nrhs, double2* partial, int nparts, cudaStream_t s) {
+                         int hstride, int nd, const int* act, int nrhs, double2* partial, int nparts, cudaStream_t s,
+                         double2* y = nullptr, const double* sc = nullptr) {
     dim3 grid(nparts, nrhs);
-    k_axpy_dots<NV><<<grid, 256, 0, s>>>(w, V, len, vstride, nv, h, hstride, nd, act, partial);
+    k_axpy_dots<NV><<<grid, 256, 0, s>>>(w, V, len, vstride, nv, h, hstride, nd, act, partial, y, sc);
 }
 
 // w -= sum_{k<nv} h[k] V_k (h may be null), then out[rhs][k] = <w, V_k> for k < nd and
@@ -857,6 +863,18 @@ void launch_axpy_multidot(double2* w, const double2* V, long long len, long long
     else if (n <= 16) axpy_dots_nv<16>(w, V, len, vstride, nv, h, hstride, nd, act, nrhs, partial, nparts, s);
     else axpy_dots_nv<24>(w, V, len, vstride, nv, h, hstride, nd, act, nrhs, partial, nparts, s);
     k_multidot_sum<<<nrhs * (nd + 1), 256, 0, s>>>(partial, nparts, out);
+}
+
+void launch_axpy_scale_to(double2* y, const double2* w, const double2* V, long long len, long long vstride, int nv,
+                          const double2* h, int hstride, const double* sc, const int* act, int nrhs, double2* partial,
+                          int nparts, cudaStream_t s) {
+    count_launch(1);
+    double2* ww = const_cast<double2*>(w);   // read only when y is given
+    if (nv <= 4) axpy_dots_nv<4>(ww, V, len, vstride, nv, h, hstride, 0, act, nrhs, partial, nparts, s, y, sc);
+    else if (nv <= 8) axpy_dots_nv<8>(ww, V, len, vstride, nv, h, hstride, 0, act, nrhs, partial, nparts, s, y, sc);
+    else if (nv <= 12) axpy_dots_nv<12>(ww, V, len, vstride, nv, h, hstride, 0, act, nrhs, partial, nparts, s, y, sc);
+    else if (nv <= 16) axpy_dots_nv<16>(ww, V, len, vstride, nv, h, hstride, 0, act, nrhs, partial, nparts, s, y, sc);
+    else axpy_dots_nv<24>(ww, V, len, vstride, nv, h, hstride, 0, act, nrhs, partial, nparts, s, y, sc);
 }
 
 void launch_multidot(const double2* w, const double2* V, long long len, long long vstride, int nv, int nrhs,

@@ -49,6 +49,11 @@ void launch_multiaxpy(double2* w, const double2* V, long long len, long long vst
                       int hstride, const int* act, int nrhs, cudaStream_t s);
 void launch_multiaxpy_add(double2* x, const double2* Z, long long len, long long vstride, int nv, const double2* c,
                           int cstride, const int* nvr, const int* act, int nrhs, cudaStream_t s);
+// y = (w - sum_{k<nv} h[k] V_k) * sc for the sources with act (w unchanged; partial receives
+// unused |w|^2 partials)
+void launch_axpy_scale_to(double2* y, const double2* w, const double2* V, long long len, long long vstride, int nv,
+                          const double2* h, int hstride, const double* sc, const int* act, int nrhs, double2* partial,
+                          int nparts, cudaStream_t s);
 void launch_scale(double2* y, const double2* x, long long len, const double* sc, const int* act, int nrhs,
                   cudaStream_t s);
 void launch_d2f(float2* y, const double2* x, long long n, cudaStream_t s);
