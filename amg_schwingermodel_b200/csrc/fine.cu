@@ -212,7 +212,8 @@ __global__ void __launch_bounds__(256) k_restrict0t(const TW* __restrict__ W, co
     const int split = blockIdx.x, nc = blockIdx.y, nblk = gridDim.y;
     const int bxi = nc / bt, bti = nc - bxi * bt;
     const int spb = xe * te;
-    const int per = (spb + nsplit - 1) / nsplit;
+    // each split takes whole tiles (a split past the end takes none and writes zeros)
+    const int per = ((spb + nsplit - 1) / nsplit + kRtTile - 1) / kRtTile * kRtTile;
     const int q0 = split * per, q1 = min(spb, q0 + per);
     const int KP = (ntest + 1) / 2, RP = (nrhs + 1) / 2, K2 = 2 * KP, R2 = 2 * RP;
     const int OT = KP * 2 * RP;
@@ -230,9 +231,38 @@ __global__ void __launch_bounds__(256) k_restrict0t(const TW* __restrict__ W, co
 #pragma unroll
     for (int a = 0; a < 2; a++) { acc[a][0] = czero<T>(); acc[a][1] = czero<T>(); }
 
+    // tiles of whole kRtTile-site runs inside one x row (te a multiple of the tile, the usual
+    // case) stage with shifts and one base index instead of a division per element
+    const bool rows = (te % kRtTile) == 0;
     for (int qt = q0; qt < q1; qt += kRtTile) {
         const int nq = min(kRtTile, q1 - qt);
         __syncthreads();
+        if (rows && nq == kRtTile) {
+            const int mx = qt / te, mt = qt - mx * te;
+            const long long n0 = (long long)(bxi * xe + mx) * nt + (bti * te + mt);
+            for (int idx = tid; idx < kRtTile * K2; idx += blockDim.x) {
+                const int k = idx / kRtTile, qq = idx % kRtTile;
+                const long long n = n0 + qq;
+                cx<T> w0 = czero<T>(), w1 = czero<T>();
+                if (k < ntest) {
+                    w0 = ccast<T>(load_cx(W + ((long long)k * N + n) * 2));
+                    w1 = ccast<T>(load_cx(W + ((long long)k * N + n) * 2 + 1));
+                }
+                Ws[qq * WR + k] = w0;
+                Ws[qq * WR + K2 + k] = w1;
+            }
+            for (int idx = tid; idx < kRtTile * R2; idx += blockDim.x) {
+                const int r = idx / kRtTile, qq = idx % kRtTile;
+                const long long n = n0 + qq;
+                cx<T> p0 = czero<T>(), p1 = czero<T>();
+                if (r < nrhs) {
+                    p0 = v[(long long)r * N * 2 + 2 * n];
+                    p1 = v[(long long)r * N * 2 + 2 * n + 1];
+                }
+                Vs[qq * VR + r] = p0;
+                Vs[qq * VR + R2 + r] = p1;
+            }
+        } else {
         for (int idx = tid; idx < nq * K2; idx += blockDim.x) {
             const int k = idx / nq, qq = idx - k * nq;
             const int q = qt + qq, mx = q / te, mt = q - mx * te;
@@ -256,6 +286,7 @@ __global__ void __launch_bounds__(256) k_restrict0t(const TW* __restrict__ W, co
             }
             Vs[qq * VR + r] = p0;
             Vs[qq * VR + R2 + r] = p1;
+        }
         }
         __syncthreads();
         if (active) {
@@ -307,7 +338,12 @@ __global__ void k_restrict0_sum(const cx<T>* __restrict__ partial, cx<T>* __rest
 
 // Level::P_v at level 0 (src/level.cpp:182-209) added into psi:
 //   psi[rhs][n][s] += sum_cc W[cc][n][s] vc[rhs][nc(n)][2cc+s]
-template <typename T, typename TW>
+// Level::P_v at level 0 added into psi (src/level.cpp:182-209): psi[n][s] += sum_k W_k[n][s]
+// vc[nc][2k+s].  One thread per site; the site's KT >= ntest test-vector entries are loaded
+// once (BF16 -> T) and kept in registers for every source, so W streams from HBM once per
+// launch and each source costs one read-modify-write of psi plus broadcast reads of its
+// coarse vector (a warp's 32 consecutive t sites share one aggregate).
+template <typename T, typename TW, int KT>
 __global__ void __launch_bounds__(256) k_prolong0_add(const TW* __restrict__ W, const cx<T>* __restrict__ vc,
                                                       cx<T>* __restrict__ psi, int nx, int nt, int bt, int xe,
                                                       int te, int ntest, int nblk, int nrhs) {
@@ -316,18 +352,47 @@ __global__ void __launch_bounds__(256) k_prolong0_add(const TW* __restrict__ W, 
     if (n >= N) return;
     const int x = n / nt, t = n - x * nt;
     const int nc = (x / xe) * bt + (t / te);
+    cx<T> w0[KT], w1[KT];
+#pragma unroll
+    for (int k = 0; k < KT; k++) {
+        if (k < ntest) {
+            w0[k] = ccast<T>(load_cx(W + ((long long)k * N + n) * 2));
+            w1[k] = ccast<T>(load_cx(W + ((long long)k * N + n) * 2 + 1));
+        }
+    }
+    // several sources per trip keep several psi loads in flight (one for FP64 with more than
+    // 16 test vectors, whose entries already fill the registers)
+    constexpr int UR = (sizeof(T) == 8 && KT > 16) ? 1 : 4;
+#pragma unroll UR
     for (int rhs = 0; rhs < nrhs; rhs++) {
         const cx<T>* pv = vc + ((long long)rhs * nblk + nc) * 2 * ntest;
         cx<T> a0 = czero<T>(), a1 = czero<T>();
-        for (int k = 0; k < ntest; k++) {
-            cx<T> w0 = ccast<T>(load_cx(W + ((long long)k * N + n) * 2));
-            cx<T> w1 = ccast<T>(load_cx(W + ((long long)k * N + n) * 2 + 1));
-            cfma(a0, w0, pv[2 * k]);
-            cfma(a1, w1, pv[2 * k + 1]);
-        }
         cx<T>* o = psi + (long long)rhs * N * 2 + 2 * n;
-        o[0] += a0;
-        o[1] += a1;
+        if constexpr (sizeof(T) == 4) {
+            // both spins of a coarse entry and of a site in one 16-byte access
+#pragma unroll
+            for (int k = 0; k < KT; k++) {
+                if (k < ntest) {
+                    const float4 q = __ldg(reinterpret_cast<const float4*>(pv + 2 * k));
+                    cfma(a0, w0[k], make_float2(q.x, q.y));
+                    cfma(a1, w1[k], make_float2(q.z, q.w));
+                }
+            }
+            float4* o4 = reinterpret_cast<float4*>(o);
+            float4 q = *o4;
+            q.x += a0.x; q.y += a0.y; q.z += a1.x; q.w += a1.y;
+            *o4 = q;
+        } else {
+#pragma unroll
+            for (int k = 0; k < KT; k++) {
+                if (k < ntest) {
+                    cfma(a0, w0[k], pv[2 * k]);
+                    cfma(a1, w1[k], pv[2 * k + 1]);
+                }
+            }
+            o[0] += a0;
+            o[1] += a1;
+        }
     }
 }
 
@@ -673,7 +738,10 @@ void launch_prolong0_add(const TW* W, const cx<T>* vc, cx<T>* psi, int nx, int n
                          int nrhs, cudaStream_t s) {
     count_launch(1);
     const int xe = nx / bx, te = nt / bt;
-    k_prolong0_add<T, TW><<<(nx * nt + 255) / 256, 256, 0, s>>>(W, vc, psi, nx, nt, bt, xe, te, ntest, bx * bt, nrhs);
+    const int grid = (nx * nt + 255) / 256;
+    if (ntest <= 8) k_prolong0_add<T, TW, 8><<<grid, 256, 0, s>>>(W, vc, psi, nx, nt, bt, xe, te, ntest, bx * bt, nrhs);
+    else if (ntest <= 16) k_prolong0_add<T, TW, 16><<<grid, 256, 0, s>>>(W, vc, psi, nx, nt, bt, xe, te, ntest, bx * bt, nrhs);
+    else k_prolong0_add<T, TW, 32><<<grid, 256, 0, s>>>(W, vc, psi, nx, nt, bt, xe, te, ntest, bx * bt, nrhs);
 }
 
 template <typename T>
