@@ -330,6 +330,18 @@ __global__ void k_inv_norm2(const double2* d2, const int* flag, int nv, double* 
 
 int ensure_capacity(amg_context* c, int R);
 
+// AMG_SAP_FUSE=1 forms the SAP residual before each red colour (and the first) inside the
+// block solves instead of as a launch of its own.  It saves the residual launches (fine
+// operator 15.1 -> 8.6 ms per 32-source step) but the D apply from global memory at the start
+// of every block solve costs the SAP kernel more (154 -> 171 ms), so it is off by default.
+bool sap_fuse_enabled() {
+    static const int on = [] {
+        const char* e = getenv("AMG_SAP_FUSE");
+        return (e && e[0] == '1') ? 1 : 0;
+    }();
+    return on != 0;
+}
+
 int engine_cluster_limit() {
     const char* e = getenv("AMG_ENGINE_CLUSTER");
     int v = e ? atoi(e) : 16;
@@ -548,7 +560,16 @@ int fine_sap(amg_context* c, PrecSet<T>& ps, const cx<T>* v, long long vstride, 
     k_set_int<<<1, 256, 0, c->stream>>>(conv, 0, R);
     count_launch(2);
     launch_norm2<T>(v, len, vstride, R, partial, vnorm2, c->stream);
-    launch_residual<T>(U, v, vstride, x, r, c->nx, c->nt, R, m0, nullptr, nullptr, nullptr, c->stream);
+    // r = v - D x before every colour (src/sap.cpp:64-174).  With fusion (opt-in) the SAP
+    // launch forms it for its own blocks (launch_sap0's vfuse); the residual after the black
+    // colour stays a launch of its own because the early exit needs its norm over the whole
+    // lattice.
+    const bool fuse = sap_fuse_enabled();
+    bool r_fresh = false;
+    if (!fuse) {
+        launch_residual<T>(U, v, vstride, x, r, c->nx, c->nt, R, m0, nullptr, nullptr, nullptr, c->stream);
+        r_fresh = true;
+    }
     const int S = h.sxe * h.ste;
     const int use_smem = sap0_smem_bytes<T>(S, p.sap_gmres_m, 1) <= 200 * 1024;
     if (!use_smem) CKR(ps.sap_scratch.alloc((size_t)h.ncol * R * (p.sap_gmres_m + 5) * 2 * S * sizeof(cx<T>)));
@@ -561,14 +582,17 @@ int fine_sap(amg_context* c, PrecSet<T>& ps, const cx<T>* v, long long vstride, 
                 ProfScope ps_(c, AMG_PROF_SAP, (double)h.ncol * S * (2.0 + 6.0 * R) * sizeof(cx<T>));
                 CK(launch_sap0<T>(U, r, x, colour == 0 ? d_red : d_black, h.ncol, R, c->nx, c->nt, h.sbt, h.sxe,
                                   h.ste, m0, p.sap_gmres_m, p.sap_gmres_restarts, (T)p.sap_gmres_tol, use_smem,
-                                  scratch, nullptr, act, c->stream, c->sap_variant));
+                                  scratch, nullptr, act, c->stream, c->sap_variant, r_fresh ? nullptr : v,
+                                  vstride));
             }
+            r_fresh = false;
             const bool last = (colour == 1) && (it == nu - 1);
             if (last && !need_ret) break;
-            {
+            if (colour == 1 || !fuse) {
                 ProfScope ps_(c, AMG_PROF_FINE_OP, (double)c->N * (2.0 + 6.0 * R) * sizeof(cx<T>));
                 launch_residual<T>(U, v, vstride, x, r, c->nx, c->nt, R, m0, partial,
                                    colour == 1 ? norm2 : nullptr, act, c->stream);
+                r_fresh = true;
             }
             if (colour == 1) {
                 k_sap_check<<<1, 256, 0, c->stream>>>(norm2, vnorm2, p.sap_tol, act, conv, R);

@@ -8,68 +8,12 @@
 #include <type_traits>
 
 #include "kernels.h"
+#include "stencil.cuh"
 #include "sap_lean.cuh"
 #include "sap_f32.cuh"
 #include "sap_ca.cuh"
 
 namespace amgb {
-
-// ---------------------------------------------------------------------------------
-// D_phi / D_dagger_phi (src/dirac_operator.cpp:3-54) for one site.  With forward
-// neighbours (a,b) = psi(n+t), (c,d) = psi(n+x) and backward (e,f) = psi(n-t),
-// (g,h) = psi(n-x):
-//   D:   t0 = sR U0 (a-b), t1 = U1 (c+id), t2 = sL U0*(n-t) (e+f), t3 = U1*(n-x) (g-ih)
-//        out0 = (m0+2) p0 - (t0+t1+t2+t3)/2,  out1 = (m0+2) p1 - (-t0 - i t1 + t2 + i t3)/2
-//   D^+: the (1 -/+ sigma) projectors swap between forward and backward hops.
-// ---------------------------------------------------------------------------------
-// The geometry and links of one site, loaded once and reused for every source.
-template <typename T>
-struct SiteOp {
-    int r0, r1, l0, l1;        // neighbours n+t, n+x, n-t, n-x
-    cx<T> u0, u1, ul0, ul1;    // U_0(n), U_1(n), conj(U_0(n-t)), conj(U_1(n-x))
-    T sR, sL;                  // antiperiodic signs of the two time hops
-};
-
-template <typename T>
-__device__ __forceinline__ SiteOp<T> site_op(const cx<T>* __restrict__ U, int n, int nx, int nt) {
-    SiteOp<T> o;
-    const int x = n / nt, t = n - x * nt;
-    o.r0 = x * nt + ((t + 1 == nt) ? 0 : t + 1);
-    o.r1 = ((x + 1 == nx) ? 0 : x + 1) * nt + t;
-    o.l0 = x * nt + ((t == 0) ? nt - 1 : t - 1);
-    o.l1 = ((x == 0) ? nx - 1 : x - 1) * nt + t;
-    o.u0 = U[2 * n];
-    o.u1 = U[2 * n + 1];
-    o.ul0 = cconj(U[2 * o.l0]);
-    o.ul1 = cconj(U[2 * o.l1 + 1]);
-    o.sR = (t == nt - 1) ? T(-1) : T(1);
-    o.sL = (t == 0) ? T(-1) : T(1);
-    return o;
-}
-
-template <typename T, bool DAG>
-__device__ __forceinline__ void dirac_site(const SiteOp<T>& L, const cx<T>* __restrict__ psi, int n, T mass,
-                                           cx<T>& o0, cx<T>& o1) {
-    const cx<T> a = psi[2 * L.r0], b = psi[2 * L.r0 + 1];
-    const cx<T> c = psi[2 * L.r1], d = psi[2 * L.r1 + 1];
-    const cx<T> e = psi[2 * L.l0], f = psi[2 * L.l0 + 1];
-    const cx<T> g = psi[2 * L.l1], h = psi[2 * L.l1 + 1];
-    const cx<T> p0 = psi[2 * n], p1 = psi[2 * n + 1];
-    cx<T> t0, t1, t2, t3;
-    if (!DAG) {
-        t0 = L.sR * cmul(L.u0, a - b);
-        t1 = cmul(L.u1, c + cmuli(d));
-        t2 = L.sL * cmul(L.ul0, e + f);
-        t3 = cmul(L.ul1, g - cmuli(h));
-    } else {
-        t0 = L.sL * cmul(L.ul0, e - f);
-        t1 = cmul(L.ul1, g + cmuli(h));
-        t2 = L.sR * cmul(L.u0, a + b);
-        t3 = cmul(L.u1, c - cmuli(d));
-    }
-    o0 = mass * p0 - T(0.5) * (t0 + t1 + t2 + t3);
-    o1 = mass * p1 - T(0.5) * ((t2 - t0) + cmuli(t3 - t1));
-}
 
 // One thread per site; the sources rhs = blockIdx.y, blockIdx.y + gridDim.y, ... share the
 // site's links, which are read from memory once per source group instead of once per
@@ -798,22 +742,23 @@ cudaError_t launch_sap0_ca(const float2* U, const float2* r, float2* x, const in
 }
 
 template <int SPT, int NW, bool CGS = false>
-cudaError_t launch_sap0_f32(const float2* U, const float2* r, float2* x, const int* blocks, int ncol, int nrhs, int nx,
+cudaError_t launch_sap0_f32(const float2* U, float2* r, float2* x, const int* blocks, int ncol, int nrhs, int nx,
                             int nt, int sbt, int sxe, int ste, float m0, int restarts, float tol, int* iters,
-                            const int* act, cudaStream_t s) {
+                            const int* act, cudaStream_t s, const float2* vsrc, long long vstride) {
     const int bytes = sap0_f32_smem<5, SPT, NW, CGS>();
     cudaError_t e = cudaFuncSetAttribute(k_sap0_f32<5, SPT, NW, CGS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e != cudaSuccess) return e;
     dim3 grid(ncol, nrhs);
     k_sap0_f32<5, SPT, NW, CGS><<<grid, 32 * NW, bytes, s>>>(U, r, x, blocks, ncol, nx, nt, sbt, sxe, ste, m0, restarts,
-                                                             tol, act, iters);
+                                                             tol, act, iters, vsrc, vstride);
     return cudaGetLastError();
 }
 
 // FP32 solves of 64- to 1024-site blocks take the paired-FP32 kernel.
-static cudaError_t launch_sap0_paired(const float2* U, const float2* r, float2* x, const int* blocks, int ncol,
+static cudaError_t launch_sap0_paired(const float2* U, float2* r, float2* x, const int* blocks, int ncol,
                                       int nrhs, int nx, int nt, int sbt, int sxe, int ste, float m0, int restarts,
-                                      float tol, int* iters, const int* act, cudaStream_t s, bool* done, int v) {
+                                      float tol, int* iters, const int* act, cudaStream_t s, bool* done, int v,
+                                      const float2* vsrc, long long vstride) {
     *done = true;
     const int S = sxe * ste;
     // the paired kernel gives each thread a run of SPT consecutive t sites (SPT = 2 for 64-site
@@ -826,11 +771,11 @@ static cudaError_t launch_sap0_paired(const float2* U, const float2* r, float2* 
     }
     if (v == SAP_VARIANT_CGS) {
         switch (S) {
-            case 64: return launch_sap0_f32<2, 1, true>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
-            case 128: return launch_sap0_f32<4, 1, true>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
-            case 256: return launch_sap0_f32<4, 2, true>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
-            case 512: return launch_sap0_f32<4, 4, true>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
-            case 1024: return launch_sap0_f32<4, 8, true>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
+            case 64: return launch_sap0_f32<2, 1, true>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s, vsrc, vstride);
+            case 128: return launch_sap0_f32<4, 1, true>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s, vsrc, vstride);
+            case 256: return launch_sap0_f32<4, 2, true>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s, vsrc, vstride);
+            case 512: return launch_sap0_f32<4, 4, true>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s, vsrc, vstride);
+            case 1024: return launch_sap0_f32<4, 8, true>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s, vsrc, vstride);
             default: break;
         }
     }
@@ -846,20 +791,20 @@ static cudaError_t launch_sap0_paired(const float2* U, const float2* r, float2* 
     }
     if (g_sap0_spt == 2) {
         switch (S) {
-            case 64: return launch_sap0_f32<2, 1>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
-            case 128: return launch_sap0_f32<2, 2>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
-            case 256: return launch_sap0_f32<2, 4>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
-            case 512: return launch_sap0_f32<2, 8>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
-            case 1024: return launch_sap0_f32<2, 16>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
+            case 64: return launch_sap0_f32<2, 1>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s, vsrc, vstride);
+            case 128: return launch_sap0_f32<2, 2>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s, vsrc, vstride);
+            case 256: return launch_sap0_f32<2, 4>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s, vsrc, vstride);
+            case 512: return launch_sap0_f32<2, 8>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s, vsrc, vstride);
+            case 1024: return launch_sap0_f32<2, 16>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s, vsrc, vstride);
             default: break;
         }
     } else {
         switch (S) {
-            case 64: return launch_sap0_f32<2, 1>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
-            case 128: return launch_sap0_f32<4, 1>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
-            case 256: return launch_sap0_f32<4, 2>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
-            case 512: return launch_sap0_f32<4, 4>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
-            case 1024: return launch_sap0_f32<4, 8>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
+            case 64: return launch_sap0_f32<2, 1>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s, vsrc, vstride);
+            case 128: return launch_sap0_f32<4, 1>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s, vsrc, vstride);
+            case 256: return launch_sap0_f32<4, 2>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s, vsrc, vstride);
+            case 512: return launch_sap0_f32<4, 4>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s, vsrc, vstride);
+            case 1024: return launch_sap0_f32<4, 8>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s, vsrc, vstride);
             default: break;
         }
     }
@@ -871,9 +816,10 @@ static cudaError_t launch_sap0_paired(const float2* U, const float2* r, float2* 
 // kernel (sap_f32.cuh) in FP32 and the lean kernel (sap_lean.cuh) in FP64; any other shape
 // or restart length takes the generic kernel above.
 template <typename T>
-cudaError_t launch_sap0(const cx<T>* U, const cx<T>* r, cx<T>* x, const int* blocks, int ncol, int nrhs, int nx,
+cudaError_t launch_sap0(const cx<T>* U, cx<T>* r, cx<T>* x, const int* blocks, int ncol, int nrhs, int nx,
                         int nt, int sbt, int sxe, int ste, T m0, int m, int restarts, T tol, int use_smem,
-                        cx<T>* gscratch, int* iters, const int* act, cudaStream_t s, int variant) {
+                        cx<T>* gscratch, int* iters, const int* act, cudaStream_t s, int variant, const cx<T>* vfuse,
+                        long long vstride) {
     count_launch(1);
     const int S = sxe * ste;
     // variant: SAP_VARIANT_* (a context's tuned choice) or -1 for the environment's default
@@ -883,11 +829,27 @@ cudaError_t launch_sap0(const cx<T>* U, const cx<T>* r, cx<T>* x, const int* blo
         v = !sap0_warp_enabled() ? SAP_VARIANT_GENERIC : (f32 ? (g_sap0_f32_variant ? g_sap0_f32_variant : SAP_VARIANT_PAIRED)
                                                                : SAP_VARIANT_LEAN);
     }
+    if (vfuse) {
+        // r = v - D x inside the block solve: the paired kernels (MGS and CGS forms) on shapes
+        // they take, when no two blocks of one colour touch (an even number of blocks in both
+        // directions, so the red/black colouring is a checkerboard, wrap-around included);
+        // otherwise the residual runs as its own launch first
+        bool fused = false;
+        if constexpr (std::is_same<T, float>::value) {
+            const int spt = (S == 64 || (v != SAP_VARIANT_CGS && g_sap0_spt == 2)) ? 2 : 4;
+            fused = m == 5 && (v == SAP_VARIANT_PAIRED || v == SAP_VARIANT_CGS) && S >= 64 && S <= 1024 &&
+                    (S & (S - 1)) == 0 && ste % spt == 0 && (nx / sxe) % 2 == 0 && sbt % 2 == 0;
+        }
+        if (!fused) {
+            launch_residual<T>(U, vfuse, vstride, x, r, nx, nt, nrhs, m0, nullptr, nullptr, act, s);
+            vfuse = nullptr;
+        }
+    }
     if constexpr (std::is_same<T, float>::value) {
         if (m == 5 && (v == SAP_VARIANT_PAIRED || v == SAP_VARIANT_CA || v == SAP_VARIANT_CGS)) {
             bool done = false;
             const cudaError_t e = launch_sap0_paired(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts,
-                                                     tol, iters, act, s, &done, v);
+                                                     tol, iters, act, s, &done, v, vfuse, vstride);
             if (done) return e;
         }
     }
@@ -1045,8 +1007,9 @@ void launch_force(const double2* U, const double2* lam, const double2* x, double
                                      double*, double*, const int*, cudaStream_t);                                \
     template void launch_norm2<T>(const cx<T>*, long long, long long, int, double*, double*, cudaStream_t);      \
     template int sap0_smem_bytes<T>(int, int, int);                                                              \
-    template cudaError_t launch_sap0<T>(const cx<T>*, const cx<T>*, cx<T>*, const int*, int, int, int, int, int, \
-                                        int, int, T, int, int, T, int, cx<T>*, int*, const int*, cudaStream_t, int);
+    template cudaError_t launch_sap0<T>(const cx<T>*, cx<T>*, cx<T>*, const int*, int, int, int, int, int, \
+                                        int, int, T, int, int, T, int, cx<T>*, int*, const int*, cudaStream_t, int, \
+                                        const cx<T>*, long long);
 INST(double)
 INST(float)
 template void launch_restrict0<double, double2>(const double2*, const cx<double>*, cx<double>*, cx<double>*, int,

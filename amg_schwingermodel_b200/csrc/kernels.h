@@ -37,9 +37,13 @@ void set_sap0_warp(int on);
 // paired kernel with classical Gram-Schmidt and re-orthogonalisation on demand)
 enum { SAP_VARIANT_GENERIC = 0, SAP_VARIANT_LEAN = 1, SAP_VARIANT_PAIRED = 2, SAP_VARIANT_CA = 3, SAP_VARIANT_CGS = 4 };
 template <typename T>
-cudaError_t launch_sap0(const cx<T>* U, const cx<T>* r, cx<T>* x, const int* blocks, int ncol, int nrhs, int nx,
+// vfuse (optional): the SAP right-hand side v; r = v - D x is then formed for the colour's
+// blocks inside the launch (in a separate residual launch where the chosen kernel cannot)
+// and r is written there, instead of r being read as given
+cudaError_t launch_sap0(const cx<T>* U, cx<T>* r, cx<T>* x, const int* blocks, int ncol, int nrhs, int nx,
                         int nt, int sbt, int sxe, int ste, T m0, int m, int restarts, T tol, int use_smem,
-                        cx<T>* gscratch, int* iters, const int* act, cudaStream_t s, int variant = -1);
+                        cx<T>* gscratch, int* iters, const int* act, cudaStream_t s, int variant = -1,
+                        const cx<T>* vfuse = nullptr, long long vstride = 0);
 void launch_multidot(const double2* w, const double2* V, long long len, long long vstride, int nv, int nrhs,
                      double2* partial, int nparts, double2* out, const int* act, cudaStream_t s);
 void launch_axpy_multidot(double2* w, const double2* V, long long len, long long vstride, int nv, const double2* h,

@@ -14,6 +14,7 @@
 #pragma once
 #include "common.cuh"
 #include "sap_lean.cuh"
+#include "stencil.cuh"
 
 namespace amgb {
 
@@ -156,11 +157,12 @@ template <int M, int NW, bool CGS>
 constexpr int sap0_f32_pst() { return CGS ? NW * (M + 2) : NW * 2; }
 
 template <int M, int SPT, int NW, bool CGS = false>
-__global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const float2* __restrict__ U, const float2* __restrict__ r,
+__global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const float2* __restrict__ U, float2* __restrict__ r,
                                                           float2* __restrict__ xg, const int* __restrict__ blocks,
                                                           int ncol, int nx, int nt, int sbt, int sxe, int ste, float m0,
                                                           int restarts, float tol, const int* __restrict__ act,
-                                                          int* __restrict__ iters_out) {
+                                                          int* __restrict__ iters_out, const float2* __restrict__ vsrc,
+                                                          long long vstride) {
     constexpr int TPB = 32 * NW, S = TPB * SPT;
     constexpr int PST = sap0_f32_pst<M, NW, CGS>();
     extern __shared__ __align__(16) unsigned char smraw_f[];
@@ -303,7 +305,7 @@ __global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const float2* __restric
         }
     };
 
-    const float4* rb4 = reinterpret_cast<const float4*>(r + off);
+    float4* rb4 = reinterpret_cast<float4*>(r + off);
     // The iterate x lives in basis slot M, which the Arnoldi process never needs (the update
     // uses V_0..V_{M-1} and each cycle restarts from the true residual), so it holds no
     // registers during the Arnoldi steps and the residual's operator reads it in place.
@@ -313,8 +315,27 @@ __global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const float2* __restric
     {
         // r = b - A x0 (x0 = b)
         SiteP b[SPT];
+        if (vsrc) {
+            // fused SAP residual (src/sap.cpp:64-174 recomputes r = v - D x after every colour):
+            // b = v - D x on this block's sites, from the global iterate, whose halo belongs to
+            // blocks of the other colour that this launch does not write; b is kept in r for
+            // the restart residuals
+            const float2* xr = xg + off;
+            const float2* vr = vsrc + (long long)rhs * vstride;
 #pragma unroll
-        for (int k = 0; k < SPT; k++) b[k] = site_from_global(__ldg(&rb4[gs[k]]));
+            for (int k = 0; k < SPT; k++) {
+                const SiteOp<float> L = site_op<float>(U, gs[k], nx, nt);
+                float2 o0, o1;
+                dirac_site<float, false>(L, xr, gs[k], mass, o0, o1);
+                const float2 v0 = vr[2 * gs[k]], v1 = vr[2 * gs[k] + 1];
+                const float4 q = make_float4(v0.x - o0.x, v0.y - o0.y, v1.x - o1.x, v1.y - o1.y);
+                rb4[gs[k]] = q;
+                b[k] = site_from_global(q);
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < SPT; k++) b[k] = site_from_global(rb4[gs[k]]);
+        }
         store(X, b);
         normb = sqrtf(norm2(b));
         lean_sync<float, NW>();
@@ -526,7 +547,7 @@ __global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const float2* __restric
         apply(X, w, false);
 #pragma unroll
         for (int k = 0; k < SPT; k++) {
-            const SiteP b = site_from_global(__ldg(&rb4[gs[k]]));
+            const SiteP b = site_from_global(rb4[gs[k]]);
             w[k].re = p_sub(b.re, w[k].re);
             w[k].im = p_sub(b.im, w[k].im);
         }

@@ -1,9 +1,10 @@
 """The alternative kernel paths give the reference's results too: the generic and the lean
 fine-level SAP block solvers, and the coarse engine on one CTA or on thread-block clusters
 of 4 and 16 CTAs, in FP64; and in the mixed form (FP32 cycle inside the FP64 outer
-FGMRES) the paired-FP32 MGS SAP kernel (default) with four or two sites per thread, the
-paired kernel with classical Gram-Schmidt, the communication-avoiding FP32 kernel and the
-lean kernel.
+FGMRES) the paired-FP32 MGS SAP kernel (default) with four or two sites per thread, with
+its residual as a launch of its own (default) or formed inside the block solves
+(AMG_SAP_FUSE=1), the paired kernel with classical Gram-Schmidt, the
+communication-avoiding FP32 kernel and the lean kernel.
 Each variant runs in its own process (the choice is read from the environment once per
 process).  Mixed-precision bars: FP64 true residual <= 1e-10, x within 1e-8 of the
 reference's, at most one outer iteration more than the reference."""
@@ -50,11 +51,13 @@ print("RESULT" + json.dumps(out))
 @pytest.mark.parametrize("sap,cluster,prec", [
     ("generic", "1", 0), ("lean", "1", 0), ("lean", "4", 0), ("lean", "16", 0),
     ("ca", "16", 1), ("ca", "1", 1), ("paired", "16", 1), ("paired2", "16", 1), ("lean", "16", 1),
-    ("paired", "4", 1), ("cgs", "16", 1), ("cgs", "1", 1)])
+    ("paired", "4", 1), ("cgs", "16", 1), ("cgs", "1", 1), ("paired_fuse", "16", 1)])
 def test_variant_matches_reference(sap, cluster, prec):
     env = dict(os.environ, AMG_SAP_KERNEL=sap, AMG_ENGINE_CLUSTER=cluster)
     if sap == "paired2":
         env["AMG_SAP_SPT"] = "2"
+    if sap == "paired_fuse":
+        env.update(AMG_SAP_KERNEL="paired", AMG_SAP_FUSE="1")
     code = SCRIPT.format(root=str(ROOT), tests=str(ROOT / "tests"), prec=prec)
     p = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=600)
     assert p.returncode == 0, p.stderr[-3000:]
