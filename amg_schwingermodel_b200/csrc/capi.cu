@@ -342,6 +342,14 @@ bool sap_fuse_enabled() {
     return on != 0;
 }
 
+// the D apply's bounded bulk-copy waits (k_dirac_tma): AMG_ERR_DEVICE_WAIT if one gave up
+int check_fine_waits(cudaStream_t s) {
+    const int e = fine_error_check(s);
+    if (e < 0) return fail(AMG_ERR_CUDA, "reading the device error flag: %s", cudaGetErrorString(cudaGetLastError()));
+    if (e > 0) return fail(AMG_ERR_DEVICE_WAIT, "a bulk-copy wait of the Dirac apply gave up");
+    return AMG_OK;
+}
+
 int engine_cluster_limit() {
     const char* e = getenv("AMG_ENGINE_CLUSTER");
     int v = e ? atoi(e) : 16;
@@ -1469,7 +1477,7 @@ int amg_dirac_apply_dev(amg_ctx c, const void* in, void* out, int nrhs, int dagg
                          dagger ? 1 : 0, c->stream);
     CKL();
     CK(cudaStreamSynchronize(c->stream));
-    return AMG_OK;
+    return check_fine_waits(c->stream);
 }
 
 int amg_dirac_apply(amg_ctx c, const double* in, double* out, int nrhs, int dagger) {
@@ -1483,7 +1491,8 @@ int amg_dirac_apply(amg_ctx c, const double* in, double* out, int nrhs, int dagg
     launch_dirac<double>(c->d.U.as<double2>(), a.as<double2>(), b.as<double2>(), c->nx, c->nt, nrhs, c->m0,
                          dagger ? 1 : 0, c->stream);
     CKL();
-    return to_host(out, b, n, c->stream);
+    CKR(to_host(out, b, n, c->stream));
+    return check_fine_waits(c->stream);
 }
 
 int amg_dirac_apply_raw(const void* U_dev, const void* in_dev, void* out_dev, int nx, int nt, int nrhs, double m0,
@@ -1505,7 +1514,8 @@ int amg_dirac_apply_host(const double* U, const double* in, double* out, int nx,
     CKR(to_dev(b, nullptr, 2 * N * nrhs, 0));
     launch_dirac<double>(u.as<double2>(), a.as<double2>(), b.as<double2>(), nx, nt, nrhs, m0, dagger ? 1 : 0, 0);
     CKL();
-    return to_host(out, b, 2 * N * nrhs, 0);
+    CKR(to_host(out, b, 2 * N * nrhs, 0));
+    return check_fine_waits(0);
 }
 
 int amg_set_initial_test_vectors(amg_ctx c, int level, const double* W) {
@@ -1721,6 +1731,7 @@ int amg_solve_dev(amg_ctx c, const void* b_dev, void* x_dev, int nrhs, amg_solve
     int flags = 0;
     CK(cudaMemcpy(&flags, c->d.eh.flags, sizeof(int), cudaMemcpyDeviceToHost));
     if (flags) return fail(AMG_ERR_UNSUPPORTED, "engine reported flags %d", flags);
+    CKR(check_fine_waits(c->stream));
     return rc;
 }
 
@@ -1787,6 +1798,7 @@ int solve_many(int count, const amg_ctx* ctx, const double2* const* b, double2* 
         int flags = 0;
         CK(cudaMemcpy(&flags, c->d.eh.flags, sizeof(int), cudaMemcpyDeviceToHost));
         if (flags) return fail(AMG_ERR_UNSUPPORTED, "engine of context %d reported flags %d", i, flags);
+        CKR(check_fine_waits(c->stream));
         if (S[i].rc == AMG_NOT_CONVERGED) rc = AMG_NOT_CONVERGED;
     }
     return rc;

@@ -9,6 +9,7 @@
 
 #include "kernels.h"
 #include "stencil.cuh"
+#include "dirac_tma.cuh"
 #include "sap_lean.cuh"
 #include "sap_f32.cuh"
 #include "sap_ca.cuh"
@@ -602,10 +603,47 @@ static int source_groups(int nsites, int nrhs) {
     return std::max(1, std::min(nrhs, want));
 }
 
+// AMG_DIRAC_TMA=0 keeps every D apply on k_dirac (A/B tests)
+static int dirac_tma_enabled() {
+    static const int on = [] {
+        const char* e = getenv("AMG_DIRAC_TMA");
+        return (e && e[0] == '0') ? 0 : 1;
+    }();
+    return on;
+}
+
+// bit 0 of the device error flag: a bulk-copy wait of k_dirac_tma gave up (the flag is read
+// and cleared; the read synchronises the stream)
+int fine_error_check(cudaStream_t s) {
+    int h = 0;
+    if (cudaMemcpyFromSymbolAsync(&h, g_fine_err, sizeof(int), 0, cudaMemcpyDeviceToHost, s) != cudaSuccess) return -1;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return -1;
+    if (h) {
+        const int z = 0;
+        cudaMemcpyToSymbolAsync(g_fine_err, &z, sizeof(int), 0, cudaMemcpyHostToDevice, s);
+    }
+    return h;
+}
+
 template <typename T>
 void launch_dirac(const cx<T>* U, const cx<T>* in, cx<T>* out, int nx, int nt, int nrhs, T m0, int dagger,
                   cudaStream_t s) {
     count_launch(1);
+    // lattices tiled by kTX x kTT sites with 16-byte aligned, distinct spinors take the
+    // bulk-copy kernel
+    if (dirac_tma_enabled() && nrhs >= 1 && nt % kTT == 0 && nx % kTX == 0 && nx >= kTX && in != out &&
+        ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15) == 0) {
+        constexpr int bytes = dirac_tma_smem<T>();
+        dim3 g(nt / kTT, nx / kTX);
+        if (dagger) {
+            cudaFuncSetAttribute(k_dirac_tma<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+            k_dirac_tma<T, true><<<g, kTT, bytes, s>>>(U, in, out, nx, nt, m0, nrhs);
+        } else {
+            cudaFuncSetAttribute(k_dirac_tma<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+            k_dirac_tma<T, false><<<g, kTT, bytes, s>>>(U, in, out, nx, nt, m0, nrhs);
+        }
+        return;
+    }
     dim3 grid((nx * nt + 255) / 256, source_groups(nx * nt, nrhs));
     if (dagger) k_dirac<T, true><<<grid, 256, 0, s>>>(U, in, out, nx, nt, m0, nrhs);
     else k_dirac<T, false><<<grid, 256, 0, s>>>(U, in, out, nx, nt, m0, nrhs);

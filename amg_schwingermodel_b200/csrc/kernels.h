@@ -15,6 +15,9 @@ inline void count_launch(int n = 1) { __atomic_add_fetch(&g_launches, (long long
 template <typename T>
 void launch_dirac(const cx<T>* U, const cx<T>* in, cx<T>* out, int nx, int nt, int nrhs, T m0, int dagger,
                   cudaStream_t s);
+// reads and clears the fine kernels' device error flag (bit 0: a bulk-copy wait of the D
+// apply gave up); synchronises the stream; -1 on a CUDA error
+int fine_error_check(cudaStream_t s);
 template <typename T>
 void launch_residual(const cx<T>* U, const cx<T>* b, long long bstride, const cx<T>* x, cx<T>* r, int nx, int nt,
                      int nrhs, T m0, double* partial, double* norm2_out, const int* act, cudaStream_t s);
