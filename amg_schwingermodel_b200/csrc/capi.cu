@@ -1504,6 +1504,16 @@ int amg_dirac_apply_raw(const void* U_dev, const void* in_dev, void* out_dev, in
     return AMG_OK;
 }
 
+int amg_debug_dirac_wait_test(const void* U_dev, const void* in_dev, void* out_dev, int nx, int nt, int nrhs) {
+    if (!U_dev || !in_dev || !out_dev || nx < 2 || nt < 2 || nrhs < 1) return fail(AMG_ERR_INVALID, "bad argument");
+    const int r = dirac_tma_wait_test((const double2*)U_dev, (const double2*)in_dev, (double2*)out_dev, nx, nt, nrhs,
+                                      0);
+    if (r < 0) return fail(AMG_ERR_INVALID, "lattice or buffers outside the bulk-copy kernel, or a CUDA error: %s",
+                           cudaGetErrorString(cudaGetLastError()));
+    if (r > 0) return fail(AMG_ERR_DEVICE_WAIT, "a bulk-copy wait of the Dirac apply gave up (self-test)");
+    return AMG_OK;
+}
+
 int amg_dirac_apply_host(const double* U, const double* in, double* out, int nx, int nt, int nrhs, double m0,
                          int dagger) {
     if (!U || !in || !out || nx < 2 || nt < 2 || nrhs < 1) return fail(AMG_ERR_INVALID, "bad argument");

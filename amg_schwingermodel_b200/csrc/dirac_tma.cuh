@@ -12,7 +12,9 @@
 //
 // Every wait on an mbarrier is bounded: after kTmaSpinLimit polls the kernel sets bit 0 of
 // the device flag g_fine_err, waits (bounded again) for the copies it still has in flight and
-// returns; the host reads the flag after the work (fine_error_check).
+// returns; the host reads the flag after the work (fine_error_check).  dirac_tma_wait_test
+// runs the kernel without issuing any copy, so its first wait runs out with nothing in flight,
+// and returns the flag (the self-test of that path).
 #pragma once
 #include "common.cuh"
 #include "stencil.cuh"
@@ -34,9 +36,9 @@ __device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
 __device__ __forceinline__ void mbar_arrive_expect_tx(unsigned bar, unsigned bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
 }
-// true once the phase with this parity has completed, false after the poll limit
-__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
-    for (int i = 0; i < kTmaSpinLimit; i++) {
+// true once the phase with this parity has completed, false after `limit` polls
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, int limit) {
+    for (int i = 0; i < limit; i++) {
         unsigned done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -67,9 +69,12 @@ __host__ __device__ constexpr int dirac_tma_buf_bytes() {
 template <typename T>
 __host__ __device__ constexpr int dirac_tma_smem() { return 2 * dirac_tma_buf_bytes<T>() + 16; }
 
+// wait_limit: polls per mbarrier wait (kTmaSpinLimit); self_test: issue no copies at all, so
+// the first wait runs out with nothing in flight (the bounded-wait self-test)
 template <typename T, bool DAG>
 __global__ void __launch_bounds__(kTT, 2) k_dirac_tma(const cx<T>* __restrict__ U, const cx<T>* __restrict__ in,
-                                                      cx<T>* __restrict__ out, int nx, int nt, T m0, int nrhs) {
+                                                      cx<T>* __restrict__ out, int nx, int nt, T m0, int nrhs,
+                                                      int wait_limit, int self_test) {
     extern __shared__ __align__(128) unsigned char smraw_d[];
     constexpr int RS = dirac_tma_row_sites<T>();       // sites per staged row segment
     constexpr int SB = 2 * (int)sizeof(cx<T>);          // bytes per site (both spins)
@@ -123,16 +128,16 @@ __global__ void __launch_bounds__(kTT, 2) k_dirac_tma(const cx<T>* __restrict__ 
         L[r].r1 = c + RS;
         L[r].l1 = c - RS;
     }
-    if (tid < 32) {
+    if (tid < 32 && !self_test) {
         issue(0, 0);
         if (nrhs > 1) issue(1, 1);
     }
-    int issued = nrhs > 1 ? 2 : 1;     // sources whose copies have been issued
+    int issued = self_test ? 0 : (nrhs > 1 ? 2 : 1);   // sources whose copies have been issued
     const T mass = m0 + T(2);
     int done = 0;                      // sources whose copies every thread has seen land
     for (int rhs = 0; rhs < nrhs; rhs++) {
         const int b = rhs & 1;
-        const bool ok = mbar_wait(b ? bar1 : bar0, (unsigned)((rhs >> 1) & 1));
+        const bool ok = mbar_wait(b ? bar1 : bar0, (unsigned)((rhs >> 1) & 1), wait_limit);
         // one decision for the whole CTA, so no thread leaves the barriers below
         if (__syncthreads_or(!ok)) break;
         done = rhs + 1;
@@ -160,7 +165,8 @@ __global__ void __launch_bounds__(kTT, 2) k_dirac_tma(const cx<T>* __restrict__ 
         if (tid == 0) atomicOr(&g_fine_err, 1);
         // let the copies still in flight land before the CTA's shared memory goes away (the
         // waits are bounded like the others)
-        for (int q = done; q < issued; q++) (void)mbar_wait((q & 1) ? bar1 : bar0, (unsigned)((q >> 1) & 1));
+        for (int q = done; q < issued; q++)
+            (void)mbar_wait((q & 1) ? bar1 : bar0, (unsigned)((q >> 1) & 1), wait_limit);
     }
 }
 

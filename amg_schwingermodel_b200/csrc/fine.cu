@@ -625,6 +625,23 @@ int fine_error_check(cudaStream_t s) {
     return h;
 }
 
+// The bounded-wait self-test: k_dirac_tma without any copy issued and 256 polls per wait, so
+// the first wait runs out with nothing in flight; returns the device flag afterwards (1 when
+// the kernel reported the timeout, 0 if it did not, -1 on a CUDA error or a lattice the
+// kernel does not take).
+int dirac_tma_wait_test(const double2* U, const double2* in, double2* out, int nx, int nt, int nrhs, cudaStream_t s) {
+    if (nrhs < 1 || nt % kTT != 0 || nx % kTX != 0 || in == out ||
+        ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15) != 0)
+        return -1;
+    constexpr int bytes = dirac_tma_smem<double>();
+    if (cudaFuncSetAttribute(k_dirac_tma<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) !=
+        cudaSuccess)
+        return -1;
+    k_dirac_tma<double, false><<<dim3(nt / kTT, nx / kTX), kTT, bytes, s>>>(U, in, out, nx, nt, -0.1, nrhs, 256, 1);
+    if (cudaGetLastError() != cudaSuccess) return -1;
+    return fine_error_check(s);
+}
+
 template <typename T>
 void launch_dirac(const cx<T>* U, const cx<T>* in, cx<T>* out, int nx, int nt, int nrhs, T m0, int dagger,
                   cudaStream_t s) {
@@ -637,10 +654,10 @@ void launch_dirac(const cx<T>* U, const cx<T>* in, cx<T>* out, int nx, int nt, i
         dim3 g(nt / kTT, nx / kTX);
         if (dagger) {
             cudaFuncSetAttribute(k_dirac_tma<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-            k_dirac_tma<T, true><<<g, kTT, bytes, s>>>(U, in, out, nx, nt, m0, nrhs);
+            k_dirac_tma<T, true><<<g, kTT, bytes, s>>>(U, in, out, nx, nt, m0, nrhs, kTmaSpinLimit, 0);
         } else {
             cudaFuncSetAttribute(k_dirac_tma<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-            k_dirac_tma<T, false><<<g, kTT, bytes, s>>>(U, in, out, nx, nt, m0, nrhs);
+            k_dirac_tma<T, false><<<g, kTT, bytes, s>>>(U, in, out, nx, nt, m0, nrhs, kTmaSpinLimit, 0);
         }
         return;
     }

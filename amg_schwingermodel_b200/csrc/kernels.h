@@ -18,6 +18,8 @@ void launch_dirac(const cx<T>* U, const cx<T>* in, cx<T>* out, int nx, int nt, i
 // reads and clears the fine kernels' device error flag (bit 0: a bulk-copy wait of the D
 // apply gave up); synchronises the stream; -1 on a CUDA error
 int fine_error_check(cudaStream_t s);
+// runs the bulk-copy D apply with waits that cannot complete and returns the device flag
+int dirac_tma_wait_test(const double2* U, const double2* in, double2* out, int nx, int nt, int nrhs, cudaStream_t s);
 template <typename T>
 void launch_residual(const cx<T>* U, const cx<T>* b, long long bstride, const cx<T>* x, cx<T>* r, int nx, int nt,
                      int nrhs, T m0, double* partial, double* norm2_out, const int* act, cudaStream_t s);

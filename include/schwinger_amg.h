@@ -126,6 +126,13 @@ AMG_API int amg_dirac_apply_dev(amg_ctx ctx, const void* in, void* out, int nrhs
  * in_dev / out_dev [nrhs][N][2] complex128, launched on `stream` (a cudaStream_t). */
 AMG_API int amg_dirac_apply_raw(const void* U_dev, const void* in_dev, void* out_dev, int nx, int nt,
                         int nrhs, double m0, int dagger, void* stream);
+/* Self-test of the bounded device waits (no reference counterpart): runs the bulk-copy D apply
+ * on caller-owned device memory (nt a multiple of 256, nx of 4, 16-byte aligned, distinct
+ * in/out) without issuing its copies, so its first wait gives up after a short poll limit
+ * with nothing in flight.  Returns AMG_ERR_DEVICE_WAIT when the kernel reported that (the
+ * expected outcome), AMG_OK if it did not, AMG_ERR_INVALID for a lattice the kernel does not
+ * take.  out is left undefined; the device stays usable. */
+AMG_API int amg_debug_dirac_wait_test(const void* U_dev, const void* in_dev, void* out_dev, int nx, int nt, int nrhs);
 /* Stand-alone FP64 stencil on host arrays, no context: D_phi / D_dagger_phi
  * (src/dirac_operator.cpp:3-54) with the reference's signature data (U[N][2], in/out
  * [nrhs][N][2]); device buffers are allocated and freed inside the call. */
