@@ -225,6 +225,9 @@ struct amg_context {
     int graphs_off = 0;            // capture failed once: run eagerly from then on
     // autotuner state: the fine SAP kernel variant (-1: default) and whether it ran
     int sap_variant = -1, tuned = 0;
+    // the FP64 vector whose FP32 copy the mixed preconditioner's input buffer vf holds (the
+    // outer FGMRES writes that copy while it normalises the basis vector), or null
+    const void* vf_src = nullptr;
     double tuned_us = 0;
     void drop_graphs() {
         for (auto& kv : graphs)
@@ -709,7 +712,10 @@ int precondition(amg_context* c, const double2* v, double2* z, int R) {
     }
     float2* vf = c->vf.as<float2>();
     float2* zf = c->zf.as<float2>();
-    launch_d2f(vf, v, R * len, c->stream);
+    if (c->vf_src != v) {
+        launch_d2f(vf, v, R * len, c->stream);
+        c->vf_src = v;
+    }
     CKR(run_graph(c, std::make_tuple(1, R, (const void*)vf, (void*)zf), [&]() -> int {
         CK(cudaMemsetAsync(zf, 0, (size_t)R * len * sizeof(float2), c->stream));
         return fine_cycle<float>(c, c->f, vf, zf, R, true);
@@ -825,6 +831,7 @@ struct OuterSolve {
 
     int init(amg_context* c_, const double2* b_, double2* x_, int R_, amg_solve_info* info_) {
         c = c_; b = b_; x = x_; R = R_; info = info_;
+        c->vf_src = nullptr;
         const amg_params& p = c->p;
         m = p.outer_m;
         len = vlen0(c);
@@ -886,7 +893,9 @@ struct OuterSolve {
         CKR(upload_masks());
         CK(cudaMemcpyAsync(c->scal.p, h_scal, R * sizeof(double), cudaMemcpyHostToDevice, c->stream));
         double2* V = c->V.as<double2>();
-        launch_scale(V, V, len, c->scal.as<double>(), act_d(), R, c->stream);
+        float2* yf = c->p.precision == AMG_PREC_MIXED ? c->vf.as<float2>() : nullptr;
+        launch_scale(V, V, len, c->scal.as<double>(), act_d(), R, c->stream, yf);
+        c->vf_src = yf ? V : nullptr;
         j = 0;
         return issue_step();
     }
@@ -921,9 +930,12 @@ struct OuterSolve {
                                                   sm_d(), R);
             count_launch(2);
             double2* Vn = V + (long long)(j + 1) * vstride;
+            // (mixed precision: the FP32 copy of V_{j+1} for the next preconditioner call too)
+            float2* yf = c->p.precision == AMG_PREC_MIXED ? c->vf.as<float2>() : nullptr;
             launch_axpy_scale_to(Vn, w, V, len, vstride, nv, d2, nv + 1, c->scal.as<double>(), pm_d(), R, dpart, np,
-                                 c->stream);
-            launch_scale(Vn, w, len, c->scal.as<double>(), sm_d(), R, c->stream);
+                                 c->stream, yf);
+            launch_scale(Vn, w, len, c->scal.as<double>(), sm_d(), R, c->stream, yf);
+            c->vf_src = yf ? Vn : nullptr;
         }
         CK(cudaMemcpyAsync(h_dots, dots, (size_t)R * 2 * (nv + 1) * sizeof(double2), cudaMemcpyDeviceToHost,
                            c->stream));
@@ -1090,6 +1102,7 @@ int ensure_capacity(amg_context* c, int R) {
         CKR(c->zd.alloc((size_t)Rn * len * sizeof(double2)));
     }
     if (c->p.precision == AMG_PREC_MIXED) {
+        c->vf_src = nullptr;
         CKR(c->vf.alloc((size_t)Rn * len * sizeof(float2)));
         CKR(c->zf.alloc((size_t)Rn * len * sizeof(float2)));
         CKR(alloc_fine<float>(c, c->f, Rn));
@@ -1166,6 +1179,7 @@ int build_mixed(amg_context* c) {
     }
     CKR(build_engine<float>(c, f, c->d.eng_cap));
     CKR(alloc_fine<float>(c, f, c->Rcap));
+    c->vf_src = nullptr;
     CKR(c->vf.alloc((size_t)c->Rcap * len * sizeof(float2)));
     CKR(c->zf.alloc((size_t)c->Rcap * len * sizeof(float2)));
     f.ready = 1;

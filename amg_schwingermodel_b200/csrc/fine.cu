@@ -489,7 +489,8 @@ __global__ void __launch_bounds__(256, (NV <= 8 ? 2 : 1)) k_axpy_dots(double2* _
                                                       long long len, long long vstride, int nv,
                                                       const double2* __restrict__ h, int hstride, int nd,
                                                       const int* __restrict__ act, double2* __restrict__ partial,
-                                                      double2* __restrict__ y, const double* __restrict__ sc) {
+                                                      double2* __restrict__ y, const double* __restrict__ sc,
+                                                      float2* __restrict__ yf) {
     __shared__ double red[8][2 * (NV + 1)];
     __shared__ double2 hk[NV];   // the axpy coefficients, read as broadcasts (fewer live registers)
     const int rhs = blockIdx.y;
@@ -505,6 +506,7 @@ __global__ void __launch_bounds__(256, (NV <= 8 ? 2 : 1)) k_axpy_dots(double2* _
     const int nload = (h && nv > nd) ? nv : nd;
     const double f = y ? sc[rhs] : 1.0;
     double2* yy = y ? y + (long long)rhs * len : nullptr;
+    float2* yyf = yf ? yf + (long long)rhs * len : nullptr;
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (long long)gridDim.x * blockDim.x) {
         double2 a = ww[e];
         // every V_k element is loaded once and kept for both the update and the dots
@@ -519,8 +521,13 @@ __global__ void __launch_bounds__(256, (NV <= 8 ? 2 : 1)) k_axpy_dots(double2* _
                     a.y -= hk[k].x * bk[k].y + hk[k].y * bk[k].x;
                 }
             }
-            if (yy) yy[e] = make_double2(f * a.x, f * a.y);
-            else ww[e] = a;
+            if (yy) {
+                const double2 o = make_double2(f * a.x, f * a.y);
+                yy[e] = o;
+                if (yyf) yyf[e] = make_float2((float)o.x, (float)o.y);
+            } else {
+                ww[e] = a;
+            }
         }
 #pragma unroll
         for (int k = 0; k < NV; k++) {
@@ -570,13 +577,18 @@ __global__ void __launch_bounds__(256) k_multiaxpy_add(double2* __restrict__ x, 
 }
 
 // y[rhs] = s[rhs] * x[rhs]  (masked; s real)
+// y = s[rhs] x, and yf = (float) y when yf is given (the FP32 copy the mixed-precision
+// preconditioner reads)
 __global__ void k_scale(double2* __restrict__ y, const double2* __restrict__ x, long long len,
-                        const double* __restrict__ s, const int* __restrict__ act) {
+                        const double* __restrict__ s, const int* __restrict__ act, float2* __restrict__ yf) {
     const int rhs = blockIdx.y;
     if (act && !act[rhs]) return;
     const double f = s[rhs];
-    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (long long)gridDim.x * blockDim.x)
-        y[(long long)rhs * len + e] = f * x[(long long)rhs * len + e];
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (long long)gridDim.x * blockDim.x) {
+        const double2 v = f * x[(long long)rhs * len + e];
+        y[(long long)rhs * len + e] = v;
+        if (yf) yf[(long long)rhs * len + e] = make_float2((float)v.x, (float)v.y);
+    }
 }
 
 // precision conversions between the FP64 outer vectors and the FP32 cycle
@@ -930,9 +942,9 @@ cudaError_t launch_sap0(const cx<T>* U, cx<T>* r, cx<T>* x, const int* blocks, i
 template <int NV>
 static void axpy_dots_nv(double2* w, const double2* V, long long len, long long vstride, int nv, const double2* h,
                          int hstride, int nd, const int* act, int nrhs, double2* partial, int nparts, cudaStream_t s,
-                         double2* y = nullptr, const double* sc = nullptr) {
+                         double2* y = nullptr, const double* sc = nullptr, float2* yf = nullptr) {
     dim3 grid(nparts, nrhs);
-    k_axpy_dots<NV><<<grid, 256, 0, s>>>(w, V, len, vstride, nv, h, hstride, nd, act, partial, y, sc);
+    k_axpy_dots<NV><<<grid, 256, 0, s>>>(w, V, len, vstride, nv, h, hstride, nd, act, partial, y, sc, yf);
 }
 
 // w -= sum_{k<nv} h[k] V_k (h may be null), then out[rhs][k] = <w, V_k> for k < nd and
@@ -952,14 +964,14 @@ void launch_axpy_multidot(double2* w, const double2* V, long long len, long long
 
 void launch_axpy_scale_to(double2* y, const double2* w, const double2* V, long long len, long long vstride, int nv,
                           const double2* h, int hstride, const double* sc, const int* act, int nrhs, double2* partial,
-                          int nparts, cudaStream_t s) {
+                          int nparts, cudaStream_t s, float2* yf) {
     count_launch(1);
     double2* ww = const_cast<double2*>(w);   // read only when y is given
-    if (nv <= 4) axpy_dots_nv<4>(ww, V, len, vstride, nv, h, hstride, 0, act, nrhs, partial, nparts, s, y, sc);
-    else if (nv <= 8) axpy_dots_nv<8>(ww, V, len, vstride, nv, h, hstride, 0, act, nrhs, partial, nparts, s, y, sc);
-    else if (nv <= 12) axpy_dots_nv<12>(ww, V, len, vstride, nv, h, hstride, 0, act, nrhs, partial, nparts, s, y, sc);
-    else if (nv <= 16) axpy_dots_nv<16>(ww, V, len, vstride, nv, h, hstride, 0, act, nrhs, partial, nparts, s, y, sc);
-    else axpy_dots_nv<24>(ww, V, len, vstride, nv, h, hstride, 0, act, nrhs, partial, nparts, s, y, sc);
+    if (nv <= 4) axpy_dots_nv<4>(ww, V, len, vstride, nv, h, hstride, 0, act, nrhs, partial, nparts, s, y, sc, yf);
+    else if (nv <= 8) axpy_dots_nv<8>(ww, V, len, vstride, nv, h, hstride, 0, act, nrhs, partial, nparts, s, y, sc, yf);
+    else if (nv <= 12) axpy_dots_nv<12>(ww, V, len, vstride, nv, h, hstride, 0, act, nrhs, partial, nparts, s, y, sc, yf);
+    else if (nv <= 16) axpy_dots_nv<16>(ww, V, len, vstride, nv, h, hstride, 0, act, nrhs, partial, nparts, s, y, sc, yf);
+    else axpy_dots_nv<24>(ww, V, len, vstride, nv, h, hstride, 0, act, nrhs, partial, nparts, s, y, sc, yf);
 }
 
 void launch_multidot(const double2* w, const double2* V, long long len, long long vstride, int nv, int nrhs,
@@ -981,10 +993,10 @@ void launch_multiaxpy_add(double2* x, const double2* Z, long long len, long long
     k_multiaxpy_add<<<grid, 256, 0, s>>>(x, Z, len, vstride, nv, c, cstride, nvr, act);
 }
 void launch_scale(double2* y, const double2* x, long long len, const double* sc, const int* act, int nrhs,
-                  cudaStream_t s) {
+                  cudaStream_t s, float2* yf) {
     count_launch(1);
     dim3 grid(592, nrhs);
-    k_scale<<<grid, 256, 0, s>>>(y, x, len, sc, act);
+    k_scale<<<grid, 256, 0, s>>>(y, x, len, sc, act, yf);
 }
 void launch_d2f(float2* y, const double2* x, long long n, cudaStream_t s) {
     count_launch(1); k_d2f<<<592, 256, 0, s>>>(y, x, n); }

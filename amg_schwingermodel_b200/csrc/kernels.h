@@ -62,9 +62,10 @@ void launch_multiaxpy_add(double2* x, const double2* Z, long long len, long long
 // unused |w|^2 partials)
 void launch_axpy_scale_to(double2* y, const double2* w, const double2* V, long long len, long long vstride, int nv,
                           const double2* h, int hstride, const double* sc, const int* act, int nrhs, double2* partial,
-                          int nparts, cudaStream_t s);
+                          int nparts, cudaStream_t s, float2* yf = nullptr);
+// y = sc[rhs] x for the sources with act; yf (optional) receives the FP32 copy of y
 void launch_scale(double2* y, const double2* x, long long len, const double* sc, const int* act, int nrhs,
-                  cudaStream_t s);
+                  cudaStream_t s, float2* yf = nullptr);
 void launch_d2f(float2* y, const double2* x, long long n, cudaStream_t s);
 void launch_f2d(double2* y, const float2* x, long long n, cudaStream_t s);
 void launch_d2bf(__nv_bfloat162* y, const double2* x, long long n, cudaStream_t s);
