@@ -696,7 +696,10 @@ int run_graph(amg_context* c, const std::tuple<int, int, const void*, void*>& ke
     return AMG_OK;
 }
 
-int precondition(amg_context* c, const double2* v, double2* z, int R) {
+// z = M v for R sources.  Mixed precision with want_z = false leaves the FP32 result in c->zf
+// for the caller (the outer step promotes it while applying D), instead of converting it
+// into z.
+int precondition(amg_context* c, const double2* v, double2* z, int R, bool want_z = true) {
     const long long len = vlen0(c);
     if (c->p.precision == AMG_PREC_F64) {
         // staged through fixed buffers, so one graph serves every Krylov slot
@@ -720,7 +723,7 @@ int precondition(amg_context* c, const double2* v, double2* z, int R) {
         CK(cudaMemsetAsync(zf, 0, (size_t)R * len * sizeof(float2), c->stream));
         return fine_cycle<float>(c, c->f, vf, zf, R, true);
     }));
-    launch_f2d(z, zf, R * len, c->stream);
+    if (want_z) launch_f2d(z, zf, R * len, c->stream);
     CKL();
     return AMG_OK;
 }
@@ -763,9 +766,9 @@ int autotune(amg_context* c, const double2* v, double2* z, int R) {
         for (int cs : clusters) {
             c->sap_variant = vv;
             *pick = cs;
-            if ((rc = precondition(c, v, z, R)) < 0) break;   // warm-up (attributes, lazy buffers)
+            if ((rc = precondition(c, v, z, R, false)) < 0) break;   // warm-up (attributes, lazy buffers)
             cudaEventRecord(a, c->stream);
-            if ((rc = precondition(c, v, z, R)) < 0) break;
+            if ((rc = precondition(c, v, z, R, false)) < 0) break;
             cudaEventRecord(b, c->stream);
             cudaEventSynchronize(b);
             float ms = 0;
@@ -911,10 +914,15 @@ struct OuterSolve {
         double2* Vj = V + (long long)j * vstride;
         double2* Zj = Z + (long long)j * vstride;
         if (!c->tuned && !c->prof_on) CKR(autotune(c, Vj, Zj, R));
-        CKR(precondition(c, Vj, Zj, R));
+        const bool mixed = c->p.precision == AMG_PREC_MIXED;
+        CKR(precondition(c, Vj, Zj, R, !mixed));
         {
             ProfScope ps_(c, AMG_PROF_FINE_OP, (double)c->N * (2.0 + 4.0 * R) * sizeof(double2));
-            launch_dirac<double>(c->d.U.as<double2>(), Zj, w, c->nx, c->nt, R, c->m0, 0, c->stream);
+            if (mixed)   // w = D z_j from the FP32 preconditioner output, Z_j = its FP64 promotion
+                launch_dirac_promote(c->d.U.as<double2>(), c->zf.as<float2>(), w, Zj, c->nx, c->nt, R, c->m0,
+                                     c->stream);
+            else
+                launch_dirac<double>(c->d.U.as<double2>(), Zj, w, c->nx, c->nt, R, c->m0, 0, c->stream);
         }
         const int nv = j + 1;
         double2* d1 = dots;

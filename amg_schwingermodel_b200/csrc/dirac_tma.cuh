@@ -59,27 +59,28 @@ __device__ __forceinline__ void bulk_g2s(unsigned dst, const void* src, unsigned
         : "memory");
 }
 
-template <typename T>
-__host__ __device__ constexpr int dirac_tma_row_sites() { return kTT + 2; }
-template <typename T>
+// shared memory per tile buffer for spinors stored as TIN
+template <typename TIN>
 __host__ __device__ constexpr int dirac_tma_buf_bytes() {
-    return (kTX + 2) * dirac_tma_row_sites<T>() * 2 * (int)sizeof(cx<T>);
+    return (kTX + 2) * (kTT + 2) * 2 * (int)sizeof(cx<TIN>);
 }
 // dynamic shared memory: two tile buffers, then two mbarriers
-template <typename T>
-__host__ __device__ constexpr int dirac_tma_smem() { return 2 * dirac_tma_buf_bytes<T>() + 16; }
+template <typename TIN>
+__host__ __device__ constexpr int dirac_tma_smem() { return 2 * dirac_tma_buf_bytes<TIN>() + 16; }
 
-// wait_limit: polls per mbarrier wait (kTmaSpinLimit); self_test: issue no copies at all, so
-// the first wait runs out with nothing in flight (the bounded-wait self-test)
-template <typename T, bool DAG>
-__global__ void __launch_bounds__(kTT, 2) k_dirac_tma(const cx<T>* __restrict__ U, const cx<T>* __restrict__ in,
+// TIN: the spinors' storage type (T, or float for FP32 spinors into the FP64 operator); COPY:
+// also write the promoted input to in_copy; wait_limit: polls per mbarrier wait
+// (kTmaSpinLimit); self_test: issue no copies at all, so the first wait runs out with nothing
+// in flight (the bounded-wait self-test)
+template <typename T, bool DAG, typename TIN = T, bool COPY = false>
+__global__ void __launch_bounds__(kTT, 2) k_dirac_tma(const cx<T>* __restrict__ U, const cx<TIN>* __restrict__ in,
                                                       cx<T>* __restrict__ out, int nx, int nt, T m0, int nrhs,
-                                                      int wait_limit, int self_test) {
+                                                      int wait_limit, int self_test, cx<T>* __restrict__ in_copy) {
     extern __shared__ __align__(128) unsigned char smraw_d[];
-    constexpr int RS = dirac_tma_row_sites<T>();       // sites per staged row segment
-    constexpr int SB = 2 * (int)sizeof(cx<T>);          // bytes per site (both spins)
-    constexpr int BUF = dirac_tma_buf_bytes<T>();
-    cx<T>* buf0 = reinterpret_cast<cx<T>*>(smraw_d);
+    constexpr int RS = kTT + 2;                         // sites per staged row segment
+    constexpr int SB = 2 * (int)sizeof(cx<TIN>);        // bytes per site (both spins)
+    constexpr int BUF = dirac_tma_buf_bytes<TIN>();
+    cx<TIN>* buf0 = reinterpret_cast<cx<TIN>*>(smraw_d);
     unsigned long long* bars = reinterpret_cast<unsigned long long*>(smraw_d + 2 * BUF);
     const unsigned bar0 = smem_u32(&bars[0]), bar1 = smem_u32(&bars[1]);
     const int N = nx * nt;
@@ -98,13 +99,13 @@ __global__ void __launch_bounds__(kTT, 2) k_dirac_tma(const cx<T>* __restrict__ 
     auto issue = [&](int rhs, int b) {
         const unsigned bar = b ? bar1 : bar0;
         const unsigned dst0 = smem_u32(smraw_d + b * BUF);
-        const cx<T>* src = in + (long long)rhs * N * 2;
+        const cx<TIN>* src = in + (long long)rhs * N * 2;
         if (tid == 0) mbar_arrive_expect_tx(bar, (unsigned)((kTX + 2) * RS * SB));
         __syncwarp();
         if (tid < kTX + 2) {
             const int xr = (x0 - 1 + tid + nx) % nx;
             const unsigned drow = dst0 + (unsigned)(tid * RS * SB);
-            const cx<T>* srow = src + (long long)xr * nt * 2;
+            const cx<TIN>* srow = src + (long long)xr * nt * 2;
             if (interior_t) {
                 bulk_g2s(drow, srow + 2 * (t0 - 1), (unsigned)(RS * SB), bar);
             } else {
@@ -141,15 +142,21 @@ __global__ void __launch_bounds__(kTT, 2) k_dirac_tma(const cx<T>* __restrict__ 
         // one decision for the whole CTA, so no thread leaves the barriers below
         if (__syncthreads_or(!ok)) break;
         done = rhs + 1;
-        const cx<T>* tile = buf0 + (size_t)b * (BUF / sizeof(cx<T>));
+        const cx<TIN>* tile = buf0 + (size_t)b * (BUF / sizeof(cx<TIN>));
         cx<T>* o = out + (long long)rhs * N * 2;
 #pragma unroll
         for (int r = 0; r < kTX; r++) {
+            const int c = (r + 1) * RS + tid + 1;
             cx<T> o0, o1;
-            dirac_site<T, DAG>(L[r], tile, (r + 1) * RS + tid + 1, mass, o0, o1);
+            dirac_site<T, DAG, TIN>(L[r], tile, c, mass, o0, o1);
             const long long n = (long long)(x0 + r) * nt + t0 + tid;
             o[2 * n] = o0;
             o[2 * n + 1] = o1;
+            if constexpr (COPY) {
+                cx<T>* ic = in_copy + (long long)rhs * N * 2;
+                ic[2 * n] = ccast<T>(tile[2 * c]);
+                ic[2 * n + 1] = ccast<T>(tile[2 * c + 1]);
+            }
         }
         __syncthreads();   // every thread is done with buffer b
         if (rhs + 2 < nrhs) {

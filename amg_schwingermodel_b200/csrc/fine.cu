@@ -35,6 +35,26 @@ __global__ void __launch_bounds__(256) k_dirac(const cx<T>* __restrict__ U, cons
     }
 }
 
+// out = D in in FP64 for FP32 spinors in (promoted exactly), with the promoted copy of in
+// written to in_copy: the outer FGMRES's w = D z_j and its FP64 z_j in one pass
+__global__ void __launch_bounds__(256) k_dirac_promote(const double2* __restrict__ U, const float2* __restrict__ in,
+                                                       double2* __restrict__ out, double2* __restrict__ in_copy, int nx,
+                                                       int nt, double m0, int nrhs) {
+    const int N = nx * nt;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    const SiteOp<double> L = site_op<double>(U, n, nx, nt);
+    for (int rhs = blockIdx.y; rhs < nrhs; rhs += gridDim.y) {
+        const long long off = (long long)rhs * N * 2;
+        double2 o0, o1;
+        dirac_site<double, false, float>(L, in + off, n, m0 + 2.0, o0, o1);
+        out[off + 2 * n] = o0;
+        out[off + 2 * n + 1] = o1;
+        in_copy[off + 2 * n] = ccast<double>(in[off + 2 * n]);
+        in_copy[off + 2 * n + 1] = ccast<double>(in[off + 2 * n + 1]);
+    }
+}
+
 // r = b - D x, and per-CTA partial sums of |r|^2 (deterministic second stage); sources
 // grouped per thread as in k_dirac.  Inactive sources (act[rhs] == 0) are skipped.
 template <typename T>
@@ -649,7 +669,8 @@ int dirac_tma_wait_test(const double2* U, const double2* in, double2* out, int n
     if (cudaFuncSetAttribute(k_dirac_tma<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) !=
         cudaSuccess)
         return -1;
-    k_dirac_tma<double, false><<<dim3(nt / kTT, nx / kTX), kTT, bytes, s>>>(U, in, out, nx, nt, -0.1, nrhs, 256, 1);
+    k_dirac_tma<double, false><<<dim3(nt / kTT, nx / kTX), kTT, bytes, s>>>(U, in, out, nx, nt, -0.1, nrhs, 256, 1,
+                                                                             nullptr);
     if (cudaGetLastError() != cudaSuccess) return -1;
     return fine_error_check(s);
 }
@@ -666,16 +687,34 @@ void launch_dirac(const cx<T>* U, const cx<T>* in, cx<T>* out, int nx, int nt, i
         dim3 g(nt / kTT, nx / kTX);
         if (dagger) {
             cudaFuncSetAttribute(k_dirac_tma<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-            k_dirac_tma<T, true><<<g, kTT, bytes, s>>>(U, in, out, nx, nt, m0, nrhs, kTmaSpinLimit, 0);
+            k_dirac_tma<T, true><<<g, kTT, bytes, s>>>(U, in, out, nx, nt, m0, nrhs, kTmaSpinLimit, 0, nullptr);
         } else {
             cudaFuncSetAttribute(k_dirac_tma<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-            k_dirac_tma<T, false><<<g, kTT, bytes, s>>>(U, in, out, nx, nt, m0, nrhs, kTmaSpinLimit, 0);
+            k_dirac_tma<T, false><<<g, kTT, bytes, s>>>(U, in, out, nx, nt, m0, nrhs, kTmaSpinLimit, 0, nullptr);
         }
         return;
     }
     dim3 grid((nx * nt + 255) / 256, source_groups(nx * nt, nrhs));
     if (dagger) k_dirac<T, true><<<grid, 256, 0, s>>>(U, in, out, nx, nt, m0, nrhs);
     else k_dirac<T, false><<<grid, 256, 0, s>>>(U, in, out, nx, nt, m0, nrhs);
+}
+
+// out = D in (FP64) for FP32 spinors in, and in_copy = in promoted to FP64
+void launch_dirac_promote(const double2* U, const float2* in, double2* out, double2* in_copy, int nx, int nt,
+                          int nrhs, double m0, cudaStream_t s) {
+    count_launch(1);
+    if (dirac_tma_enabled() && nrhs >= 1 && nt % kTT == 0 && nx % kTX == 0 && nx >= kTX &&
+        ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out) |
+          reinterpret_cast<uintptr_t>(in_copy)) & 15) == 0) {
+        constexpr int bytes = dirac_tma_smem<float>();
+        cudaFuncSetAttribute(k_dirac_tma<double, false, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             bytes);
+        k_dirac_tma<double, false, float, true><<<dim3(nt / kTT, nx / kTX), kTT, bytes, s>>>(
+            U, in, out, nx, nt, m0, nrhs, kTmaSpinLimit, 0, in_copy);
+        return;
+    }
+    dim3 grid((nx * nt + 255) / 256, source_groups(nx * nt, nrhs));
+    k_dirac_promote<<<grid, 256, 0, s>>>(U, in, out, in_copy, nx, nt, m0, nrhs);
 }
 
 template <typename T>

@@ -15,6 +15,9 @@ inline void count_launch(int n = 1) { __atomic_add_fetch(&g_launches, (long long
 template <typename T>
 void launch_dirac(const cx<T>* U, const cx<T>* in, cx<T>* out, int nx, int nt, int nrhs, T m0, int dagger,
                   cudaStream_t s);
+// out = D in (FP64) for FP32 spinors in (promoted exactly), and in_copy = in promoted to FP64
+void launch_dirac_promote(const double2* U, const float2* in, double2* out, double2* in_copy, int nx, int nt,
+                          int nrhs, double m0, cudaStream_t s);
 // reads and clears the fine kernels' device error flag (bit 0: a bulk-copy wait of the D
 // apply gave up); synchronises the stream; -1 on a CUDA error
 int fine_error_check(cudaStream_t s);

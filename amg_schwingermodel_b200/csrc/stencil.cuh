@@ -40,14 +40,16 @@ __device__ __forceinline__ SiteOp<T> site_op(const cx<T>* __restrict__ U, int n,
     return o;
 }
 
-template <typename T, bool DAG>
-__device__ __forceinline__ void dirac_site(const SiteOp<T>& L, const cx<T>* __restrict__ psi, int n, T mass,
+// psi may be stored in a narrower type TP (FP32 spinors into the FP64 operator): its values
+// are promoted exactly, so the result equals the T-precision operator on the promoted field.
+template <typename T, bool DAG, typename TP = T>
+__device__ __forceinline__ void dirac_site(const SiteOp<T>& L, const cx<TP>* __restrict__ psi, int n, T mass,
                                            cx<T>& o0, cx<T>& o1) {
-    const cx<T> a = psi[2 * L.r0], b = psi[2 * L.r0 + 1];
-    const cx<T> c = psi[2 * L.r1], d = psi[2 * L.r1 + 1];
-    const cx<T> e = psi[2 * L.l0], f = psi[2 * L.l0 + 1];
-    const cx<T> g = psi[2 * L.l1], h = psi[2 * L.l1 + 1];
-    const cx<T> p0 = psi[2 * n], p1 = psi[2 * n + 1];
+    const cx<T> a = ccast<T>(psi[2 * L.r0]), b = ccast<T>(psi[2 * L.r0 + 1]);
+    const cx<T> c = ccast<T>(psi[2 * L.r1]), d = ccast<T>(psi[2 * L.r1 + 1]);
+    const cx<T> e = ccast<T>(psi[2 * L.l0]), f = ccast<T>(psi[2 * L.l0 + 1]);
+    const cx<T> g = ccast<T>(psi[2 * L.l1]), h = ccast<T>(psi[2 * L.l1 + 1]);
+    const cx<T> p0 = ccast<T>(psi[2 * n]), p1 = ccast<T>(psi[2 * n + 1]);
     cx<T> t0, t1, t2, t3;
     if (!DAG) {
         t0 = L.sR * cmul(L.u0, a - b);
