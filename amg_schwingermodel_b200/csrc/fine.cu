@@ -198,62 +198,8 @@ __global__ void __launch_bounds__(256) k_restrict0t(const TW* __restrict__ W, co
 
     // tiles of whole kRtTile-site runs inside one x row (te a multiple of the tile, the usual
     // case) stage with shifts and one base index instead of a division per element
-    const bool rows = (te % kRtTile) == 0;
-    for (int qt = q0; qt < q1; qt += kRtTile) {
-        const int nq = min(kRtTile, q1 - qt);
-        __syncthreads();
-        if (rows && nq == kRtTile) {
-            const int mx = qt / te, mt = qt - mx * te;
-            const long long n0 = (long long)(bxi * xe + mx) * nt + (bti * te + mt);
-            for (int idx = tid; idx < kRtTile * K2; idx += blockDim.x) {
-                const int k = idx / kRtTile, qq = idx % kRtTile;
-                const long long n = n0 + qq;
-                cx<T> w0 = czero<T>(), w1 = czero<T>();
-                if (k < ntest) {
-                    w0 = ccast<T>(load_cx(W + ((long long)k * N + n) * 2));
-                    w1 = ccast<T>(load_cx(W + ((long long)k * N + n) * 2 + 1));
-                }
-                Ws[qq * WR + k] = w0;
-                Ws[qq * WR + K2 + k] = w1;
-            }
-            for (int idx = tid; idx < kRtTile * R2; idx += blockDim.x) {
-                const int r = idx / kRtTile, qq = idx % kRtTile;
-                const long long n = n0 + qq;
-                cx<T> p0 = czero<T>(), p1 = czero<T>();
-                if (r < nrhs) {
-                    p0 = v[(long long)r * N * 2 + 2 * n];
-                    p1 = v[(long long)r * N * 2 + 2 * n + 1];
-                }
-                Vs[qq * VR + r] = p0;
-                Vs[qq * VR + R2 + r] = p1;
-            }
-        } else {
-        for (int idx = tid; idx < nq * K2; idx += blockDim.x) {
-            const int k = idx / nq, qq = idx - k * nq;
-            const int q = qt + qq, mx = q / te, mt = q - mx * te;
-            const long long n = (long long)(bxi * xe + mx) * nt + (bti * te + mt);
-            cx<T> w0 = czero<T>(), w1 = czero<T>();
-            if (k < ntest) {
-                w0 = ccast<T>(load_cx(W + ((long long)k * N + n) * 2));
-                w1 = ccast<T>(load_cx(W + ((long long)k * N + n) * 2 + 1));
-            }
-            Ws[qq * WR + k] = w0;
-            Ws[qq * WR + K2 + k] = w1;
-        }
-        for (int idx = tid; idx < nq * R2; idx += blockDim.x) {
-            const int r = idx / nq, qq = idx - r * nq;
-            const int q = qt + qq, mx = q / te, mt = q - mx * te;
-            const long long n = (long long)(bxi * xe + mx) * nt + (bti * te + mt);
-            cx<T> p0 = czero<T>(), p1 = czero<T>();
-            if (r < nrhs) {
-                p0 = v[(long long)r * N * 2 + 2 * n];
-                p1 = v[(long long)r * N * 2 + 2 * n + 1];
-            }
-            Vs[qq * VR + r] = p0;
-            Vs[qq * VR + R2 + r] = p1;
-        }
-        }
-        __syncthreads();
+    // the tile's products, accumulated over its sites by this thread's site group
+    auto compute = [&](int nq) {
         if (active) {
             for (int qq = grp; qq < nq; qq += G) {
                 const cx<T>* wp = Ws + qq * WR + s * K2 + 2 * kp;
@@ -264,6 +210,94 @@ __global__ void __launch_bounds__(256) k_restrict0t(const TW* __restrict__ W, co
                 cfmac(acc[1][0], wb, va);
                 cfmac(acc[1][1], wb, vb);
             }
+        }
+    };
+    // Tiles of whole kRtTile-site runs inside one x row (te a multiple of the tile, the usual
+    // case) stage with shifts and one base index instead of a division per element, and when a
+    // thread's share of a tile fits in registers (kPW test-vector and kPV source elements) the
+    // next tile's loads are issued before the current tile is computed, so their latency hides
+    // behind the products.
+    constexpr int kPW = 4, kPV = 8;
+    const bool rows = (te % kRtTile) == 0;
+    if (rows && blockDim.x == 256 && K2 * kRtTile <= kPW * 256 && R2 * kRtTile <= kPV * 256) {
+        cx<T> pw[kPW][2], pv[kPV][2];
+        auto fetch = [&](int qt) {
+            const int mx = qt / te, mt = qt - mx * te;
+            const long long n0 = (long long)(bxi * xe + mx) * nt + (bti * te + mt);
+#pragma unroll
+            for (int i = 0; i < kPW; i++) {
+                const int idx = tid + 256 * i, k = idx / kRtTile;
+                const long long n = n0 + idx % kRtTile;
+                pw[i][0] = pw[i][1] = czero<T>();
+                if (k < ntest) {
+                    pw[i][0] = ccast<T>(load_cx(W + ((long long)k * N + n) * 2));
+                    pw[i][1] = ccast<T>(load_cx(W + ((long long)k * N + n) * 2 + 1));
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < kPV; i++) {
+                const int idx = tid + 256 * i, r = idx / kRtTile;
+                const long long n = n0 + idx % kRtTile;
+                pv[i][0] = pv[i][1] = czero<T>();
+                if (r < nrhs) {
+                    pv[i][0] = v[(long long)r * N * 2 + 2 * n];
+                    pv[i][1] = v[(long long)r * N * 2 + 2 * n + 1];
+                }
+            }
+        };
+        if (q0 < q1) fetch(q0);
+        for (int qt = q0; qt < q1; qt += kRtTile) {
+            __syncthreads();   // the previous tile's products are done
+#pragma unroll
+            for (int i = 0; i < kPW; i++) {
+                const int idx = tid + 256 * i, k = idx / kRtTile, qq = idx % kRtTile;
+                if (idx < kRtTile * K2) {
+                    Ws[qq * WR + k] = pw[i][0];
+                    Ws[qq * WR + K2 + k] = pw[i][1];
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < kPV; i++) {
+                const int idx = tid + 256 * i, r = idx / kRtTile, qq = idx % kRtTile;
+                if (idx < kRtTile * R2) {
+                    Vs[qq * VR + r] = pv[i][0];
+                    Vs[qq * VR + R2 + r] = pv[i][1];
+                }
+            }
+            __syncthreads();
+            if (qt + kRtTile < q1) fetch(qt + kRtTile);
+            compute(kRtTile);
+        }
+    } else {
+        for (int qt = q0; qt < q1; qt += kRtTile) {
+            const int nq = min(kRtTile, q1 - qt);
+            __syncthreads();
+            for (int idx = tid; idx < nq * K2; idx += blockDim.x) {
+                const int k = idx / nq, qq = idx - k * nq;
+                const int q = qt + qq, mx = q / te, mt = q - mx * te;
+                const long long n = (long long)(bxi * xe + mx) * nt + (bti * te + mt);
+                cx<T> w0 = czero<T>(), w1 = czero<T>();
+                if (k < ntest) {
+                    w0 = ccast<T>(load_cx(W + ((long long)k * N + n) * 2));
+                    w1 = ccast<T>(load_cx(W + ((long long)k * N + n) * 2 + 1));
+                }
+                Ws[qq * WR + k] = w0;
+                Ws[qq * WR + K2 + k] = w1;
+            }
+            for (int idx = tid; idx < nq * R2; idx += blockDim.x) {
+                const int r = idx / nq, qq = idx - r * nq;
+                const int q = qt + qq, mx = q / te, mt = q - mx * te;
+                const long long n = (long long)(bxi * xe + mx) * nt + (bti * te + mt);
+                cx<T> p0 = czero<T>(), p1 = czero<T>();
+                if (r < nrhs) {
+                    p0 = v[(long long)r * N * 2 + 2 * n];
+                    p1 = v[(long long)r * N * 2 + 2 * n + 1];
+                }
+                Vs[qq * VR + r] = p0;
+                Vs[qq * VR + R2 + r] = p1;
+            }
+            __syncthreads();
+            compute(nq);
         }
     }
     // sum the site groups and write this split's partials
