@@ -69,13 +69,14 @@ template <typename TIN>
 __host__ __device__ constexpr int dirac_tma_smem() { return 2 * dirac_tma_buf_bytes<TIN>() + 16; }
 
 // TIN: the spinors' storage type (T, or float for FP32 spinors into the FP64 operator); COPY:
-// also write the promoted input to in_copy; wait_limit: polls per mbarrier wait
-// (kTmaSpinLimit); self_test: issue no copies at all, so the first wait runs out with nothing
-// in flight (the bounded-wait self-test)
-template <typename T, bool DAG, typename TIN = T, bool COPY = false>
+// also write the promoted input to in_copy; SELF_TEST: issue no copies at all and poll 256
+// times per wait, so the first wait runs out with nothing in flight (the bounded-wait
+// self-test)
+template <typename T, bool DAG, typename TIN = T, bool COPY = false, bool SELF_TEST = false>
 __global__ void __launch_bounds__(kTT, 2) k_dirac_tma(const cx<T>* __restrict__ U, const cx<TIN>* __restrict__ in,
                                                       cx<T>* __restrict__ out, int nx, int nt, T m0, int nrhs,
-                                                      int wait_limit, int self_test, cx<T>* __restrict__ in_copy) {
+                                                      cx<T>* __restrict__ in_copy) {
+    constexpr int wait_limit = SELF_TEST ? 256 : kTmaSpinLimit;
     extern __shared__ __align__(128) unsigned char smraw_d[];
     constexpr int RS = kTT + 2;                         // sites per staged row segment
     constexpr int SB = 2 * (int)sizeof(cx<TIN>);        // bytes per site (both spins)
@@ -129,11 +130,11 @@ __global__ void __launch_bounds__(kTT, 2) k_dirac_tma(const cx<T>* __restrict__ 
         L[r].r1 = c + RS;
         L[r].l1 = c - RS;
     }
-    if (tid < 32 && !self_test) {
+    if (tid < 32 && !SELF_TEST) {
         issue(0, 0);
         if (nrhs > 1) issue(1, 1);
     }
-    int issued = self_test ? 0 : (nrhs > 1 ? 2 : 1);   // sources whose copies have been issued
+    int issued = SELF_TEST ? 0 : (nrhs > 1 ? 2 : 1);   // sources whose copies have been issued
     const T mass = m0 + T(2);
     int done = 0;                      // sources whose copies every thread has seen land
     for (int rhs = 0; rhs < nrhs; rhs++) {

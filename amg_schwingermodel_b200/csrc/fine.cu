@@ -700,11 +700,11 @@ int dirac_tma_wait_test(const double2* U, const double2* in, double2* out, int n
         ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15) != 0)
         return -1;
     constexpr int bytes = dirac_tma_smem<double>();
-    if (cudaFuncSetAttribute(k_dirac_tma<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) !=
-        cudaSuccess)
+    if (cudaFuncSetAttribute(k_dirac_tma<double, false, double, false, true>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess)
         return -1;
-    k_dirac_tma<double, false><<<dim3(nt / kTT, nx / kTX), kTT, bytes, s>>>(U, in, out, nx, nt, -0.1, nrhs, 256, 1,
-                                                                             nullptr);
+    k_dirac_tma<double, false, double, false, true><<<dim3(nt / kTT, nx / kTX), kTT, bytes, s>>>(U, in, out, nx, nt,
+                                                                                                 -0.1, nrhs, nullptr);
     if (cudaGetLastError() != cudaSuccess) return -1;
     return fine_error_check(s);
 }
@@ -721,10 +721,10 @@ void launch_dirac(const cx<T>* U, const cx<T>* in, cx<T>* out, int nx, int nt, i
         dim3 g(nt / kTT, nx / kTX);
         if (dagger) {
             cudaFuncSetAttribute(k_dirac_tma<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-            k_dirac_tma<T, true><<<g, kTT, bytes, s>>>(U, in, out, nx, nt, m0, nrhs, kTmaSpinLimit, 0, nullptr);
+            k_dirac_tma<T, true><<<g, kTT, bytes, s>>>(U, in, out, nx, nt, m0, nrhs, nullptr);
         } else {
             cudaFuncSetAttribute(k_dirac_tma<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-            k_dirac_tma<T, false><<<g, kTT, bytes, s>>>(U, in, out, nx, nt, m0, nrhs, kTmaSpinLimit, 0, nullptr);
+            k_dirac_tma<T, false><<<g, kTT, bytes, s>>>(U, in, out, nx, nt, m0, nrhs, nullptr);
         }
         return;
     }
@@ -744,7 +744,7 @@ void launch_dirac_promote(const double2* U, const float2* in, double2* out, doub
         cudaFuncSetAttribute(k_dirac_tma<double, false, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              bytes);
         k_dirac_tma<double, false, float, true><<<dim3(nt / kTT, nx / kTX), kTT, bytes, s>>>(
-            U, in, out, nx, nt, m0, nrhs, kTmaSpinLimit, 0, in_copy);
+            U, in, out, nx, nt, m0, nrhs, in_copy);
         return;
     }
     dim3 grid((nx * nt + 255) / 256, source_groups(nx * nt, nrhs));

@@ -3,6 +3,8 @@
 //
 // Layout: psi[n][spin] complex (double2 or float2), n = x*Nt + t; U[n][mu].
 #pragma once
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace amgb {
@@ -42,14 +44,19 @@ __device__ __forceinline__ SiteOp<T> site_op(const cx<T>* __restrict__ U, int n,
 
 // psi may be stored in a narrower type TP (FP32 spinors into the FP64 operator): its values
 // are promoted exactly, so the result equals the T-precision operator on the promoted field.
+template <typename T, typename TP>
+__device__ __forceinline__ cx<T> promote_cx(const cx<TP>& v) {
+    if constexpr (std::is_same<T, TP>::value) return v;
+    else return ccast<T>(v);
+}
 template <typename T, bool DAG, typename TP = T>
 __device__ __forceinline__ void dirac_site(const SiteOp<T>& L, const cx<TP>* __restrict__ psi, int n, T mass,
                                            cx<T>& o0, cx<T>& o1) {
-    const cx<T> a = ccast<T>(psi[2 * L.r0]), b = ccast<T>(psi[2 * L.r0 + 1]);
-    const cx<T> c = ccast<T>(psi[2 * L.r1]), d = ccast<T>(psi[2 * L.r1 + 1]);
-    const cx<T> e = ccast<T>(psi[2 * L.l0]), f = ccast<T>(psi[2 * L.l0 + 1]);
-    const cx<T> g = ccast<T>(psi[2 * L.l1]), h = ccast<T>(psi[2 * L.l1 + 1]);
-    const cx<T> p0 = ccast<T>(psi[2 * n]), p1 = ccast<T>(psi[2 * n + 1]);
+    const cx<T> a = promote_cx<T, TP>(psi[2 * L.r0]), b = promote_cx<T, TP>(psi[2 * L.r0 + 1]);
+    const cx<T> c = promote_cx<T, TP>(psi[2 * L.r1]), d = promote_cx<T, TP>(psi[2 * L.r1 + 1]);
+    const cx<T> e = promote_cx<T, TP>(psi[2 * L.l0]), f = promote_cx<T, TP>(psi[2 * L.l0 + 1]);
+    const cx<T> g = promote_cx<T, TP>(psi[2 * L.l1]), h = promote_cx<T, TP>(psi[2 * L.l1 + 1]);
+    const cx<T> p0 = promote_cx<T, TP>(psi[2 * n]), p1 = promote_cx<T, TP>(psi[2 * n + 1]);
     cx<T> t0, t1, t2, t3;
     if (!DAG) {
         t0 = L.sR * cmul(L.u0, a - b);
