@@ -10,8 +10,10 @@ One step = one batched solve of R seeded complex-Gaussian sources on one seeded 
 field per GPU (inputs resident in HBM; the working set of a step is far above the 126 MB
 L2).  With N GPUs every rank solves its own gauge field and sources (replicas, weak
 scaling); timing is CUDA events on the solver's stream, max over ranks.  Rank 0 prints one
-JSON line.  `--impl reference` times the reference's own CPU code on the same workload
-(a bounded sample).
+JSON line.  `--impl reference` times the reference's own CPU code (compiled from its
+sources into oracle/_ref) on the same workload: the reference's set-up with its test-vector
+smoothing skipped, then a bounded sample of outer FGMRES iterations (one K-cycle from the
+fine level plus D_phi each) scaled to the workload's iteration count.
 """
 from __future__ import annotations
 
