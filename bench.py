@@ -35,9 +35,8 @@ sys.path.insert(0, str(ROOT))
 NX = NT = 1024
 ROWS = [[0, 8, 8, 16, 32, 32], [1, 4, 4, 16, 4, 4], [2, 2, 2, 16, 2, 2]]
 # DRAM bytes (read + write) of one fine SAP launch per (block, source) it solves, from an ncu
-# capture of this workload at 2 sources (profiles/k_sap0_f32_1024x1024_r2.md: 42.02 MB read
-# + 0.37 MB written for 512 blocks x 2 sources); the traffic grows with the blocks x sources
-# a launch solves.
+# capture of this workload at 2 sources (42.02 MB read + 0.37 MB written for 512 blocks x 2
+# sources); the traffic grows with the blocks x sources a launch solves.
 SAP_DRAM_BYTES_PER_BLOCK_SOURCE = 42.391808e6 / 1024
 BETA, M0, TOL = 4.0, -0.05, 1e-10
 METRIC = "1024^2 solves/s at FP64 resid <=1e-10: mixed+batched vs FP64 GPU; D-apply GB/s"
