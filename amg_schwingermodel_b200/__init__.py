@@ -133,6 +133,11 @@ class AMGContext:
         self.m0 = float(m0)
         check(lib().amg_set_mass(self._h, self.m0), "amg_set_mass")
 
+    def set_preconditioner(self, kind: int) -> None:
+        """amg_set_preconditioner: _lib.AMG_PRECOND_MG (FGMRES_AMG, default) or
+        _lib.AMG_PRECOND_SAP (the reference's FGMRES_SAP, include/sap.h:194-225)."""
+        check(lib().amg_set_preconditioner(self._h, int(kind)), "amg_set_preconditioner")
+
     def dirac(self, psi, dagger: bool = False) -> np.ndarray:
         """D_phi / D_dagger_phi on [N][2] or [nrhs][N][2]."""
         psi = _c128(psi)

@@ -23,6 +23,8 @@ AMG_PREC_F64 = 0
 AMG_PREC_MIXED = 1
 AMG_CYCLE_V = 0
 AMG_CYCLE_K = 1
+AMG_PRECOND_MG = 0
+AMG_PRECOND_SAP = 1
 
 
 class AmgParams(C.Structure):
@@ -71,6 +73,7 @@ SIGNATURES = {
     "amg_restrict_raw_noalloc": (_I, [_P, _P, _P, _I, _I, _I, _I, _I, _I, _P]),
     "amg_dirac_apply_host": (_I, [_P, _P, _P, _I, _I, _I, _D, _I]),
     "amg_set_cycle": (_I, [_P, _I]),
+    "amg_set_preconditioner": (_I, [_P, _I]),
     "amg_set_initial_test_vectors": (_I, [_P, _I, _P]),
     "amg_setup": (_I, [_P]),
     "amg_get_test_vectors": (_I, [_P, _I, _P]),

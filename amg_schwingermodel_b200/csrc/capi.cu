@@ -225,6 +225,7 @@ struct amg_context {
     int graphs_off = 0;            // capture failed once: run eagerly from then on
     // autotuner state: the fine SAP kernel variant (-1: default) and whether it ran
     int sap_variant = -1, tuned = 0;
+    int precond = AMG_PRECOND_MG;   // amg_set_preconditioner
     // the FP64 vector whose FP32 copy the mixed preconditioner's input buffer vf holds (the
     // outer FGMRES writes that copy while it normalises the basis vector), or null
     const void* vf_src = nullptr;
@@ -708,6 +709,7 @@ int precondition(amg_context* c, const double2* v, double2* z, int R, bool want_
         CK(cudaMemcpyAsync(vs, v, (size_t)R * len * sizeof(double2), cudaMemcpyDeviceToDevice, c->stream));
         CKR(run_graph(c, std::make_tuple(0, R, (const void*)vs, (void*)zs), [&]() -> int {
             CK(cudaMemsetAsync(zs, 0, (size_t)R * len * sizeof(double2), c->stream));
+            if (c->precond == AMG_PRECOND_SAP) return fine_sap<double>(c, c->d, vs, len, zs, 1, R, 0);
             return fine_cycle<double>(c, c->d, vs, zs, R, true);
         }));
         CK(cudaMemcpyAsync(z, zs, (size_t)R * len * sizeof(double2), cudaMemcpyDeviceToDevice, c->stream));
@@ -721,6 +723,7 @@ int precondition(amg_context* c, const double2* v, double2* z, int R, bool want_
     }
     CKR(run_graph(c, std::make_tuple(1, R, (const void*)vf, (void*)zf), [&]() -> int {
         CK(cudaMemsetAsync(zf, 0, (size_t)R * len * sizeof(float2), c->stream));
+        if (c->precond == AMG_PRECOND_SAP) return fine_sap<float>(c, c->f, vf, len, zf, 1, R, 0);
         return fine_cycle<float>(c, c->f, vf, zf, R, true);
     }));
     if (want_z) launch_f2d(z, zf, R * len, c->stream);
@@ -1468,6 +1471,15 @@ int amg_set_cycle(amg_ctx c, int cycle) {
     if (!c) return fail(AMG_ERR_INVALID, "null context");
     if (cycle != AMG_CYCLE_K && cycle != AMG_CYCLE_V) return fail(AMG_ERR_INVALID, "cycle must be AMG_CYCLE_K or AMG_CYCLE_V");
     c->p.cycle = cycle;
+    c->drop_graphs();
+    return AMG_OK;
+}
+
+int amg_set_preconditioner(amg_ctx c, int kind) {
+    if (!c) return fail(AMG_ERR_INVALID, "null context");
+    if (kind != AMG_PRECOND_MG && kind != AMG_PRECOND_SAP)
+        return fail(AMG_ERR_INVALID, "preconditioner must be AMG_PRECOND_MG or AMG_PRECOND_SAP");
+    c->precond = kind;
     c->drop_graphs();
     return AMG_OK;
 }

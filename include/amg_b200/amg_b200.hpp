@@ -54,6 +54,9 @@ inline int sap_gmres_restarts = 5;
 inline double sap_gmres_tolerance = 1e-3;
 inline double sap_tolerance = 1e-10;
 inline int sap_blocks_per_proc = 1;  // accepted and ignored: every block is solved on the GPU
+// blocks per direction of the fine SAP that FGMRES_SAP uses (include/variables.h:35-36)
+constexpr int sap_block_x = 4;
+constexpr int sap_block_t = 4;
 }  // namespace SAPV
 
 namespace AMGV {
@@ -410,6 +413,35 @@ private:
     }
 };
 
+namespace amg_b200 {
+// FGMRES::fgmres (include/fgmres.h:36) on a context's solver: x for D x = phi from x0;
+// returns the iteration count k*m + j, or restarts*m if the tolerance was not met
+inline int fgmres_on(amg_ctx ctx, const spinor& phi, const spinor& x0, spinor& x, bool print_message, int* status) {
+    std::vector<c_double> b = flatten(phi), x0f = flatten(x0), xf(b.size());
+    bool zero = true;
+    for (const auto& v : x0f) zero = zero && v == c_double(0);
+    if (!zero) {  // solve for the correction to x0: D e = b - D x0
+        std::vector<c_double> dx(b.size());
+        check(amg_dirac_apply(ctx, dptr(x0f), dptr(dx), 1, 0), "fgmres");
+        for (size_t i = 0; i < b.size(); i++) b[i] -= dx[i];
+    }
+    amg_solve_info info{};
+    const int st = check(amg_solve(ctx, dptr(b), dptr(xf), 1, &info), "fgmres");
+    if (!zero)
+        for (size_t i = 0; i < xf.size(); i++) xf[i] += x0f[i];
+    unflatten(xf, x);
+    if (print_message) {
+        if (st == AMG_OK)
+            std::cout << "FGMRES converged with " << info.iterations << " iterations, relative residual "
+                      << info.rel_residual << std::endl;
+        else
+            std::cout << "FGMRES did not converge, relative residual " << info.rel_residual << std::endl;
+    }
+    if (status) *status = st;
+    return info.iterations;
+}
+}  // namespace amg_b200
+
 // ---- FGMRES_AMG (include/amg.h:99-145) -------------------------------------------------
 // FGMRES(m, restarts, tol) with D_phi and one AMG cycle (AMGV::cycle) as preconditioner;
 // the constructor runs the set-up with AMGV::Nit, as the reference's does.
@@ -436,28 +468,10 @@ public:
     // restarts*m if the tolerance was not met
     int fgmres(const spinor& phi, const spinor& x0, spinor& x, const bool& print_message = false,
                const bool save_res = false) {
-        std::vector<c_double> b = amg_b200::flatten(phi), x0f = amg_b200::flatten(x0), xf(b.size());
-        bool zero = true;
-        for (const auto& v : x0f) zero = zero && v == c_double(0);
-        if (!zero) {  // solve for the correction to x0: D e = b - D x0
-            std::vector<c_double> dx(b.size());
-            amg_b200::check(amg_dirac_apply(ctx_->get(), amg_b200::dptr(x0f), amg_b200::dptr(dx), 1, 0), "fgmres");
-            for (size_t i = 0; i < b.size(); i++) b[i] -= dx[i];
-        }
-        amg_solve_info info{};
-        const int st = amg_b200::check(amg_solve(ctx_->get(), amg_b200::dptr(b), amg_b200::dptr(xf), 1, &info), "fgmres");
-        if (!zero)
-            for (size_t i = 0; i < xf.size(); i++) xf[i] += x0f[i];
-        amg_b200::unflatten(xf, x);
-        if (print_message) {
-            if (st == AMG_OK)
-                std::cout << "FGMRES converged with " << info.iterations << " iterations, relative residual "
-                          << info.rel_residual << std::endl;
-            else
-                std::cout << "FGMRES did not converge, relative residual " << info.rel_residual << std::endl;
-        }
+        int st = AMG_OK;
+        const int it = amg_b200::fgmres_on(ctx_->get(), phi, x0, x, print_message, &st);
         if (save_res && st == AMG_OK) save_residuals();
-        return info.iterations;
+        return it;
     }
     amg_ctx ctx() const { return ctx_->get(); }
 
@@ -479,6 +493,47 @@ private:
         std::ofstream f(name.str());
         for (int i = 0; i < n; i++) f << i << std::setw(30) << std::setprecision(17) << std::scientific << h[i] << "\n";
     }
+};
+
+// ---- FGMRES_SAP (include/sap.h:194-225) -------------------------------------------------
+// FGMRES(m, restarts, tol) with D_phi and one fine-level SAP sweep (nu = 1, z zeroed first)
+// as the preconditioner, on SAPV::sap_block_x x SAPV::sap_block_t SAP blocks as the
+// reference's global fine-level SAP object uses them.  The context still runs its set-up,
+// which owns the SAP work buffers.
+class FGMRES_SAP {
+public:
+    FGMRES_SAP(const int& dim1, const int& dim2, const int& m, const int& restarts, const double& tol,
+               const c_matrix& U, const double& m0, int precision = AMG_PREC_F64)
+        : dim1(dim1), dim2(dim2), m0(m0) {
+        const int sm = FGMRESV::fgmres_restart_length, sr = FGMRESV::fgmres_restarts;
+        const double st = FGMRESV::fgmres_tolerance;
+        const int sbx = LevelV::SAP_Block_x[0], sbt = LevelV::SAP_Block_t[0];
+        FGMRESV::fgmres_restart_length = m;
+        FGMRESV::fgmres_restarts = restarts;
+        FGMRESV::fgmres_tolerance = tol;
+        LevelV::SAP_Block_x[0] = SAPV::sap_block_x;
+        LevelV::SAP_Block_t[0] = SAPV::sap_block_t;
+        ctx_ = std::make_unique<amg_b200::Context>(U, m0, 0, precision);
+        FGMRESV::fgmres_restart_length = sm;
+        FGMRESV::fgmres_restarts = sr;
+        FGMRESV::fgmres_tolerance = st;
+        LevelV::SAP_Block_x[0] = sbx;
+        LevelV::SAP_Block_t[0] = sbt;
+        amg_b200::check(amg_setup(ctx_->get()), "FGMRES_SAP");
+        amg_b200::check(amg_set_preconditioner(ctx_->get(), AMG_PRECOND_SAP), "FGMRES_SAP");
+    }
+    // FGMRES::fgmres (include/fgmres.h:36)
+    int fgmres(const spinor& phi, const spinor& x0, spinor& x, const bool& print_message = false,
+               const bool save_res = false) {
+        (void)save_res;
+        return amg_b200::fgmres_on(ctx_->get(), phi, x0, x, print_message, nullptr);
+    }
+    amg_ctx ctx() const { return ctx_->get(); }
+
+private:
+    int dim1, dim2;
+    double m0;
+    std::unique_ptr<amg_b200::Context> ctx_;
 };
 
 #endif

@@ -47,6 +47,10 @@ extern "C" {
 #define AMG_CYCLE_V 0            /* AMGV::cycle = 0 (include/variables.h:64) */
 #define AMG_CYCLE_K 1
 
+/* preconditioner of the outer FGMRES (amg_set_preconditioner) */
+#define AMG_PRECOND_MG 0         /* FGMRES_AMG: the K- or V-cycle (include/amg.h:99-145) */
+#define AMG_PRECOND_SAP 1        /* FGMRES_SAP: one fine-level SAP sweep (include/sap.h:194-225) */
+
 typedef struct amg_context* amg_ctx;
 
 /* Solver knobs.  Defaults (amg_params_default) are the reference's:
@@ -110,6 +114,13 @@ AMG_API int amg_set_mass(amg_ctx ctx, double m0);
 /* Replaces assigning AMGV::cycle (include/variables.h:64) after creation: AMG_CYCLE_K or
  * AMG_CYCLE_V for the amg_cycle, amg_solve and bootstrap calls that follow. */
 AMG_API int amg_set_cycle(amg_ctx ctx, int cycle);
+/* Chooses the outer FGMRES's preconditioner for the amg_solve* calls that follow:
+ * AMG_PRECOND_MG (default, FGMRES_AMG) or AMG_PRECOND_SAP, the reference's comparison solver
+ * FGMRES_SAP (include/sap.h:194-225, run by Tests::FGMRES_sap, src/tests.cpp:33-46): each
+ * preconditioner call zeroes z and applies SAP_C::SAP(v, z, nu = 1) on the fine level, with
+ * the fine SAP kernels of the context's precision.  The solve still needs amg_setup (the SAP
+ * work buffers live with the hierarchy). */
+AMG_API int amg_set_preconditioner(amg_ctx ctx, int kind);
 /* Level sizes as LevelV fills them: out[l] = {Nsites, NxSites, NtSites, DOF, Colors, Ntest}. */
 AMG_API int amg_level_info(amg_ctx ctx, int level, int* out6);
 

@@ -695,6 +695,16 @@ class AMG:
                       p.outer_tol, history)
 
 
+    def solve_sap(self, b: np.ndarray, history: list | None = None):
+        """FGMRES_SAP::fgmres(b, x0 = 0, x) (include/sap.h:194-225, run by Tests::FGMRES_sap,
+        src/tests.cpp:33-46): func = D_phi; the preconditioner zeroes z and applies
+        SAP_C::SAP(v, z, nu = 1) on the fine level."""
+        p = self.p
+        func = lambda z: d_phi(self.U, z, p.m0, self.ns, self.nt)
+        precond = lambda v, z: self.sap(0, v, np.zeros_like(v), 1)[0]
+        return fgmres(func, precond, b, np.zeros_like(b), p.outer_m, p.outer_restarts, p.outer_tol, history)
+
+
 def true_residual(U, x, b, m0, nx, nt) -> float:
     r = b - d_phi(U, x, m0, nx, nt)
     return float(np.linalg.norm(r) / np.linalg.norm(b))

@@ -57,6 +57,14 @@ int main(int argc, char** argv) {
         dump(wd + "/x.bin", x);
         res << "iterations " << it << "\n";
 
+        // Tests::FGMRES_sap (src/tests.cpp:33-46): FGMRES with one SAP sweep as preconditioner
+        spinor xsap(LevelV::Nsites[0], c_vector(LevelV::DOF[0], 0));
+        FGMRES_SAP sap_solver(LV::Ntot, 2, FGMRESV::fgmres_restart_length, FGMRESV::fgmres_restarts,
+                              FGMRESV::fgmres_tolerance, GConf.Conf, m0);
+        const int its = sap_solver.fgmres(rhs, x0, xsap, false, false);
+        dump(wd + "/x_sap.bin", xsap);
+        res << "sap_solver_iterations " << its << "\n";
+
         spinor d(LevelV::Nsites[0], c_vector(2, 0));
         D_phi(GConf.Conf, rhs, d, m0);
         dump(wd + "/dphi.bin", d);

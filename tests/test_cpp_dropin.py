@@ -2,12 +2,14 @@
 (tests/cpp/dropin_main.cpp) written against the reference's class and function names --
 readParameters, GaugeConf::read_conf, read_rhs, FGMRES_AMG::fgmres, D_phi, D_dagger_phi,
 AlgebraicMG::setUpPhase / k_cycle / applyMultilevel, Level::D_operator / Pt_v / P_v,
-SAP_level_l::SAP, GMRES_level_l::fgmres -- built with g++ against libschwinger_amg.so.
+SAP_level_l::SAP, GMRES_level_l::fgmres, FGMRES_SAP::fgmres -- built with g++ against
+libschwinger_amg.so.
 
 CPU: the driver compiles and links for two lattice configurations.
 GPU: it reproduces the golden fixtures (outputs of the reference itself on the same
 inputs, passed in the reference's text formats): iteration count equal, x within 1e-8,
-D and D^dagger within 1e-13, level operations within 1e-8.
+D and D^dagger within 1e-13, level operations within 1e-8; FGMRES_SAP within one iteration
+and 1e-8 of the restatement.
 """
 import subprocess
 from pathlib import Path
@@ -16,6 +18,7 @@ import numpy as np
 import pytest
 
 from conftest import load_golden, rel
+from oracle import restatement as R
 
 ROOT = Path(__file__).resolve().parents[1]
 PKG = ROOT / "amg_schwingermodel_b200"
@@ -75,6 +78,13 @@ def test_driver_reproduces_reference(name, tmp_path):
 
     assert int(res["iterations"]) == m["iterations"]
     assert rel(out("x", g["x"]), g["x"]) < 1e-8
+    # FGMRES_SAP (include/sap.h:194-225) on the reference's 4 x 4 SAP blocks, against the
+    # restatement (the reference's own main never runs it): within one outer iteration
+    rows4 = [list(r) for r in m["rows"]]
+    rows4[0][4] = rows4[0][5] = 4
+    x_ref, it_ref = R.AMG(g["gauge"], m["ns"], m["nt"], rows4, R.SolverParams(m0=m["m0"])).solve_sap(g["rhs"])
+    assert abs(int(res["sap_solver_iterations"]) - it_ref) <= 1, (res["sap_solver_iterations"], it_ref)
+    assert rel(out("x_sap", x_ref), x_ref) < 1e-8
     assert rel(out("dphi", g["dphi"]), g["dphi"]) < 1e-13
     assert rel(out("ddagphi", g["ddagphi"]), g["ddagphi"]) < 1e-13
     assert rel(out("dop_l0", g["dop_l0"]), g["dop_l0"]) < 1e-13
