@@ -133,6 +133,28 @@ class AMGContext:
         self.m0 = float(m0)
         check(lib().amg_set_mass(self._h, self.m0), "amg_set_mass")
 
+    def cg_normal(self, phi, max_iter: int = 100000, tol: float = 1e-10):
+        """conjugate_gradient (src/conjugate_gradient.cpp:5-65): x = (D D^dagger)^{-1} phi.
+        Returns (x, iterations, converged)."""
+        phi = _c128(phi, (self.nx * self.nt, 2))
+        x = np.empty_like(phi)
+        it = C.c_int(0)
+        st = check(lib().amg_cg_normal(self._h, _cptr(phi), _cptr(x), int(max_iter), float(tol), C.byref(it)),
+                   "amg_cg_normal")
+        return x, it.value, st == _lib.AMG_OK
+
+    def bicgstab(self, phi, x0=None, max_iter: int = 100000, tol: float = 1e-10):
+        """bi_cgstab (src/bi_cgstab.cpp:5-89): D x = phi from x0 (zero when None).
+        Returns (x, iterations, converged)."""
+        phi = _c128(phi, (self.nx * self.nt, 2))
+        x = np.empty_like(phi)
+        it = C.c_int(0)
+        x0a = None if x0 is None else _c128(x0, (self.nx * self.nt, 2))
+        x0p = None if x0a is None else _cptr(x0a)
+        st = check(lib().amg_bicgstab(self._h, _cptr(phi), x0p, _cptr(x), int(max_iter), float(tol), C.byref(it)),
+                   "amg_bicgstab")
+        return x, it.value, st == _lib.AMG_OK
+
     def set_preconditioner(self, kind: int) -> None:
         """amg_set_preconditioner: _lib.AMG_PRECOND_MG (FGMRES_AMG, default) or
         _lib.AMG_PRECOND_SAP (the reference's FGMRES_SAP, include/sap.h:194-225)."""

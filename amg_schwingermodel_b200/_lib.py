@@ -70,6 +70,8 @@ SIGNATURES = {
     "amg_dirac_apply_dev": (_I, [_P, _P, _P, _I, _I]),
     "amg_dirac_apply_raw": (_I, [_P, _P, _P, _I, _I, _I, _D, _I, _P]),
     "amg_debug_dirac_wait_test": (_I, [_P, _P, _P, _I, _I, _I]),
+    "amg_cg_normal": (_I, [_P, _P, _P, _I, _D, _P]),
+    "amg_bicgstab": (_I, [_P, _P, _P, _P, _I, _D, _P]),
     "amg_restrict_raw_noalloc": (_I, [_P, _P, _P, _I, _I, _I, _I, _I, _I, _P]),
     "amg_dirac_apply_host": (_I, [_P, _P, _P, _I, _I, _I, _D, _I]),
     "amg_set_cycle": (_I, [_P, _I]),

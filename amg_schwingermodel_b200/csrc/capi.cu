@@ -1514,6 +1514,189 @@ int amg_dirac_apply_dev(amg_ctx c, const void* in, void* out, int nrhs, int dagg
     return check_fine_waits(c->stream);
 }
 
+// ---------------------------------------------------------------------------------
+// Comparison solvers on the fine stencil (FP64, one source): conjugate_gradient
+// (src/conjugate_gradient.cpp:5-65) on D D^dagger and bi_cgstab (src/bi_cgstab.cpp:5-89),
+// each a host loop over device kernels; every vector update evaluates the reference's
+// expression in its order, and every dot is the reference's dot(x, y) = sum x conj(y).
+// ---------------------------------------------------------------------------------
+namespace {
+// y += a x
+__global__ void k_cs_xpay(double2* __restrict__ y, const double2* __restrict__ x, double2 a, long long n) {
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+        y[e] = y[e] + cmul(a, x[e]);
+}
+// y = r - a q
+__global__ void k_cs_rmaq(double2* __restrict__ y, const double2* __restrict__ r, const double2* __restrict__ q,
+                          double2 a, long long n) {
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+        y[e] = r[e] - cmul(a, q[e]);
+}
+// d = d beta + r (CG)
+__global__ void k_cs_dbr(double2* __restrict__ d, const double2* __restrict__ r, double2 beta, long long n) {
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+        d[e] = cmul(d[e], beta) + r[e];
+}
+// d = r + beta (d - omega Ad) (BiCGStab)
+__global__ void k_cs_bicg_d(double2* __restrict__ d, const double2* __restrict__ r, const double2* __restrict__ Ad,
+                            double2 beta, double2 omega, long long n) {
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+        d[e] = r[e] + cmul(beta, d[e] - cmul(omega, Ad[e]));
+}
+// x = x + alpha d + omega s (BiCGStab)
+__global__ void k_cs_x3(double2* __restrict__ x, const double2* __restrict__ d, const double2* __restrict__ s,
+                        double2 alpha, double2 omega, long long n) {
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+        x[e] = x[e] + cmul(alpha, d[e]) + cmul(omega, s[e]);
+}
+
+struct FineKrylov {
+    amg_context* c;
+    long long n;          // complex entries of one fine vector
+    int np;
+    DevBuf part, out;
+    std::complex<double> hdot[2];
+    int init(amg_context* c_) {
+        c = c_;
+        n = vlen0(c);
+        np = (int)std::min<long long>(592, (n + 255) / 256);
+        CKR(part.alloc((size_t)np * 2 * sizeof(double2)));
+        CKR(out.alloc(2 * sizeof(double2)));
+        return AMG_OK;
+    }
+    dim3 grid() const { return dim3((unsigned)std::min<long long>(592, (n + 255) / 256)); }
+    // dot(a, b) = sum a conj(b) (include/lin_alg_op.h:32-40)
+    int dot(const double2* a, const double2* b, std::complex<double>& r) {
+        launch_axpy_multidot(const_cast<double2*>(a), b, n, n, 0, nullptr, 0, 1, nullptr, 1, part.as<double2>(), np,
+                             out.as<double2>(), c->stream);
+        CK(cudaMemcpyAsync(hdot, out.p, 2 * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        r = hdot[0];
+        return AMG_OK;
+    }
+    void dirac(const double2* in, double2* o, int dagger) {
+        launch_dirac<double>(c->d.U.as<double2>(), in, o, c->nx, c->nt, 1, c->m0, dagger, c->stream);
+    }
+};
+inline double2 d2(std::complex<double> z) { return make_double2(z.real(), z.imag()); }
+}  // namespace
+
+int amg_cg_normal(amg_ctx c, const double* phi, double* x, int max_iter, double tol, int* iterations) {
+    CKR(check_ready(c, 0, false));
+    if (!phi || !x || max_iter < 0 || !(tol > 0)) return fail(AMG_ERR_INVALID, "bad argument");
+    CKR(select_device(c));
+    FineKrylov K;
+    CKR(K.init(c));
+    const long long n = K.n;
+    DevBuf P, X, R, D, AD, T;
+    CKR(to_dev(P, phi, n, c->stream));
+    CKR(to_dev(X, phi, n, c->stream));   // x = phi
+    CKR(to_dev(R, nullptr, n, c->stream));
+    CKR(to_dev(D, nullptr, n, c->stream));
+    CKR(to_dev(AD, nullptr, n, c->stream));
+    CKR(to_dev(T, nullptr, n, c->stream));
+    double2 *p = P.as<double2>(), *xv = X.as<double2>(), *r = R.as<double2>(), *d = D.as<double2>(),
+            *ad = AD.as<double2>(), *t = T.as<double2>();
+    const dim3 g = K.grid();
+    auto ddag = [&](const double2* in, double2* o) {   // D_D_dagger_phi (src/dirac_operator.cpp:57-61)
+        K.dirac(in, t, 1);
+        K.dirac(t, o, 0);
+    };
+    ddag(xv, ad);
+    k_cs_rmaq<<<g, 256, 0, c->stream>>>(r, p, ad, make_double2(1.0, 0.0), n);
+    CK(cudaMemcpyAsync(d, r, (size_t)n * sizeof(double2), cudaMemcpyDeviceToDevice, c->stream));
+    std::complex<double> r_norm2, pp, dad, rr;
+    CKR(K.dot(r, r, r_norm2));
+    CKR(K.dot(p, p, pp));
+    const double phi_norm = std::sqrt(pp.real());
+    int k = 0, conv = 0;
+    while (k < max_iter) {
+        ddag(d, ad);
+        CKR(K.dot(d, ad, dad));
+        const std::complex<double> alpha = r_norm2 / dad;
+        k_cs_xpay<<<g, 256, 0, c->stream>>>(xv, d, d2(alpha), n);
+        k_cs_xpay<<<g, 256, 0, c->stream>>>(r, ad, d2(-alpha), n);
+        CKR(K.dot(r, r, rr));
+        const double err_sqr = rr.real();
+        if (std::sqrt(err_sqr) < tol * phi_norm) {
+            conv = 1;
+            break;
+        }
+        const std::complex<double> beta = err_sqr / r_norm2;
+        k_cs_dbr<<<g, 256, 0, c->stream>>>(d, r, d2(beta), n);
+        r_norm2 = err_sqr;
+        k++;
+    }
+    CKL();
+    CKR(to_host(x, X, n, c->stream));
+    if (iterations) *iterations = k;
+    CKR(check_fine_waits(c->stream));
+    return conv ? AMG_OK : AMG_NOT_CONVERGED;
+}
+
+int amg_bicgstab(amg_ctx c, const double* phi, const double* x0, double* x, int max_iter, double tol,
+                 int* iterations) {
+    CKR(check_ready(c, 0, false));
+    if (!phi || !x || max_iter < 0 || !(tol > 0)) return fail(AMG_ERR_INVALID, "bad argument");
+    CKR(select_device(c));
+    FineKrylov K;
+    CKR(K.init(c));
+    const long long n = K.n;
+    DevBuf P, X, R, RT, D, S, T, AD;
+    CKR(to_dev(P, phi, n, c->stream));
+    CKR(to_dev(X, x0, n, c->stream));
+    if (!x0) CK(cudaMemsetAsync(X.p, 0, (size_t)n * sizeof(double2), c->stream));
+    CKR(to_dev(R, nullptr, n, c->stream));
+    CKR(to_dev(RT, nullptr, n, c->stream));
+    CKR(to_dev(D, nullptr, n, c->stream));
+    CKR(to_dev(S, nullptr, n, c->stream));
+    CKR(to_dev(T, nullptr, n, c->stream));
+    CKR(to_dev(AD, nullptr, n, c->stream));
+    double2 *p = P.as<double2>(), *xv = X.as<double2>(), *r = R.as<double2>(), *rt = RT.as<double2>(),
+            *d = D.as<double2>(), *sv = S.as<double2>(), *t = T.as<double2>(), *ad = AD.as<double2>();
+    const dim3 g = K.grid();
+    K.dirac(xv, ad, 0);
+    k_cs_rmaq<<<g, 256, 0, c->stream>>>(r, p, ad, make_double2(1.0, 0.0), n);   // r = b - A x
+    CK(cudaMemcpyAsync(rt, r, (size_t)n * sizeof(double2), cudaMemcpyDeviceToDevice, c->stream));
+    std::complex<double> pp, rho_i, rho_i_2, alpha, beta, omega, tmp, st, tt, ss;
+    CKR(K.dot(p, p, pp));
+    const double norm_phi = std::sqrt(pp.real());
+    int k = 0, conv = 0;
+    while (k < max_iter) {
+        CKR(K.dot(r, rt, rho_i));
+        if (k == 0) {
+            CK(cudaMemcpyAsync(d, r, (size_t)n * sizeof(double2), cudaMemcpyDeviceToDevice, c->stream));
+        } else {
+            beta = alpha * rho_i / (omega * rho_i_2);
+            k_cs_bicg_d<<<g, 256, 0, c->stream>>>(d, r, ad, d2(beta), d2(omega), n);
+        }
+        K.dirac(d, ad, 0);
+        CKR(K.dot(ad, rt, tmp));
+        alpha = rho_i / tmp;
+        k_cs_rmaq<<<g, 256, 0, c->stream>>>(sv, r, ad, d2(alpha), n);
+        CKR(K.dot(sv, sv, ss));
+        if (std::sqrt(ss.real()) < tol * norm_phi) {
+            k_cs_xpay<<<g, 256, 0, c->stream>>>(xv, d, d2(alpha), n);
+            conv = 1;
+            k++;
+            break;
+        }
+        K.dirac(sv, t, 0);
+        CKR(K.dot(sv, t, st));
+        CKR(K.dot(t, t, tt));
+        omega = st / tt;
+        k_cs_rmaq<<<g, 256, 0, c->stream>>>(r, sv, t, d2(omega), n);
+        k_cs_x3<<<g, 256, 0, c->stream>>>(xv, d, sv, d2(alpha), d2(omega), n);
+        rho_i_2 = rho_i;
+        k++;
+    }
+    CKL();
+    CKR(to_host(x, X, n, c->stream));
+    if (iterations) *iterations = k;
+    CKR(check_fine_waits(c->stream));
+    return conv ? AMG_OK : AMG_NOT_CONVERGED;
+}
+
 int amg_dirac_apply(amg_ctx c, const double* in, double* out, int nrhs, int dagger) {
     if (!c || !in || !out || nrhs < 1) return fail(AMG_ERR_INVALID, "bad argument");
     if (!c->gauge_set) return fail(AMG_ERR_STATE, "gauge field not set");

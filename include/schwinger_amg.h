@@ -137,6 +137,18 @@ AMG_API int amg_dirac_apply_dev(amg_ctx ctx, const void* in, void* out, int nrhs
  * in_dev / out_dev [nrhs][N][2] complex128, launched on `stream` (a cudaStream_t). */
 AMG_API int amg_dirac_apply_raw(const void* U_dev, const void* in_dev, void* out_dev, int nx, int nt,
                         int nrhs, double m0, int dagger, void* stream);
+/* Comparison solvers on the fine stencil (FP64, one source, host arrays; they need the gauge
+ * field, not the set-up):
+ * amg_cg_normal: conjugate_gradient (src/conjugate_gradient.cpp:5-65, run by Tests::CG,
+ *   src/tests.cpp:24-31): x = (D D^dagger)^{-1} phi from x = phi, CG until |r| < tol |phi|
+ *   (the reference's CG::tol = 1e-10, CG::max_iter = 100000, src/variables.cpp:84-87);
+ *   iterations = the reference's k at convergence.
+ * amg_bicgstab: bi_cgstab (src/bi_cgstab.cpp:5-89, run by Tests::BiCG with tol 1e-10): D x =
+ *   phi from x0 (NULL: zero); iterations = k + 1 at convergence.
+ * Both return AMG_OK when converged, AMG_NOT_CONVERGED after max_iter. */
+AMG_API int amg_cg_normal(amg_ctx ctx, const double* phi, double* x, int max_iter, double tol, int* iterations);
+AMG_API int amg_bicgstab(amg_ctx ctx, const double* phi, const double* x0, double* x, int max_iter, double tol,
+                         int* iterations);
 /* Self-test of the bounded device waits (no reference counterpart): runs the bulk-copy D apply
  * on caller-owned device memory (nt a multiple of 256, nx of 4, 16-byte aligned, distinct
  * in/out) without issuing its copies, so its first wait gives up after a short poll limit

@@ -40,6 +40,8 @@
 #include "params.h"
 #include "boundary.h"
 #include "amg.h"
+#include "bi_cgstab.h"
+#include "conjugate_gradient.h"
 #undef private
 
 namespace {
@@ -238,6 +240,21 @@ int main(int argc, char** argv) {
             for (int r = 0; r < reps; r++) D_phi(GConf.Conf, rhs, out, m0);
             info << "dphi_seconds_per_apply " << (now_s() - t0) / reps << "\n";
         }
+    }
+    // The comparison solvers (src/conjugate_gradient.cpp:5-65, src/bi_cgstab.cpp:5-89) on the
+    // rhs, as Tests::CG and Tests::BiCG run them (src/tests.cpp:3-31); their iteration counts
+    // are in the reference's own stdout lines.
+    if ((int)jd(job, "krylov", 0)) {
+        spinor y(N, c_vector(2, 0));
+        conjugate_gradient(GConf.Conf, rhs, y, m0);
+        dump_spinor("cg_x", y);
+        const spinor x0(N, c_vector(2, 0));
+        const spinor xb = bi_cgstab(&D_phi, N, 2, GConf.Conf, rhs, x0, m0, (int)jd(job, "bicg_max_iter", 100000),
+                                    1e-10, true, false);
+        dump_spinor("bicg_x", xb);
+        std::cout.flush();
+        g_manifest.close();
+        return 0;
     }
     if ((int)jd(job, "dphi_only", 0)) { g_manifest.close(); return 0; }
 

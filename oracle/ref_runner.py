@@ -55,7 +55,7 @@ def read_outputs(workdir: Path) -> dict:
 def run(ns: int, nt: int, rows, gauge: np.ndarray, rhs: np.ndarray, *, m0: float,
         cycle: int = 1, nit: int = 0, sap_tv_iters: int = 4, nu1: int = 0, nu2: int = 2,
         solve: int = 1, phases: int = 0, dump_hierarchy: int = 1, dphi_reps: int = 0,
-        dphi_only: int = 0, outer_iteration_reps: int = 0, hierarchy: dict | None = None, probes=None, workdir: str | None = None, timeout: float = 3600) -> dict:
+        dphi_only: int = 0, outer_iteration_reps: int = 0, hierarchy: dict | None = None, probes=None, workdir: str | None = None, timeout: float = 3600, krylov: int = 0) -> dict:
     """Writes the job, runs the binary for (ns, nt, len(rows)+1 levels), returns its dumps."""
     levels = len(rows) + 1
     b = binary(ns, nt, levels)
@@ -71,7 +71,7 @@ def run(ns: int, nt: int, rows, gauge: np.ndarray, rhs: np.ndarray, *, m0: float
     job = dict(m0=repr(float(m0)), cycle=cycle, nit=nit, sap_tv_iters=sap_tv_iters, nu1=nu1,
                nu2=nu2, solve=solve, phases=phases, dump_hierarchy=dump_hierarchy,
                dphi_reps=dphi_reps, dphi_only=dphi_only,
-               outer_iteration_reps=outer_iteration_reps)
+               outer_iteration_reps=outer_iteration_reps, krylov=krylov)
     (wd / "job.txt").write_text("".join(f"{k} {v}\n" for k, v in job.items()))
     np.ascontiguousarray(gauge, dtype=np.complex128).tofile(wd / "gauge.bin")
     np.ascontiguousarray(rhs, dtype=np.complex128).tofile(wd / "rhs.bin")

@@ -705,6 +705,64 @@ class AMG:
         return fgmres(func, precond, b, np.zeros_like(b), p.outer_m, p.outer_restarts, p.outer_tol, history)
 
 
+def cg_normal(U, phi, m0, nx, nt, max_iter: int = 100000, tol: float = 1e-10):
+    """conjugate_gradient (src/conjugate_gradient.cpp:5-65): x = (D D^dagger)^{-1} phi from
+    x = phi; returns (x, k, converged) with k the reference's iteration count at convergence."""
+    ddag = lambda v: d_phi(U, d_dagger_phi(U, v, m0, nx, nt), m0, nx, nt)
+    x = phi.astype(np.complex128).copy()
+    r = phi - ddag(x)
+    d = r.copy()
+    r_norm2 = np.sum(r * np.conj(r))
+    phi_norm = np.sqrt(np.real(np.sum(phi * np.conj(phi))))
+    k = 0
+    while k < max_iter:
+        Ad = ddag(d)
+        alpha = r_norm2 / np.sum(d * np.conj(Ad))
+        x = x + alpha * d
+        r = r - alpha * Ad
+        err_sqr = np.real(np.sum(r * np.conj(r)))
+        if np.sqrt(err_sqr) < tol * phi_norm:
+            return x, k, True
+        beta = err_sqr / r_norm2
+        d = d * beta + r
+        r_norm2 = err_sqr
+        k += 1
+    return x, k, False
+
+
+def bicgstab(U, phi, x0, m0, nx, nt, max_iter: int = 100000, tol: float = 1e-10):
+    """bi_cgstab (src/bi_cgstab.cpp:5-89) with func = D_phi: D x = phi from x0; returns
+    (x, iterations, converged) with iterations = k + 1 at convergence."""
+    A = lambda v: d_phi(U, v, m0, nx, nt)
+    x = x0.astype(np.complex128).copy()
+    r = phi - A(x)
+    r_tilde = r.copy()
+    norm_phi = np.sqrt(np.real(np.sum(phi * np.conj(phi))))
+    k = 0
+    alpha = omega = rho_i_2 = 0.0
+    d = np.zeros_like(r)
+    Ad = np.zeros_like(r)
+    while k < max_iter:
+        rho_i = np.sum(r * np.conj(r_tilde))
+        if k == 0:
+            d = r.copy()
+        else:
+            beta = alpha * rho_i / (omega * rho_i_2)
+            d = r + beta * (d - omega * Ad)
+        Ad = A(d)
+        alpha = rho_i / np.sum(Ad * np.conj(r_tilde))
+        s = r - alpha * Ad
+        if np.sqrt(np.real(np.sum(s * np.conj(s)))) < tol * norm_phi:
+            return x + alpha * d, k + 1, True
+        t = A(s)
+        omega = np.sum(s * np.conj(t)) / np.sum(t * np.conj(t))
+        r = s - omega * t
+        x = x + alpha * d + omega * s
+        rho_i_2 = rho_i
+        k += 1
+    return x, k, False
+
+
 def true_residual(U, x, b, m0, nx, nt) -> float:
     r = b - d_phi(U, x, m0, nx, nt)
     return float(np.linalg.norm(r) / np.linalg.norm(b))

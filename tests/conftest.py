@@ -24,8 +24,9 @@ def load_golden(name: str) -> dict:
 
 
 def golden_names():
-    """The solve-path fixtures (the adjoint fixtures, adj*, hold only the two solves)."""
-    return sorted(p.stem for p in GOLDEN.glob("*.npz") if not p.stem.startswith("adj"))
+    """The solve-path fixtures (the adjoint fixtures, adj*, hold only the two solves; the
+    krylov* fixtures only the comparison solvers)."""
+    return sorted(p.stem for p in GOLDEN.glob("*.npz") if not p.stem.startswith(("adj", "krylov")))
 
 
 def rel(a, b) -> float:

@@ -11,6 +11,10 @@ vectors and coarse links), per-level operator / P / P^dagger / SAP / GMRES probe
 preconditioner application, and the outer solve (x, iteration count, residual history).
 Large arrays are dropped for the bigger lattices to keep the files small.
 
+The Krylov fixture (KRYLOV) holds the reference's comparison solvers on one source: the
+conjugate_gradient solution of D D^dagger y = phi and the bi_cgstab solution of D x = phi,
+with the iteration counts the reference prints.
+
 The adjoint fixture (ADJOINT) holds the reference's two solves behind the gradient of
 L = Re(eta^dagger D^{-1} b): x = D^{-1} b and y = D^{-1} gamma5 eta (so lambda = gamma5 y),
 each a full FGMRES_AMG run of the reference; the gauge field and the two sources are
@@ -19,6 +23,7 @@ regenerated from the seeds in its meta.
 from __future__ import annotations
 
 import json
+import re
 import sys
 from pathlib import Path
 
@@ -49,6 +54,14 @@ CONFIGS = {
 # b = gaussian_spinor(N, 2, seed + 1000), eta = gaussian_spinor(N, 2, seed + 3000)
 ADJOINT = {
     "adj128_l3": (128, [[0, 8, 8, 12, 4, 4], [1, 4, 4, 12, 4, 4]], 2.0, -0.1, 21),
+}
+
+# The comparison solvers conjugate_gradient (on D D^dagger) and bi_cgstab of the reference
+# (src/conjugate_gradient.cpp:5-65, src/bi_cgstab.cpp:5-89) on one source:
+# name: (ns, rows, beta, m0, seed); U = gauge_field(ns, ns, beta, seed),
+# phi = gaussian_spinor(N, 2, seed + 1); iteration counts from the reference's own output.
+KRYLOV = {
+    "krylov32": (32, [[0, 4, 4, 8, 4, 4], [1, 2, 2, 8, 2, 2]], 3.0, -0.1, 31),
 }
 
 SMALL_KEYS_ALWAYS = ("dphi", "ddagphi", "x", "cycle0_rhs")
@@ -105,8 +118,27 @@ def make_adjoint(name: str, cfg) -> dict:
     return {"x": ox["x"], "y": oy["x"], "meta": np.array(json.dumps(meta))}
 
 
+def make_krylov(name: str, cfg) -> dict:
+    ns, rows, beta, m0, seed = cfg
+    ref_runner.build(ns, ns, len(rows) + 1)
+    U = gauge_field(ns, ns, beta, seed)
+    phi = gaussian_spinor(ns * ns, 2, seed + 1)
+    out = ref_runner.run(ns, ns, rows, U, phi, m0=m0, krylov=1, dump_hierarchy=0)
+    cg = re.search(r"^Converged in (\d+) iterations", out["stdout"], re.M)
+    bi = re.search(r"^Bi-CG-stab for D converged in (\d+) iterations", out["stdout"], re.M)
+    meta = dict(ns=ns, nt=ns, rows=rows, beta=beta, m0=m0, seed=seed,
+                cg_iterations=int(cg.group(1)), bicg_iterations=int(bi.group(1)))
+    return {"cg_x": out["cg_x"], "bicg_x": out["bicg_x"], "meta": np.array(json.dumps(meta))}
+
+
 def main(names=None):
     here = Path(__file__).resolve().parent
+    for name, cfg in KRYLOV.items():
+        if names and name not in names:
+            continue
+        arrays = make_krylov(name, cfg)
+        np.savez_compressed(here / f"{name}.npz", **arrays)
+        print(name, (here / f"{name}.npz").stat().st_size // 1024, "KiB")
     for name, cfg in ADJOINT.items():
         if names and name not in names:
             continue
