@@ -22,7 +22,8 @@ def binary(ns: int, nt: int, levels: int) -> Path:
 
 def build(ns: int, nt: int, levels: int, refdir: str = "/root/reference") -> Path:
     b = binary(ns, nt, levels)
-    if not b.exists():
+    # (re)built when missing or older than the harness source
+    if not b.exists() or b.stat().st_mtime < (HERE / "ref_harness.cpp").stat().st_mtime:
         subprocess.run([str(HERE / "build_ref.sh"), str(ns), str(nt), str(levels), refdir],
                        check=True, capture_output=True)
     return b
