@@ -156,8 +156,9 @@ class AMGContext:
         return x, it.value, st == _lib.AMG_OK
 
     def set_preconditioner(self, kind: int) -> None:
-        """amg_set_preconditioner: _lib.AMG_PRECOND_MG (FGMRES_AMG, default) or
-        _lib.AMG_PRECOND_SAP (the reference's FGMRES_SAP, include/sap.h:194-225)."""
+        """amg_set_preconditioner: _lib.AMG_PRECOND_MG (FGMRES_AMG, default),
+        _lib.AMG_PRECOND_SAP (the reference's FGMRES_SAP, include/sap.h:194-225) or
+        _lib.AMG_PRECOND_NONE (FGMRES_fine_level, include/fgmres.h:126-148)."""
         check(lib().amg_set_preconditioner(self._h, int(kind)), "amg_set_preconditioner")
 
     def dirac(self, psi, dagger: bool = False) -> np.ndarray:

@@ -25,6 +25,7 @@ AMG_CYCLE_V = 0
 AMG_CYCLE_K = 1
 AMG_PRECOND_MG = 0
 AMG_PRECOND_SAP = 1
+AMG_PRECOND_NONE = 2
 
 
 class AmgParams(C.Structure):

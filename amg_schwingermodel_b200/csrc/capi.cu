@@ -702,6 +702,10 @@ int run_graph(amg_context* c, const std::tuple<int, int, const void*, void*>& ke
 // into z.
 int precondition(amg_context* c, const double2* v, double2* z, int R, bool want_z = true) {
     const long long len = vlen0(c);
+    if (c->precond == AMG_PRECOND_NONE) {   // FGMRES_fine_level::preconditioner: z = v
+        CK(cudaMemcpyAsync(z, v, (size_t)R * len * sizeof(double2), cudaMemcpyDeviceToDevice, c->stream));
+        return AMG_OK;
+    }
     if (c->p.precision == AMG_PREC_F64) {
         // staged through fixed buffers, so one graph serves every Krylov slot
         double2* vs = c->vd.as<double2>();
@@ -916,8 +920,8 @@ struct OuterSolve {
         double2* dots = c->dots.as<double2>();
         double2* Vj = V + (long long)j * vstride;
         double2* Zj = Z + (long long)j * vstride;
-        if (!c->tuned && !c->prof_on) CKR(autotune(c, Vj, Zj, R));
-        const bool mixed = c->p.precision == AMG_PREC_MIXED;
+        if (!c->tuned && !c->prof_on && c->precond != AMG_PRECOND_NONE) CKR(autotune(c, Vj, Zj, R));
+        const bool mixed = c->p.precision == AMG_PREC_MIXED && c->precond != AMG_PRECOND_NONE;
         CKR(precondition(c, Vj, Zj, R, !mixed));
         {
             ProfScope ps_(c, AMG_PROF_FINE_OP, (double)c->N * (2.0 + 4.0 * R) * sizeof(double2));
@@ -1477,8 +1481,8 @@ int amg_set_cycle(amg_ctx c, int cycle) {
 
 int amg_set_preconditioner(amg_ctx c, int kind) {
     if (!c) return fail(AMG_ERR_INVALID, "null context");
-    if (kind != AMG_PRECOND_MG && kind != AMG_PRECOND_SAP)
-        return fail(AMG_ERR_INVALID, "preconditioner must be AMG_PRECOND_MG or AMG_PRECOND_SAP");
+    if (kind != AMG_PRECOND_MG && kind != AMG_PRECOND_SAP && kind != AMG_PRECOND_NONE)
+        return fail(AMG_ERR_INVALID, "preconditioner must be AMG_PRECOND_MG, AMG_PRECOND_SAP or AMG_PRECOND_NONE");
     c->precond = kind;
     c->drop_graphs();
     return AMG_OK;

@@ -82,6 +82,11 @@ inline int fgmres_restart_length = 20;
 inline int fgmres_restarts = 50;
 }  // namespace FGMRESV
 
+namespace CG {
+inline int max_iter = 100000;
+inline double tol = 1e-10;
+}  // namespace CG
+
 namespace LevelV {
 constexpr int maxLevel = AMGV::levels - 1;
 inline int BlocksX[AMGV::levels - 1] = {};
@@ -535,5 +540,76 @@ private:
     double m0;
     std::unique_ptr<amg_b200::Context> ctx_;
 };
+
+// ---- FGMRES_fine_level (include/fgmres.h:126-148): GMRES without preconditioning -------
+class FGMRES_fine_level {
+public:
+    FGMRES_fine_level(const int& dim1, const int& dim2, const int& m, const int& restarts, const double& tol,
+                      const c_matrix& U, const double& m0)
+        : dim1(dim1), dim2(dim2), m0(m0) {
+        const int sm = FGMRESV::fgmres_restart_length, sr = FGMRESV::fgmres_restarts;
+        const double st = FGMRESV::fgmres_tolerance;
+        FGMRESV::fgmres_restart_length = m;
+        FGMRESV::fgmres_restarts = restarts;
+        FGMRESV::fgmres_tolerance = tol;
+        ctx_ = std::make_unique<amg_b200::Context>(U, m0, 0);
+        FGMRESV::fgmres_restart_length = sm;
+        FGMRESV::fgmres_restarts = sr;
+        FGMRESV::fgmres_tolerance = st;
+        amg_b200::check(amg_setup(ctx_->get()), "FGMRES_fine_level");
+        amg_b200::check(amg_set_preconditioner(ctx_->get(), AMG_PRECOND_NONE), "FGMRES_fine_level");
+    }
+    // FGMRES::fgmres (include/fgmres.h:36)
+    int fgmres(const spinor& phi, const spinor& x0, spinor& x, const bool& print_message = false,
+               const bool save_res = false) {
+        (void)save_res;
+        return amg_b200::fgmres_on(ctx_->get(), phi, x0, x, print_message, nullptr);
+    }
+
+private:
+    int dim1, dim2;
+    double m0;
+    std::unique_ptr<amg_b200::Context> ctx_;
+};
+
+// ---- conjugate_gradient (include/conjugate_gradient.h:19): x = (D D^dagger)^{-1} phi ----
+// from x = phi with CG::max_iter and CG::tol; returns the iteration count at convergence, or
+// CG::max_iter when it did not converge (the reference prints a message then)
+inline int conjugate_gradient(const c_matrix& U, const spinor& phi, spinor& x, const double& m0) {
+    amg_b200::Context ctx(U, m0, 0);
+    std::vector<c_double> b = amg_b200::flatten(phi), xf(b.size());
+    int it = 0;
+    const int st = amg_b200::check(amg_cg_normal(ctx.get(), amg_b200::dptr(b), amg_b200::dptr(xf), CG::max_iter,
+                                                 CG::tol, &it),
+                                   "conjugate_gradient");
+    amg_b200::unflatten(xf, x);
+    if (st != AMG_OK) std::cout << "CG did not converge in " << CG::max_iter << " iterations" << std::endl;
+    return it;
+}
+
+// ---- bi_cgstab (include/bi_cgstab.h:27-29) with func = D_phi ----------------------------
+// returns the solution of D x = phi from x0; other operators than D_phi are not offered
+inline spinor bi_cgstab(void (*func)(const c_matrix&, const spinor&, spinor&, const double&), const int& dim1,
+                        const int& dim2, const c_matrix& U, const c_matrix& phi, const c_matrix& x0, const double& m0,
+                        const int& max_iter, const double& tol, const bool& print_message,
+                        const bool& save_residuals) {
+    (void)save_residuals;
+    if (func != &D_phi) throw amg_b200::Error(AMG_ERR_INVALID, "bi_cgstab: only func = D_phi is offered");
+    amg_b200::Context ctx(U, m0, 0);
+    std::vector<c_double> b = amg_b200::flatten(phi), x0f = amg_b200::flatten(x0), xf(b.size());
+    int it = 0;
+    const int st = amg_b200::check(amg_bicgstab(ctx.get(), amg_b200::dptr(b), amg_b200::dptr(x0f),
+                                                amg_b200::dptr(xf), max_iter, tol, &it),
+                                   "bi_cgstab");
+    spinor x(dim1, c_vector(dim2, 0));
+    amg_b200::unflatten(xf, x);
+    if (print_message) {
+        if (st == AMG_OK)
+            std::cout << "Bi-CG-stab for D converged in " << it << " iterations" << std::endl;
+        else
+            std::cout << "Bi-CG-stab did not converge in " << max_iter << " iterations" << std::endl;
+    }
+    return x;
+}
 
 #endif

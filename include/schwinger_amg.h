@@ -50,6 +50,7 @@ extern "C" {
 /* preconditioner of the outer FGMRES (amg_set_preconditioner) */
 #define AMG_PRECOND_MG 0         /* FGMRES_AMG: the K- or V-cycle (include/amg.h:99-145) */
 #define AMG_PRECOND_SAP 1        /* FGMRES_SAP: one fine-level SAP sweep (include/sap.h:194-225) */
+#define AMG_PRECOND_NONE 2       /* FGMRES_fine_level: no preconditioner (include/fgmres.h:126-148) */
 
 typedef struct amg_context* amg_ctx;
 
@@ -115,10 +116,13 @@ AMG_API int amg_set_mass(amg_ctx ctx, double m0);
  * AMG_CYCLE_V for the amg_cycle, amg_solve and bootstrap calls that follow. */
 AMG_API int amg_set_cycle(amg_ctx ctx, int cycle);
 /* Chooses the outer FGMRES's preconditioner for the amg_solve* calls that follow:
- * AMG_PRECOND_MG (default, FGMRES_AMG) or AMG_PRECOND_SAP, the reference's comparison solver
+ * AMG_PRECOND_MG (default, FGMRES_AMG); AMG_PRECOND_SAP, the reference's comparison solver
  * FGMRES_SAP (include/sap.h:194-225, run by Tests::FGMRES_sap, src/tests.cpp:33-46): each
  * preconditioner call zeroes z and applies SAP_C::SAP(v, z, nu = 1) on the fine level, with
- * the fine SAP kernels of the context's precision.  The solve still needs amg_setup (the SAP
+ * the fine SAP kernels of the context's precision; or AMG_PRECOND_NONE, GMRES without
+ * preconditioning (FGMRES_fine_level, include/fgmres.h:126-148, run by Tests::GMRES,
+ * src/tests.cpp:13-22; FP64 whatever the context's precision; amg_params.outer_m /
+ * outer_restarts give its restart length and count).  The solve still needs amg_setup (the
  * work buffers live with the hierarchy). */
 AMG_API int amg_set_preconditioner(amg_ctx ctx, int kind);
 /* Level sizes as LevelV fills them: out[l] = {Nsites, NxSites, NtSites, DOF, Colors, Ntest}. */

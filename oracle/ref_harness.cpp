@@ -252,6 +252,12 @@ int main(int argc, char** argv) {
         const spinor xb = bi_cgstab(&D_phi, N, 2, GConf.Conf, rhs, x0, m0, (int)jd(job, "bicg_max_iter", 100000),
                                     1e-10, true, false);
         dump_spinor("bicg_x", xb);
+        // Tests::GMRES (src/tests.cpp:13-22): FGMRES_fine_level(20, 50, 1e-10), x0 = 0
+        FGMRES_fine_level fg(N, 2, 20, 50, 1e-10, GConf.Conf, m0);
+        spinor xg(N, c_vector(2, 0));
+        const int git = fg.fgmres(rhs, x0, xg, false, false);
+        dump_spinor("gmres_x", xg);
+        info << "gmres_iterations " << git << "\n";
         std::cout.flush();
         g_manifest.close();
         return 0;

@@ -705,6 +705,14 @@ class AMG:
         return fgmres(func, precond, b, np.zeros_like(b), p.outer_m, p.outer_restarts, p.outer_tol, history)
 
 
+def gmres_fine(U, phi, x0, m0, nx, nt, m: int = 20, restarts: int = 50, tol: float = 1e-10,
+               history: list | None = None):
+    """FGMRES_fine_level::fgmres (include/fgmres.h:126-148, run by Tests::GMRES,
+    src/tests.cpp:13-22): func = D_phi, the identity as preconditioner; returns (x, iterations)."""
+    func = lambda z: d_phi(U, z, m0, nx, nt)
+    return fgmres(func, lambda v, z: v.copy(), phi, x0, m, restarts, tol, history)
+
+
 def cg_normal(U, phi, m0, nx, nt, max_iter: int = 100000, tol: float = 1e-10):
     """conjugate_gradient (src/conjugate_gradient.cpp:5-65): x = (D D^dagger)^{-1} phi from
     x = phi; returns (x, k, converged) with k the reference's iteration count at convergence."""

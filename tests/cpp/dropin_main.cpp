@@ -7,7 +7,7 @@
 //   dropin_main <workdir>
 // reads  parameters.dat, gauge.ctxt ("x t mu re im"), rhs.rhs ("x t spin re im"), m0.txt,
 //        probe_l<l>.bin (complex128 [N_l][DOF_l])
-// writes x.bin, dphi.bin, ddagphi.bin, dop_l<l>.bin, pt_l0.bin, ppt_l0.bin, sap_l0.bin,
+// writes x.bin, x_sap.bin, x_gmres.bin, x_cg.bin, x_bicg.bin, dphi.bin, ddagphi.bin, dop_l<l>.bin, pt_l0.bin, ppt_l0.bin, sap_l0.bin,
 //        gmres_l<L-1>.bin, cycle0_rhs.bin (complex128) and results.txt
 #include <cstdio>
 
@@ -64,6 +64,17 @@ int main(int argc, char** argv) {
         const int its = sap_solver.fgmres(rhs, x0, xsap, false, false);
         dump(wd + "/x_sap.bin", xsap);
         res << "sap_solver_iterations " << its << "\n";
+
+        // Tests::GMRES, Tests::CG, Tests::BiCG (src/tests.cpp:5-31): the comparison solvers
+        spinor xg(LevelV::Nsites[0], c_vector(LevelV::DOF[0], 0));
+        FGMRES_fine_level gmres(LV::Ntot, 2, 20, 50, 1e-10, GConf.Conf, m0);
+        res << "gmres_iterations " << gmres.fgmres(rhs, x0, xg, false, false) << "\n";
+        dump(wd + "/x_gmres.bin", xg);
+        spinor xc(LevelV::Nsites[0], c_vector(LevelV::DOF[0], 0));
+        res << "cg_iterations " << conjugate_gradient(GConf.Conf, rhs, xc, m0) << "\n";
+        dump(wd + "/x_cg.bin", xc);
+        const spinor xb = bi_cgstab(&D_phi, LV::Ntot, 2, GConf.Conf, rhs, x0, m0, 100000, 1e-10, false, false);
+        dump(wd + "/x_bicg.bin", xb);
 
         spinor d(LevelV::Nsites[0], c_vector(2, 0));
         D_phi(GConf.Conf, rhs, d, m0);

@@ -12,8 +12,8 @@ preconditioner application, and the outer solve (x, iteration count, residual hi
 Large arrays are dropped for the bigger lattices to keep the files small.
 
 The Krylov fixture (KRYLOV) holds the reference's comparison solvers on one source: the
-conjugate_gradient solution of D D^dagger y = phi and the bi_cgstab solution of D x = phi,
-with the iteration counts the reference prints.
+conjugate_gradient solution of D D^dagger y = phi, the bi_cgstab solution of D x = phi and
+the unpreconditioned FGMRES_fine_level(20, 50) solution, with their iteration counts.
 
 The adjoint fixture (ADJOINT) holds the reference's two solves behind the gradient of
 L = Re(eta^dagger D^{-1} b): x = D^{-1} b and y = D^{-1} gamma5 eta (so lambda = gamma5 y),
@@ -56,8 +56,9 @@ ADJOINT = {
     "adj128_l3": (128, [[0, 8, 8, 12, 4, 4], [1, 4, 4, 12, 4, 4]], 2.0, -0.1, 21),
 }
 
-# The comparison solvers conjugate_gradient (on D D^dagger) and bi_cgstab of the reference
-# (src/conjugate_gradient.cpp:5-65, src/bi_cgstab.cpp:5-89) on one source:
+# The comparison solvers conjugate_gradient (on D D^dagger), bi_cgstab and the
+# unpreconditioned FGMRES_fine_level of the reference (src/conjugate_gradient.cpp:5-65,
+# src/bi_cgstab.cpp:5-89, include/fgmres.h:126-148) on one source:
 # name: (ns, rows, beta, m0, seed); U = gauge_field(ns, ns, beta, seed),
 # phi = gaussian_spinor(N, 2, seed + 1); iteration counts from the reference's own output.
 KRYLOV = {
@@ -127,8 +128,10 @@ def make_krylov(name: str, cfg) -> dict:
     cg = re.search(r"^Converged in (\d+) iterations", out["stdout"], re.M)
     bi = re.search(r"^Bi-CG-stab for D converged in (\d+) iterations", out["stdout"], re.M)
     meta = dict(ns=ns, nt=ns, rows=rows, beta=beta, m0=m0, seed=seed,
-                cg_iterations=int(cg.group(1)), bicg_iterations=int(bi.group(1)))
-    return {"cg_x": out["cg_x"], "bicg_x": out["bicg_x"], "meta": np.array(json.dumps(meta))}
+                cg_iterations=int(cg.group(1)), bicg_iterations=int(bi.group(1)),
+                gmres_iterations=int(out["info:gmres_iterations"]))
+    return {"cg_x": out["cg_x"], "bicg_x": out["bicg_x"], "gmres_x": out["gmres_x"],
+            "meta": np.array(json.dumps(meta))}
 
 
 def main(names=None):

@@ -2,14 +2,16 @@
 (tests/cpp/dropin_main.cpp) written against the reference's class and function names --
 readParameters, GaugeConf::read_conf, read_rhs, FGMRES_AMG::fgmres, D_phi, D_dagger_phi,
 AlgebraicMG::setUpPhase / k_cycle / applyMultilevel, Level::D_operator / Pt_v / P_v,
-SAP_level_l::SAP, GMRES_level_l::fgmres, FGMRES_SAP::fgmres -- built with g++ against
-libschwinger_amg.so.
+SAP_level_l::SAP, GMRES_level_l::fgmres, FGMRES_SAP::fgmres, FGMRES_fine_level::fgmres,
+conjugate_gradient, bi_cgstab -- built with g++ against libschwinger_amg.so.
 
 CPU: the driver compiles and links for two lattice configurations.
 GPU: it reproduces the golden fixtures (outputs of the reference itself on the same
 inputs, passed in the reference's text formats): iteration count equal, x within 1e-8,
-D and D^dagger within 1e-13, level operations within 1e-8; FGMRES_SAP within one iteration
-and 1e-8 of the restatement.
+D and D^dagger within 1e-13, level operations within 1e-8; FGMRES_SAP and the
+unpreconditioned FGMRES_fine_level within one iteration and 1e-8 of the restatement;
+conjugate_gradient within two iterations and 1e-8, bi_cgstab within 1e-8 of the restatement
+(itself equal to the reference's runs on the Krylov fixture).
 """
 import subprocess
 from pathlib import Path
@@ -85,6 +87,15 @@ def test_driver_reproduces_reference(name, tmp_path):
     x_ref, it_ref = R.AMG(g["gauge"], m["ns"], m["nt"], rows4, R.SolverParams(m0=m["m0"])).solve_sap(g["rhs"])
     assert abs(int(res["sap_solver_iterations"]) - it_ref) <= 1, (res["sap_solver_iterations"], it_ref)
     assert rel(out("x_sap", x_ref), x_ref) < 1e-8
+    ns, nt, m0 = m["ns"], m["nt"], m["m0"]
+    x_g, it_g = R.gmres_fine(g["gauge"], g["rhs"], np.zeros_like(g["rhs"]), m0, ns, nt)
+    assert abs(int(res["gmres_iterations"]) - it_g) <= 1, (res["gmres_iterations"], it_g)
+    assert rel(out("x_gmres", x_g), x_g) < 1e-8
+    x_c, it_c, _ = R.cg_normal(g["gauge"], g["rhs"], m0, ns, nt)
+    assert abs(int(res["cg_iterations"]) - it_c) <= 2, (res["cg_iterations"], it_c)
+    assert rel(out("x_cg", x_c), x_c) < 1e-8
+    x_b, _, _ = R.bicgstab(g["gauge"], g["rhs"], np.zeros_like(g["rhs"]), m0, ns, nt)
+    assert rel(out("x_bicg", x_b), x_b) < 1e-8
     assert rel(out("dphi", g["dphi"]), g["dphi"]) < 1e-13
     assert rel(out("ddagphi", g["ddagphi"]), g["ddagphi"]) < 1e-13
     assert rel(out("dop_l0", g["dop_l0"]), g["dop_l0"]) < 1e-13

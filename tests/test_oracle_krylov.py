@@ -1,7 +1,8 @@
 """The restated comparison solvers against the reference's own runs (tests/golden/krylov32.npz,
 made by tests/golden/make_golden.py from the compiled reference): conjugate_gradient on
-D D^dagger (src/conjugate_gradient.cpp:5-65) and bi_cgstab (src/bi_cgstab.cpp:5-89) give
-the reference's iteration counts exactly and its solutions to 1e-10."""
+D D^dagger (src/conjugate_gradient.cpp:5-65), bi_cgstab (src/bi_cgstab.cpp:5-89) and the
+unpreconditioned FGMRES_fine_level(20, 50) (include/fgmres.h:126-148) give the reference's
+iteration counts exactly and its solutions to 1e-10."""
 import numpy as np
 
 from conftest import load_golden, rel
@@ -21,3 +22,15 @@ def test_restated_cg_and_bicgstab_match_reference():
     x, k2, ok2 = R.bicgstab(U, phi, np.zeros_like(phi), m0, ns, ns)
     assert ok2 and k2 == m["bicg_iterations"], (k2, m["bicg_iterations"])
     assert rel(x, g["bicg_x"]) < 1e-10
+
+
+def test_restated_unpreconditioned_gmres_matches_reference():
+    from amg_schwingermodel_b200.inputs import gauge_field, gaussian_spinor
+    g = load_golden("krylov32")
+    m = g["meta"]
+    ns, m0 = m["ns"], m["m0"]
+    U = gauge_field(ns, ns, m["beta"], m["seed"])
+    phi = gaussian_spinor(ns * ns, 2, m["seed"] + 1)
+    x, it = R.gmres_fine(U, phi, np.zeros_like(phi), m0, ns, ns)
+    assert it == m["gmres_iterations"], (it, m["gmres_iterations"])
+    assert rel(x, g["gmres_x"]) < 1e-10
