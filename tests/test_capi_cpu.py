@@ -72,3 +72,18 @@ def test_bad_blocking_is_rejected_on_the_host():
     r = np.array([0, 8, 8, 10, 4, 4], dtype=np.int32)
     st = L.amg_create(C.byref(h), 64, 64, 7, r.ctypes.data_as(C.c_void_p), -0.1, C.byref(p), 0)
     assert st == _lib.AMG_ERR_INVALID
+
+
+def test_header_constants_match_the_python_binding():
+    """Every integer constant the header defines has the same value in _lib: the status codes,
+    precision, cycle and preconditioner selectors by name, the profiling slots through
+    _lib.PROF_SLOTS."""
+    consts = dict(re.findall(r"^#define (AMG_[A-Z0-9_]+)\s+\(?(-?\d+)\)?", HEADER.read_text(), flags=re.M))
+    assert "AMG_PRECOND_NONE" in consts and len(consts) >= 20
+    prof = {k: int(consts.pop(k)) for k in list(consts) if k.startswith("AMG_PROF_")}
+    assert prof.pop("AMG_PROF_SLOTS") == len(_lib.PROF_SLOTS)
+    assert {k[len("AMG_PROF_"):].lower(): v for k, v in prof.items()} == _lib.PROF_SLOTS
+    missing = [k for k in consts if not hasattr(_lib, k)]
+    assert not missing, missing
+    wrong = {k: (v, getattr(_lib, k)) for k, v in consts.items() if getattr(_lib, k) != int(v)}
+    assert not wrong, wrong
