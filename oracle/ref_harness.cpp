@@ -13,6 +13,9 @@
  *   <workdir>/rhs.bin      b[N][2] complex128
  *   <workdir>/probe_l<l>.bin  optional per-level probe vectors [N_l][DOF_l] complex128
  * Outputs (raw little-endian arrays, listed with dtype and shape in <workdir>/manifest.txt).
+ * With `ranks N` in job.txt the job runs as N processes (the reference's MPI layout, see
+ * oracle/mpi_shim/mpi.h); rank 0 writes the outputs above, ranks r > 0 write theirs under
+ * <workdir>/rank<r>/.
  *
  * The reference's private members are needed to dump the set-up hierarchy that
  * FGMRES_AMG builds in its constructor (include/amg.h:101-119); they are opened by
@@ -36,6 +39,8 @@
 #include <utility>
 #include <vector>
 
+#include <sys/stat.h>
+
 #define private public
 #include "params.h"
 #include "boundary.h"
@@ -46,7 +51,8 @@
 
 namespace {
 
-std::string g_dir;
+std::string g_dir;   // the job's directory: inputs, and rank 0's outputs
+std::string g_out;   // where this rank writes (rank r > 0: <workdir>/rank<r>)
 std::ofstream g_manifest;
 
 double now_s() {
@@ -56,7 +62,7 @@ double now_s() {
 
 void dump_raw(const std::string& name, const void* data, size_t bytes, const char* dtype,
               const std::vector<long>& shape) {
-    std::ofstream f(g_dir + "/" + name + ".bin", std::ios::binary);
+    std::ofstream f(g_out + "/" + name + ".bin", std::ios::binary);
     f.write(reinterpret_cast<const char*>(data), (std::streamsize)bytes);
     g_manifest << name << " " << dtype;
     for (long s : shape) g_manifest << " " << s;
@@ -77,6 +83,48 @@ void dump_cvec(const std::string& name, const c_vector& v) {
 
 void dump_ivec(const std::string& name, const std::vector<int>& v) {
     dump_raw(name, v.data(), v.size() * sizeof(int), "i4", {(long)v.size()});
+}
+
+// Runs the rest of the job as `ranks` processes (oracle/mpi_shim/mpi.h), the reference's
+// MPI layout on this host's cores: the SAP blocks of each colour are split among the ranks
+// as SAPV::sap_blocks_per_proc says (src/sap.cpp:77-78), everything else is repeated by
+// every rank.  Ranks r > 0 write under <workdir>/rank<r>/ from here on; `info`, when given,
+// is flushed before the fork and reopened there by those ranks.  Started after the set-up,
+// the ranks share its pages copy-on-write; an MPI run holds the same hierarchy on every rank
+// (one seed for all ranks, src/amg.cpp:8, and exact SAP sums), so what follows is the
+// np-rank run's.
+bool start_ranks(int ranks, std::ofstream* info) {
+    if (ranks <= 1) return true;
+    size_t slot = 0;
+    int coloring = 1;
+    for (int l = 0; l < AMGV::levels; l++) {
+        slot = std::max(slot, (size_t)LevelV::Nsites[l] * LevelV::DOF[l] * sizeof(c_double));
+        const int nb = LevelV::SAP_Block_x[l] * LevelV::SAP_Block_t[l];
+        coloring = std::max(coloring, nb != 1 ? nb / 2 : 1);
+    }
+    if (info) info->flush();
+    if (g_manifest.is_open()) g_manifest.flush();
+    std::cout.flush();
+    std::cerr.flush();
+    oracle_mpi_spawn(ranks, slot);
+    SAPV::sap_blocks_per_proc = (coloring + ranks - 1) / ranks;
+    if (oracle_mpi().rank == 0) return true;
+    g_out = g_dir + "/rank" + std::to_string(oracle_mpi().rank);
+    mkdir(g_out.c_str(), 0755);
+    if (chdir(g_out.c_str()) != 0) {
+        std::cerr << "cannot enter " << g_out << "\n";
+        return false;
+    }
+    if (info) {
+        info->close();
+        info->open(g_out + "/info.txt");
+        *info << std::setprecision(17);
+    }
+    if (g_manifest.is_open()) {
+        g_manifest.close();
+        g_manifest.open(g_out + "/manifest.txt");
+    }
+    return true;
 }
 
 bool read_spinor(const std::string& path, spinor& v) {
@@ -196,11 +244,24 @@ int main(int argc, char** argv) {
         std::cerr << "usage: " << argv[0] << " <workdir>\n";
         return 2;
     }
-    g_dir = argv[1];
-    g_manifest.open(g_dir + "/manifest.txt");
+    {
+        char* abs = realpath(argv[1], nullptr);
+        if (!abs) { std::cerr << "workdir " << argv[1] << " not found\n"; return 2; }
+        g_dir = abs;
+        std::free(abs);
+    }
     auto job = read_job(g_dir + "/job.txt");
 
     readParameters(g_dir + "/params.dat");
+    // `ranks` > 1: the reference's MPI layout on this host's cores, see start_ranks.  With
+    // `ranks_after_setup` 1 the ranks start just before a timed loop instead of here.
+    const int ranks = std::max(1, (int)jd(job, "ranks", 1));
+    const bool late_ranks = (int)jd(job, "ranks_after_setup", 0) != 0;
+    // with one rank every block of a colour is solved by this process (src/sap.cpp:77-78)
+    SAPV::sap_blocks_per_proc = 1 << 30;
+    g_out = g_dir;
+    if (!late_ranks && !start_ranks(ranks, nullptr)) return 3;
+    g_manifest.open(g_out + "/manifest.txt");
     Coordinates();
     boundary();
 
@@ -210,8 +271,6 @@ int main(int argc, char** argv) {
     AMGV::nu1 = (int)jd(job, "nu1", 0);
     AMGV::nu2 = (int)jd(job, "nu2", 2);
     mass::m0 = jd(job, "m0", -0.1);
-    // Every block of a colour must be solved by this single rank (src/sap.cpp:77-78).
-    SAPV::sap_blocks_per_proc = 1 << 30;
     const double m0 = mass::m0;
     const int N = LV::Ntot;
 
@@ -224,7 +283,7 @@ int main(int argc, char** argv) {
     spinor rhs(N, c_vector(2, 0));
     if (!read_spinor(g_dir + "/rhs.bin", rhs)) { std::cerr << "rhs.bin missing\n"; return 3; }
 
-    std::ofstream info(g_dir + "/info.txt");
+    std::ofstream info(g_out + "/info.txt");
     info << std::setprecision(17);
 
     // D_phi / D_dagger_phi (src/dirac_operator.cpp:3-54) on the rhs.
@@ -308,6 +367,7 @@ int main(int argc, char** argv) {
         spinor v(N, c_vector(2, 0)), z(N, c_vector(2, 0)), w(N, c_vector(2, 0));
         double nb = std::sqrt(std::real(dot(rhs, rhs)));
         for (int n = 0; n < N; n++) for (int a = 0; a < 2; a++) v[n][a] = rhs[n][a] / nb;
+        if (late_ranks && !start_ranks(ranks, &info)) return 3;
         for (int r = 0; r < reps; r++) {
             double t1 = now_s();
             for (auto& row : z) { row[0] = 0; row[1] = 0; }
@@ -389,6 +449,7 @@ int main(int argc, char** argv) {
         spinor v(N, c_vector(2, 0)), z(N, c_vector(2, 0)), w(N, c_vector(2, 0));
         double nb = std::sqrt(std::real(dot(rhs, rhs)));
         for (int n = 0; n < N; n++) for (int a = 0; a < 2; a++) v[n][a] = rhs[n][a] / nb;
+        if (late_ranks && !start_ranks(ranks, &info)) return 3;
         double t1 = now_s();
         for (int r = 0; r < reps; r++) {
             double t2 = now_s();

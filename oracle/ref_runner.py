@@ -20,7 +20,15 @@ def binary(ns: int, nt: int, levels: int) -> Path:
     return REF_DIR / f"ref_{ns}x{nt}_l{levels}"
 
 
-def build(ns: int, nt: int, levels: int, refdir: str = "/root/reference") -> Path:
+DEFAULT_REFDIR = os.environ.get("AMG_REFERENCE_DIR", "/root/reference")
+
+
+def available(ns: int, nt: int, levels: int, refdir: str = DEFAULT_REFDIR) -> bool:
+    """The binary exists, or the reference sources to build it do."""
+    return binary(ns, nt, levels).exists() or (Path(refdir) / "src" / "amg.cpp").exists()
+
+
+def build(ns: int, nt: int, levels: int, refdir: str = DEFAULT_REFDIR) -> Path:
     b = binary(ns, nt, levels)
     # (re)built when missing or older than the harness source
     if not b.exists() or b.stat().st_mtime < (HERE / "ref_harness.cpp").stat().st_mtime:
@@ -56,8 +64,14 @@ def read_outputs(workdir: Path) -> dict:
 def run(ns: int, nt: int, rows, gauge: np.ndarray, rhs: np.ndarray, *, m0: float,
         cycle: int = 1, nit: int = 0, sap_tv_iters: int = 4, nu1: int = 0, nu2: int = 2,
         solve: int = 1, phases: int = 0, dump_hierarchy: int = 1, dphi_reps: int = 0,
-        dphi_only: int = 0, outer_iteration_reps: int = 0, hierarchy: dict | None = None, probes=None, workdir: str | None = None, timeout: float = 3600, krylov: int = 0) -> dict:
-    """Writes the job, runs the binary for (ns, nt, len(rows)+1 levels), returns its dumps."""
+        dphi_only: int = 0, outer_iteration_reps: int = 0, hierarchy: dict | None = None, probes=None,
+        workdir: str | None = None, timeout: float = 3600, krylov: int = 0, ranks: int = 1,
+        ranks_after_setup: int = 0) -> dict:
+    """Writes the job, runs the binary for (ns, nt, len(rows)+1 levels), returns its dumps
+    (rank 0's).  ranks > 1 runs the reference's MPI layout as that many processes on this
+    host (oracle/mpi_shim/mpi.h): its SAP block solves split among them; with
+    ranks_after_setup = 1 the ranks start after the set-up, just before the timed outer
+    iterations (they then share the set-up's memory)."""
     levels = len(rows) + 1
     b = binary(ns, nt, levels)
     if not b.exists():
@@ -72,7 +86,8 @@ def run(ns: int, nt: int, rows, gauge: np.ndarray, rhs: np.ndarray, *, m0: float
     job = dict(m0=repr(float(m0)), cycle=cycle, nit=nit, sap_tv_iters=sap_tv_iters, nu1=nu1,
                nu2=nu2, solve=solve, phases=phases, dump_hierarchy=dump_hierarchy,
                dphi_reps=dphi_reps, dphi_only=dphi_only,
-               outer_iteration_reps=outer_iteration_reps, krylov=krylov)
+               outer_iteration_reps=outer_iteration_reps, krylov=krylov, ranks=ranks,
+               ranks_after_setup=ranks_after_setup)
     (wd / "job.txt").write_text("".join(f"{k} {v}\n" for k, v in job.items()))
     np.ascontiguousarray(gauge, dtype=np.complex128).tofile(wd / "gauge.bin")
     np.ascontiguousarray(rhs, dtype=np.complex128).tofile(wd / "rhs.bin")
