@@ -70,7 +70,7 @@ inline int oracle_mpi_type_size(MPI_Datatype t) {
 struct oracle_mpi_ctl {
     std::atomic<int> count;   // ranks arrived at the open barrier
     std::atomic<int> gen;     // barrier generation
-    std::atomic<int> failed;  // set by a rank that gave up
+    std::atomic<int> failed;  // 1: a rank gave up; 2: rank 0 has finished the job
 };
 
 struct oracle_mpi_state {
@@ -103,11 +103,14 @@ inline char* oracle_mpi_slot(int r) {
     std::_Exit(70);
 }
 
-// Called while a barrier of generation g is open: gives up when a rank has failed, when the
-// parent (rank 0) is gone, or when a child rank has exited while the barrier is still open.
+// Called while a barrier of generation g is open: gives up when a rank has failed or rank 0
+// has finished (the flag counts only if this barrier is still open after it was read), when
+// the parent (rank 0) is gone, or when a child rank has exited while the barrier is open.
 inline void oracle_mpi_check_alive(oracle_mpi_ctl* c, int g) {
     auto& s = oracle_mpi();
-    if (c->failed.load()) oracle_mpi_fail("another rank failed");
+    const int f = c->failed.load(std::memory_order_acquire);
+    if (f != 0 && c->gen.load(std::memory_order_acquire) == g)
+        oracle_mpi_fail(f == 1 ? "another rank failed" : "rank 0 finished while this rank waits in a collective");
     if (s.rank != 0 && getppid() != s.parent) oracle_mpi_fail("rank 0 is gone");
     for (pid_t k : s.kids) {
         siginfo_t info;
@@ -140,6 +143,8 @@ inline void oracle_mpi_barrier() {
 inline void oracle_mpi_join() {
     auto& s = oracle_mpi();
     if (s.rank != 0) return;
+    // a rank still waiting in a collective now can never be released: let it give up
+    if (s.shm) oracle_mpi_control()->failed.store(2, std::memory_order_release);
     bool ok = true;
     for (pid_t k : s.kids) {
         int st = 0;

@@ -30,8 +30,9 @@ def available(ns: int, nt: int, levels: int, refdir: str = DEFAULT_REFDIR) -> bo
 
 def build(ns: int, nt: int, levels: int, refdir: str = DEFAULT_REFDIR) -> Path:
     b = binary(ns, nt, levels)
-    # (re)built when missing or older than the harness source
-    if not b.exists() or b.stat().st_mtime < (HERE / "ref_harness.cpp").stat().st_mtime:
+    # (re)built when missing or older than the harness or the MPI stand-in
+    newest = max((HERE / f).stat().st_mtime for f in ("ref_harness.cpp", "mpi_shim/mpi.h", "build_ref.sh"))
+    if not b.exists() or b.stat().st_mtime < newest:
         subprocess.run([str(HERE / "build_ref.sh"), str(ns), str(nt), str(levels), refdir],
                        check=True, capture_output=True)
     return b
