@@ -4,7 +4,9 @@ reference's MPI layout, its SAP block solves of each colour split among the rank
 run's results exactly -- the solution, the iteration count and the residual history -- for
 2, 3 and 4 ranks (an uneven split of the 8 blocks per colour included), with the ranks
 started at the beginning or after the set-up (the timed-sample mode the CPU baseline
-uses).  Needs the reference sources to build oracle/_ref/ref_32x32_l3; skipped without."""
+uses).  A rank that leaves before its first collective ends the job with an error within
+seconds instead of leaving the others waiting.  Needs the reference sources to build
+oracle/_ref/ref_32x32_l3; skipped without."""
 import numpy as np
 import pytest
 
@@ -51,3 +53,12 @@ def test_ranks_started_after_setup_give_the_one_rank_cycle(oracle_binary):
         assert all(out[f"info:outer_iteration_seconds_{r}"] > 0 for r in range(2))
     assert np.array_equal(z[4], z[1]) and np.array_equal(z[3], z[1])
     assert np.linalg.norm(z[1]) > 0
+
+
+def test_a_lost_rank_ends_the_job_with_an_error(oracle_binary):
+    import time
+    U, b = _inputs()
+    t0 = time.time()
+    with pytest.raises(RuntimeError, match="exited inside a collective"):
+        ref_runner.run(NS, NS, ROWS, U, b, m0=M0, dump_hierarchy=0, ranks=3, drill_exit_rank=2, timeout=120)
+    assert time.time() - t0 < 60
