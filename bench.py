@@ -158,12 +158,32 @@ def reference_ranks() -> int:
     AMG_REF_RANKS overrides."""
     if os.environ.get("AMG_REF_RANKS"):
         return max(1, int(os.environ["AMG_REF_RANKS"]))
+
+    def read(path):
+        try:
+            return Path(path).read_text().split()
+        except OSError:
+            return None
+
     cores = len(os.sched_getaffinity(0))
+    # a CPU quota of this container (cgroup v2, then v1) bounds the cores too
+    q = read("/sys/fs/cgroup/cpu.max")
+    if q and q[0] != "max":
+        cores = min(cores, max(1, int(q[0]) // int(q[1])))
+    q, per = read("/sys/fs/cgroup/cpu/cpu.cfs_quota_us"), read("/sys/fs/cgroup/cpu/cpu.cfs_period_us")
+    if q and per and int(q[0]) > 0:
+        cores = min(cores, max(1, int(q[0]) // int(per[0])))
     try:
         with open("/proc/meminfo") as f:
             avail = next(int(l.split()[1]) * 1024 for l in f if l.startswith("MemAvailable:"))
     except (OSError, StopIteration, ValueError):
         return 1
+    # and so does a memory limit of this container (cgroup v2, then v1)
+    for lim, use in (("/sys/fs/cgroup/memory.max", "/sys/fs/cgroup/memory.current"),
+                     ("/sys/fs/cgroup/memory/memory.limit_in_bytes", "/sys/fs/cgroup/memory/memory.usage_in_bytes")):
+        a, b = read(lim), read(use)
+        if a and b and a[0] != "max" and int(a[0]) < (1 << 60):
+            avail = min(avail, int(a[0]) - int(b[0]))
     by_mem = int((0.5 * avail - 20e9) // 6e9) + 1
     return max(1, min(cores, 8, by_mem))
 
