@@ -52,3 +52,17 @@ def test_two_gloo_ranks_barrier_max_and_replica_seeds():
     seeds = [s for _, _, s, _ in res]
     assert len(set(seeds)) == world
     assert res[1][3] is True
+
+
+def test_reference_rank_count(monkeypatch):
+    """The reference's CPU runs take 1..8 ranks, no more than the usable cores, and
+    AMG_REF_RANKS overrides the choice."""
+    sys.path.insert(0, str(ROOT))
+    import bench
+    monkeypatch.delenv("AMG_REF_RANKS", raising=False)
+    n = bench.reference_ranks()
+    assert 1 <= n <= min(8, len(os.sched_getaffinity(0)))
+    monkeypatch.setenv("AMG_REF_RANKS", "5")
+    assert bench.reference_ranks() == 5
+    monkeypatch.setenv("AMG_REF_RANKS", "0")
+    assert bench.reference_ranks() == 1
