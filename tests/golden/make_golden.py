@@ -63,6 +63,7 @@ ADJOINT = {
 # phi = gaussian_spinor(N, 2, seed + 1); iteration counts from the reference's own output.
 KRYLOV = {
     "krylov32": (32, [[0, 4, 4, 8, 4, 4], [1, 2, 2, 8, 2, 2]], 3.0, -0.1, 31),
+    "krylov64": (64, [[0, 8, 8, 8, 4, 4]], 2.0, -0.05, 43),
 }
 
 SMALL_KEYS_ALWAYS = ("dphi", "ddagphi", "x", "cycle0_rhs")

@@ -1,17 +1,22 @@
-"""The restated comparison solvers against the reference's own runs (tests/golden/krylov32.npz,
-made by tests/golden/make_golden.py from the compiled reference): conjugate_gradient on
+"""The restated comparison solvers against the reference's own runs (tests/golden/krylov32.npz
+and krylov64.npz, made by tests/golden/make_golden.py from the compiled reference): conjugate_gradient on
 D D^dagger (src/conjugate_gradient.cpp:5-65), bi_cgstab (src/bi_cgstab.cpp:5-89) and the
 unpreconditioned FGMRES_fine_level(20, 50) (include/fgmres.h:126-148) give the reference's
 iteration counts exactly and its solutions to 1e-10."""
 import numpy as np
+import pytest
 
 from conftest import load_golden, rel
 from oracle import restatement as R
 
 
-def test_restated_cg_and_bicgstab_match_reference():
+CASES = ["krylov32", "krylov64"]
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_restated_cg_and_bicgstab_match_reference(name):
     from amg_schwingermodel_b200.inputs import gauge_field, gaussian_spinor
-    g = load_golden("krylov32")
+    g = load_golden(name)
     m = g["meta"]
     ns, m0 = m["ns"], m["m0"]
     U = gauge_field(ns, ns, m["beta"], m["seed"])
@@ -24,9 +29,10 @@ def test_restated_cg_and_bicgstab_match_reference():
     assert rel(x, g["bicg_x"]) < 1e-10
 
 
-def test_restated_unpreconditioned_gmres_matches_reference():
+@pytest.mark.parametrize("name", CASES)
+def test_restated_unpreconditioned_gmres_matches_reference(name):
     from amg_schwingermodel_b200.inputs import gauge_field, gaussian_spinor
-    g = load_golden("krylov32")
+    g = load_golden(name)
     m = g["meta"]
     ns, m0 = m["ns"], m["m0"]
     U = gauge_field(ns, ns, m["beta"], m["seed"])
