@@ -209,7 +209,7 @@ def cpu_reference_sample(U, b0, hierarchy, reps: int, ranks: int = 1, timeout: f
     b = ref_runner.binary(NX, NT, len(ROWS) + 1)
     if not b.exists():
         return None, f"{b.name} not built"
-    kw = dict(m0=M0, solve=1, dump_hierarchy=0, dphi_reps=3, outer_iteration_reps=reps, sap_tv_iters=0)
+    kw = dict(m0=M0, solve=1, dump_hierarchy=0, dphi_reps=20, outer_iteration_reps=reps, sap_tv_iters=0)
     if hierarchy is not None:
         kw["hierarchy"] = hierarchy
     out, used = run_reference_job(ranks, gauge=U, rhs=b0, timeout=timeout, **kw)
@@ -239,7 +239,7 @@ def run_reference(args, world, rank):
     reps = args.warmup + args.steps
     t0 = time.time()
     out, ranks = run_reference_job(reference_ranks(), gauge=U, rhs=b0, m0=M0, solve=1, dump_hierarchy=0,
-                                   dphi_reps=3, outer_iteration_reps=reps, sap_tv_iters=0, timeout=3600)
+                                   dphi_reps=20, outer_iteration_reps=reps, sap_tv_iters=0, timeout=3600)
     times = [out[f"info:outer_iteration_seconds_{r}"] for r in range(reps)][args.warmup:]
     it_s = statistics.mean(times)
     iters = args.ref_iterations
