@@ -320,6 +320,16 @@ int main(int argc, char** argv) {
         const int git = fg.fgmres(rhs, x0, xg, false, false);
         dump_spinor("gmres_x", xg);
         info << "gmres_iterations " << git << "\n";
+        // Tests::FGMRES_sap (src/tests.cpp:33-46) with the global SAP object given the gauge
+        // field first through its public SAP_fine_level::set_params (include/sap.h:145-148),
+        // which the reference's own main never calls: FGMRES(20, 50, 1e-10) with one SAP
+        // sweep on SAPV::sap_block_x x sap_block_t blocks as preconditioner
+        sap.set_params(GConf.Conf, m0);
+        FGMRES_SAP fs(N, 2, 20, 50, 1e-10, GConf.Conf, m0);
+        spinor xs(N, c_vector(2, 0));
+        const int sit = fs.fgmres(rhs, x0, xs, false, false);
+        dump_spinor("sap_x", xs);
+        info << "sap_iterations " << sit << "\n";
         std::cout.flush();
         g_manifest.close();
         return 0;

@@ -12,8 +12,9 @@ preconditioner application, and the outer solve (x, iteration count, residual hi
 Large arrays are dropped for the bigger lattices to keep the files small.
 
 The Krylov fixture (KRYLOV) holds the reference's comparison solvers on one source: the
-conjugate_gradient solution of D D^dagger y = phi, the bi_cgstab solution of D x = phi and
-the unpreconditioned FGMRES_fine_level(20, 50) solution, with their iteration counts.
+conjugate_gradient solution of D D^dagger y = phi, the bi_cgstab solution of D x = phi, the
+unpreconditioned FGMRES_fine_level(20, 50) solution and the FGMRES_SAP(20, 50) solution (the
+global SAP object given the gauge field by its set_params), with their iteration counts.
 
 The adjoint fixture (ADJOINT) holds the reference's two solves behind the gradient of
 L = Re(eta^dagger D^{-1} b): x = D^{-1} b and y = D^{-1} gamma5 eta (so lambda = gamma5 y),
@@ -130,8 +131,9 @@ def make_krylov(name: str, cfg) -> dict:
     bi = re.search(r"^Bi-CG-stab for D converged in (\d+) iterations", out["stdout"], re.M)
     meta = dict(ns=ns, nt=ns, rows=rows, beta=beta, m0=m0, seed=seed,
                 cg_iterations=int(cg.group(1)), bicg_iterations=int(bi.group(1)),
-                gmres_iterations=int(out["info:gmres_iterations"]))
-    return {"cg_x": out["cg_x"], "bicg_x": out["bicg_x"], "gmres_x": out["gmres_x"],
+                gmres_iterations=int(out["info:gmres_iterations"]),
+                sap_iterations=int(out["info:sap_iterations"]))
+    return {"cg_x": out["cg_x"], "bicg_x": out["bicg_x"], "gmres_x": out["gmres_x"], "sap_x": out["sap_x"],
             "meta": np.array(json.dumps(meta))}
 
 

@@ -81,7 +81,7 @@ def test_driver_reproduces_reference(name, tmp_path):
     assert int(res["iterations"]) == m["iterations"]
     assert rel(out("x", g["x"]), g["x"]) < 1e-8
     # FGMRES_SAP (include/sap.h:194-225) on the reference's 4 x 4 SAP blocks, against the
-    # restatement (the reference's own main never runs it): within one outer iteration
+    # restatement (itself equal to the reference's own FGMRES_SAP runs): within one outer iteration
     rows4 = [list(r) for r in m["rows"]]
     rows4[0][4] = rows4[0][5] = 4
     x_ref, it_ref = R.AMG(g["gauge"], m["ns"], m["nt"], rows4, R.SolverParams(m0=m["m0"])).solve_sap(g["rhs"])

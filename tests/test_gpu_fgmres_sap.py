@@ -1,9 +1,9 @@
 """The reference's comparison solver FGMRES_SAP (include/sap.h:194-225): the outer FGMRES with
 one fine-level SAP sweep as its preconditioner, selected by amg_set_preconditioner.  The
-reference's main never runs it (its global SAP object is never given a gauge field), so the
-oracle is the restatement built from the pinned SAP_C::SAP and FGMRES pieces
-(oracle/restatement.py AMG.solve_sap).  Lattices with 4 x 4 SAP blocks, the blocking the
-reference's FGMRES_SAP uses (SAPV::sap_block_x/t = 4, include/variables.h:35-36).
+oracle is the restatement (oracle/restatement.py AMG.solve_sap), which gives the reference's
+own FGMRES_SAP runs exactly (tests/golden/krylov*.npz, tests/test_oracle_krylov.py).
+Lattices with 4 x 4 SAP blocks, the blocking the reference's FGMRES_SAP uses
+(SAPV::sap_block_x/t = 4, include/variables.h:35-36).
 Bars: FP64 within one iteration of the restatement (the outer Gram-Schmidt is CGS2 here, MGS
 there, so rounding may move the stopping step), mixed precision at most one more; x within
 1e-8 and FP64 true residual <= 1e-10 for both; switching back to the multigrid

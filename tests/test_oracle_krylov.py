@@ -40,3 +40,21 @@ def test_restated_unpreconditioned_gmres_matches_reference(name):
     x, it = R.gmres_fine(U, phi, np.zeros_like(phi), m0, ns, ns)
     assert it == m["gmres_iterations"], (it, m["gmres_iterations"])
     assert rel(x, g["gmres_x"]) < 1e-10
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_restated_fgmres_sap_matches_reference(name):
+    """FGMRES_SAP (include/sap.h:194-225) as Tests::FGMRES_sap runs it, with the global SAP
+    object given the gauge field by its set_params: the restatement (4 x 4 SAP blocks, the
+    global object's SAPV::sap_block_x/t) takes the reference's iteration count and solution."""
+    from amg_schwingermodel_b200.inputs import gauge_field, gaussian_spinor
+    g = load_golden(name)
+    m = g["meta"]
+    ns, m0 = m["ns"], m["m0"]
+    U = gauge_field(ns, ns, m["beta"], m["seed"])
+    phi = gaussian_spinor(ns * ns, 2, m["seed"] + 1)
+    rows4 = [list(r) for r in m["rows"]]
+    rows4[0][4] = rows4[0][5] = 4
+    x, it = R.AMG(U, ns, ns, rows4, R.SolverParams(m0=m0)).solve_sap(phi)
+    assert it == m["sap_iterations"], (it, m["sap_iterations"])
+    assert rel(x, g["sap_x"]) < 1e-10
