@@ -473,6 +473,7 @@ int main(int argc, char** argv) {
         }
         info << "outer_iteration_seconds " << (now_s() - t1) / reps << "\n";
         info << "setup_seconds " << t_setup << "\n";
+        dump_spinor("sample_z", z);
         g_manifest.close();
         return 0;
     }

@@ -62,3 +62,16 @@ def test_a_lost_rank_ends_the_job_with_an_error(oracle_binary):
     with pytest.raises(RuntimeError, match="exited inside a collective"):
         ref_runner.run(NS, NS, ROWS, U, b, m0=M0, dump_hierarchy=0, ranks=3, drill_exit_rank=2, timeout=120)
     assert time.time() - t0 < 60
+
+
+def test_ranks_started_after_the_reference_setup_give_the_one_rank_cycle(oracle_binary):
+    """The reference arm's mode: the reference's own set-up (with test-vector smoothing),
+    then the ranks, then the timed outer iterations."""
+    U, b = _inputs()
+    z = {}
+    for ranks in (1, 4):
+        out = ref_runner.run(NS, NS, ROWS, U, b, m0=M0, dump_hierarchy=0, outer_iteration_reps=2,
+                             sap_tv_iters=2, ranks=ranks, ranks_after_setup=1)
+        z[ranks] = out["sample_z"]
+        assert out["info:outer_iteration_seconds"] > 0
+    assert np.array_equal(z[4], z[1]) and np.linalg.norm(z[1]) > 0
