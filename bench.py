@@ -13,7 +13,8 @@ scaling); timing is CUDA events on the solver's stream, max over ranks.  Rank 0 
 JSON line.  `--impl reference` times the reference's own CPU code (compiled from its
 sources into oracle/_ref) on the same workload: the reference's set-up with its test-vector
 smoothing skipped, then a bounded sample of outer FGMRES iterations (one K-cycle from the
-fine level plus D_phi each) scaled to the workload's iteration count.
+fine level plus D_phi each) scaled to the workload's iteration count, run in the
+reference's MPI layout on up to 8 host cores (reference_ranks).
 """
 from __future__ import annotations
 
