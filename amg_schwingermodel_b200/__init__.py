@@ -18,7 +18,7 @@ from . import _lib
 from ._lib import AmgError, AmgParams, AmgSolveInfo, check, default_params, lib  # noqa: F401
 
 __all__ = ["AMGContext", "AmgError", "AmgParams", "default_params", "read_parameters", "dirac_apply_raw",
-           "solve_many"]
+           "solve_many", "solve_many_dev"]
 
 
 def _cptr(a: np.ndarray):
@@ -67,6 +67,21 @@ def solve_many(ctxs, bs):
     check(lib().amg_solve_many(n, hs, bp, xp, nrhs, ip), "amg_solve_many")
     return xs, [[dict(iterations=i.iterations, converged=bool(i.converged), rel_residual=i.rel_residual)
                  for i in inf] for inf in infos]
+
+
+def solve_many_dev(ctxs, b_ptrs, x_ptrs, nrhs):
+    """amg_solve_many_dev: as solve_many, on device buffers (one [nrhs_i][N_i][2] complex128
+    source and solution buffer per context, on that context's device).  Returns the infos."""
+    n = len(ctxs)
+    nr = (C.c_int * n)(*[int(r) for r in nrhs])
+    infos = [(AmgSolveInfo * nr[i])() for i in range(n)]
+    hs = (C.c_void_p * n)(*[c._h.value for c in ctxs])
+    bp = (C.c_void_p * n)(*[int(p) for p in b_ptrs])
+    xp = (C.c_void_p * n)(*[int(p) for p in x_ptrs])
+    ip = (C.c_void_p * n)(*[C.cast(i, C.c_void_p).value for i in infos])
+    check(lib().amg_solve_many_dev(n, hs, bp, xp, nr, ip), "amg_solve_many_dev")
+    return [[dict(iterations=i.iterations, converged=bool(i.converged), rel_residual=i.rel_residual) for i in inf]
+            for inf in infos]
 
 
 class AMGContext:

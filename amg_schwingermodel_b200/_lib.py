@@ -92,6 +92,8 @@ SIGNATURES = {
     "amg_solve_dev": (_I, [_P, _P, _P, _I, _P]),
     "amg_solve_many": (_I, [_I, _P, _P, _P, _P, _P]),
     "amg_solve_many_dev": (_I, [_I, _P, _P, _P, _P, _P]),
+    "amg_restrict0_mixed_dev": (_I, [_P, _P, _P, _I]),
+    "amg_prolong0_mixed_dev": (_I, [_P, _P, _P, _I]),
     "amg_residual_history": (_I, [_P, _P, _I, C.POINTER(_I)]),
     "amg_solve_adjoint": (_I, [_P, _P, _P, _I, _P]),
     "amg_solve_adjoint_dev": (_I, [_P, _P, _P, _I, _P]),

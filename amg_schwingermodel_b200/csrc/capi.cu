@@ -1867,6 +1867,34 @@ int amg_prolong(amg_ctx c, int level, const double* in, double* out) {
     return to_host(out, b, (long long)h.n * h.K, c->stream);
 }
 
+// The mixed form's level-0 transfers on device buffers (complex64), the kernels its cycles run
+static int transfer0_mixed(amg_ctx c, int op, const void* in_dev, void* out_dev, int nrhs) {
+    CKR(check_ready(c, 0, true));
+    if (c->p.precision != AMG_PREC_MIXED) return fail(AMG_ERR_STATE, "the context is not in the mixed form");
+    if (c->L < 2) return fail(AMG_ERR_INVALID, "one level: no transfer");
+    if (nrhs < 1) return fail(AMG_ERR_INVALID, "nrhs < 1");
+    if (!in_dev || !out_dev) return fail(AMG_ERR_INVALID, "null device pointer");
+    CKR(select_device(c));
+    CKR(ensure_capacity(c, nrhs));
+    if (op == 0)
+        fine_restrict<float>(c, c->f, static_cast<const float2*>(in_dev), static_cast<float2*>(out_dev), nrhs);
+    else
+        fine_prolong_add<float>(c, c->f, static_cast<const float2*>(in_dev), static_cast<float2*>(out_dev), nrhs);
+    CKL();
+    const int e = fine_error_check(c->stream);
+    if (e < 0) return fail(AMG_ERR_CUDA, "transfer: %s", cudaGetErrorString(cudaGetLastError()));
+    if (e) return fail(AMG_ERR_DEVICE_WAIT, "transfer: a device wait gave up (flag %d)", e);
+    return AMG_OK;
+}
+
+int amg_restrict0_mixed_dev(amg_ctx c, const void* in_dev, void* out_dev, int nrhs) {
+    return transfer0_mixed(c, 0, in_dev, out_dev, nrhs);
+}
+
+int amg_prolong0_mixed_dev(amg_ctx c, const void* in_dev, void* out_dev, int nrhs) {
+    return transfer0_mixed(c, 1, in_dev, out_dev, nrhs);
+}
+
 int amg_sap(amg_ctx c, int level, const double* v, double* x, int nu) {
     CKR(check_ready(c, level, level > 0));
     if (level >= c->L - 1) return fail(AMG_ERR_INVALID, "no SAP on the coarsest level");

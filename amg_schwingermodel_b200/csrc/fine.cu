@@ -3,6 +3,7 @@
 // BLAS-1 kernels of the outer FGMRES.
 //
 // Layout: psi[rhs][n][spin] complex (double2 or float2), n = x*Nt + t; U[n][mu].
+#include <atomic>
 #include <cstdlib>
 #include <cstring>
 #include <type_traits>
@@ -13,6 +14,7 @@
 #include "sap_lean.cuh"
 #include "sap_f32.cuh"
 #include "sap_ca.cuh"
+#include "tc_transfer.cuh"
 
 namespace amgb {
 
@@ -795,26 +797,115 @@ int sap0_warp_enabled() {
 }
 void set_sap0_warp(int on) { g_sap0_warp = on; }
 
+// Multiprocessors of the current device, looked up once per device.
+int sm_count() {
+    static std::atomic<int> cache[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+    int v = cache[dev].load(std::memory_order_relaxed);
+    if (v <= 0) {
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
+        cache[dev].store(v, std::memory_order_relaxed);
+    }
+    return v;
+}
+
+// Largest dynamic shared memory one block may opt into on the current device, looked up once
+// per device.
+int smem_optin_bytes() {
+    static std::atomic<int> cache[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 48 * 1024;
+    int v = cache[dev].load(std::memory_order_relaxed);
+    if (v <= 0) {
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess || v <= 0)
+            v = 48 * 1024;
+        cache[dev].store(v, std::memory_order_relaxed);
+    }
+    return v;
+}
+
+// Returns the status of its own attribute call and launches (cudaGetLastError is not read, so
+// an error pending from earlier work on this thread is neither reported nor cleared here).
+// The mixed form's level-0 transfers on the tensor cores (tc_transfer.cuh) unless
+// AMG_TC_TRANSFER=0 (read once per process): then the CUDA-core kernels run.
+int tc_transfer_enabled() {
+    static int on = -1;
+    if (on < 0) {
+        const char* e = getenv("AMG_TC_TRANSFER");
+        on = (e && !strcmp(e, "0")) ? 0 : 1;
+    }
+    return on;
+}
+
+// Tensor-core restriction for BF16 test vectors and FP32 sources; returns false (nothing
+// launched) for shapes it does not take.
 template <typename T, typename TW>
-void launch_restrict0(const TW* W, const cx<T>* v, cx<T>* out, cx<T>* partial, int nx, int nt, int bx, int bt,
-                      int ntest, int nrhs, int nchunk, cudaStream_t s) {
+bool launch_restrict0_tc(const TW* W, const cx<T>* v, cx<T>* partial, int nx, int nt, int bx, int bt, int ntest,
+                         int nrhs, int nchunk, cudaStream_t s, cudaError_t* err) {
+    if constexpr (!std::is_same<T, float>::value || !std::is_same<TW, __nv_bfloat162>::value) {
+        return false;
+    } else {
+        const int xe = nx / bx, te = nt / bt, nblk = bx * bt;
+        if (!tc_transfer_enabled() || te % kRtcSites || ntest < 1 || ntest > 32 || nrhs < 1 || nrhs > 256 ||
+            nblk > 65535 || nchunk < 1)
+            return false;
+        const int NP = (nrhs + 15) / 16 * 16;
+        dim3 grid(nchunk, nblk);
+        if (ntest <= 16) {
+            const int bytes = rtc_smem_bytes(64, NP);
+            if (bytes > smem_optin_bytes()) return false;
+            *err = cudaFuncSetAttribute(k_restrict0_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+            if (*err != cudaSuccess) return true;
+            k_restrict0_tc<64><<<grid, 128, bytes, s>>>(W, v, partial, nx, nt, bt, xe, te, nchunk, ntest, nrhs, NP);
+        } else {
+            const int bytes = rtc_smem_bytes(128, NP);
+            if (bytes > smem_optin_bytes()) return false;
+            *err = cudaFuncSetAttribute(k_restrict0_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+            if (*err != cudaSuccess) return true;
+            k_restrict0_tc<128><<<grid, 128, bytes, s>>>(W, v, partial, nx, nt, bt, xe, te, nchunk, ntest, nrhs, NP);
+        }
+        *err = cudaPeekAtLastError();
+        return true;
+    }
+}
+
+template <typename T, typename TW>
+cudaError_t launch_restrict0(const TW* W, const cx<T>* v, cx<T>* out, cx<T>* partial, int nx, int nt, int bx,
+                             int bt, int ntest, int nrhs, int nchunk, cudaStream_t s) {
     count_launch(2);
     const int xe = nx / bx, te = nt / bt, nblk = bx * bt;
     dim3 grid(nchunk, nblk);
-    if (rt_out_tiles(ntest, nrhs) <= 256) {
-        const int bytes = rt_smem_bytes<T>(ntest, nrhs);
-        if (bytes > 48 * 1024) cudaFuncSetAttribute(k_restrict0t<T, TW>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-        k_restrict0t<T, TW><<<grid, 256, bytes, s>>>(W, v, partial, nx, nt, bt, xe, te, nchunk, ntest, nrhs);
-        dim3 g2((nblk * 2 * ntest + 127) / 128, nrhs);
-        k_restrict0_sum<T><<<g2, 128, 0, s>>>(partial, out, nblk, nchunk, 2 * ntest);
-        return;
-    }
-    const int thr = nrhs >= 8 ? 256 : 32 * nrhs;
-    if (ntest <= 8) k_restrict0m<T, TW, 8><<<grid, thr, 0, s>>>(W, v, partial, nx, nt, bt, xe, te, nchunk, ntest, nrhs);
-    else if (ntest <= 16) k_restrict0m<T, TW, 16><<<grid, thr, 0, s>>>(W, v, partial, nx, nt, bt, xe, te, nchunk, ntest, nrhs);
-    else k_restrict0m<T, TW, 32><<<grid, thr, 0, s>>>(W, v, partial, nx, nt, bt, xe, te, nchunk, ntest, nrhs);
     dim3 g2((nblk * 2 * ntest + 127) / 128, nrhs);
+    cudaError_t tce = cudaSuccess;
+    if (launch_restrict0_tc<T, TW>(W, v, partial, nx, nt, bx, bt, ntest, nrhs, nchunk, s, &tce)) {
+        if (tce != cudaSuccess) return tce;
+        k_restrict0_sum<T><<<g2, 128, 0, s>>>(partial, out, nblk, nchunk, 2 * ntest);
+        return cudaPeekAtLastError();
+    }
+    // the tiled kernel when its output tiles fit one CTA and its staging fits the device's
+    // shared memory (few test vectors with many sources need more than a block may hold)
+    const int bytes = rt_smem_bytes<T>(ntest, nrhs);
+    if (rt_out_tiles(ntest, nrhs) <= 256 && bytes <= smem_optin_bytes()) {
+        if (bytes > 48 * 1024) {
+            const cudaError_t e =
+                cudaFuncSetAttribute(k_restrict0t<T, TW>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+            if (e != cudaSuccess) return e;
+        }
+        k_restrict0t<T, TW><<<grid, 256, bytes, s>>>(W, v, partial, nx, nt, bt, xe, te, nchunk, ntest, nrhs);
+    } else {
+        const int thr = nrhs >= 8 ? 256 : 32 * nrhs;
+        if (ntest <= 8)
+            k_restrict0m<T, TW, 8><<<grid, thr, 0, s>>>(W, v, partial, nx, nt, bt, xe, te, nchunk, ntest, nrhs);
+        else if (ntest <= 16)
+            k_restrict0m<T, TW, 16><<<grid, thr, 0, s>>>(W, v, partial, nx, nt, bt, xe, te, nchunk, ntest, nrhs);
+        else
+            k_restrict0m<T, TW, 32><<<grid, thr, 0, s>>>(W, v, partial, nx, nt, bt, xe, te, nchunk, ntest, nrhs);
+    }
+    cudaError_t e = cudaPeekAtLastError();
+    if (e != cudaSuccess) return e;
     k_restrict0_sum<T><<<g2, 128, 0, s>>>(partial, out, nblk, nchunk, 2 * ntest);
+    return cudaPeekAtLastError();
 }
 
 template <typename T, typename TW>
@@ -822,6 +913,20 @@ void launch_prolong0_add(const TW* W, const cx<T>* vc, cx<T>* psi, int nx, int n
                          int nrhs, cudaStream_t s) {
     count_launch(1);
     const int xe = nx / bx, te = nt / bt;
+    if constexpr (std::is_same<T, float>::value && std::is_same<TW, __nv_bfloat162>::value) {
+        // tensor cores: 32-site tiles along t, several CTAs per aggregation block
+        const int nblk = bx * bt, NP = (nrhs + 15) / 16 * 16;
+        const int bytes = ptc_smem_bytes(ntest, NP);
+        if (tc_transfer_enabled() && te % kPtcSites == 0 && ntest >= 1 && ntest <= 32 && nrhs >= 1 && nrhs <= 256 &&
+            nblk <= 65535 && bytes <= smem_optin_bytes() &&
+            cudaFuncSetAttribute(k_prolong0_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) == cudaSuccess) {
+            const int tiles = xe * (te / kPtcSites);
+            const int nsplit = std::max(1, std::min(tiles, (4 * sm_count() + nblk - 1) / nblk));
+            dim3 grid(nsplit, nblk);
+            k_prolong0_tc<<<grid, 128, bytes, s>>>(W, vc, psi, nx, nt, bt, xe, te, ntest, nblk, nrhs, NP, nsplit);
+            return;
+        }
+    }
     const int grid = (nx * nt + 255) / 256;
     if (ntest <= 8) k_prolong0_add<T, TW, 8><<<grid, 256, 0, s>>>(W, vc, psi, nx, nt, bt, xe, te, ntest, bx * bt, nrhs);
     else if (ntest <= 16) k_prolong0_add<T, TW, 16><<<grid, 256, 0, s>>>(W, vc, psi, nx, nt, bt, xe, te, ntest, bx * bt, nrhs);
@@ -1152,11 +1257,11 @@ void launch_force(const double2* U, const double2* lam, const double2* x, double
                                         const cx<T>*, long long);
 INST(double)
 INST(float)
-template void launch_restrict0<double, double2>(const double2*, const cx<double>*, cx<double>*, cx<double>*, int,
+template cudaError_t launch_restrict0<double, double2>(const double2*, const cx<double>*, cx<double>*, cx<double>*, int,
                                                  int, int, int, int, int, int, cudaStream_t);
-template void launch_restrict0<float, float2>(const float2*, const cx<float>*, cx<float>*, cx<float>*, int, int,
+template cudaError_t launch_restrict0<float, float2>(const float2*, const cx<float>*, cx<float>*, cx<float>*, int, int,
                                                int, int, int, int, int, cudaStream_t);
-template void launch_restrict0<float, __nv_bfloat162>(const __nv_bfloat162*, const cx<float>*, cx<float>*,
+template cudaError_t launch_restrict0<float, __nv_bfloat162>(const __nv_bfloat162*, const cx<float>*, cx<float>*,
                                                        cx<float>*, int, int, int, int, int, int, int, cudaStream_t);
 template void launch_prolong0_add<double, double2>(const double2*, const cx<double>*, cx<double>*, int, int, int,
                                                     int, int, int, cudaStream_t);

@@ -31,8 +31,9 @@ void launch_norm2(const cx<T>* v, long long len, long long stride, int nrhs, dou
                   cudaStream_t s);
 int residual_partials(int nx, int nt);
 template <typename T, typename TW>
-void launch_restrict0(const TW* W, const cx<T>* v, cx<T>* out, cx<T>* partial, int nx, int nt, int bx, int bt,
-                      int ntest, int nrhs, int nchunk, cudaStream_t s);
+cudaError_t launch_restrict0(const TW* W, const cx<T>* v, cx<T>* out, cx<T>* partial, int nx, int nt, int bx,
+                             int bt, int ntest, int nrhs, int nchunk, cudaStream_t s);
+int smem_optin_bytes();
 template <typename T, typename TW>
 void launch_prolong0_add(const TW* W, const cx<T>* vc, cx<T>* psi, int nx, int nt, int bx, int bt, int ntest,
                          int nrhs, cudaStream_t s);

@@ -9,8 +9,10 @@
 // extra device memory the restriction needs is the per-chunk partial sums, and here those live
 // in g_restrict_scratch, a file-scope __device__ array that exists on every GPU that loads the
 // library, from module load until the process exits.
+#include <climits>
 #include <cstdint>
 #include <mutex>
+#include <string>
 
 #include "kernels.h"
 #include "../../include/schwinger_amg.h"
@@ -36,7 +38,9 @@ void* g_scratch_addr[kMaxDevices] = {};
 
 // Device address of g_restrict_scratch on the current device.  In host code the array's name
 // refers to a host-side shadow, not to device memory, so the address is looked up once per
-// device with that device current and kept.
+// device with that device current and kept for the life of the process.  A cudaDeviceReset
+// unloads the module and makes the kept address stale: a process that resets a device must
+// not call amg_restrict_raw_noalloc on it afterwards.
 int scratch_address(void** out) {
     int dev = -1;
     cudaError_t e = cudaGetDevice(&dev);
@@ -81,6 +85,7 @@ extern "C" AMG_API int amg_restrict_raw_noalloc(const void* W_dev, const void* v
     if (!aligned16(W_dev) || !aligned16(v_dev) || !aligned16(out_dev))
         return invalid("device pointers must be 16-byte aligned (complex128 arrays)");
     if (nx < 2 || nt < 2) return invalid("lattice must be at least 2x2");
+    if ((long long)nx * nt * 2 > INT_MAX) return invalid("nx * nt * 2 must fit in an int");
     if (bx < 1 || bt < 1 || nx % bx || nt % bt) return invalid("lattice not divisible into bx x bt aggregates");
     if (ntest < 1 || ntest > 32) return invalid("ntest must be in [1, 32]");
     if (nrhs < 1 || nrhs > 65535) return invalid("nrhs must be in [1, 65535]");
@@ -95,14 +100,22 @@ extern "C" AMG_API int amg_restrict_raw_noalloc(const void* W_dev, const void* v
     long long nchunk = std::max(1ll, std::min(std::max(1ll, spb / 128), (1184 + nblk - 1) / nblk));
     nchunk = std::min(nchunk, kScratchElems / per_chunk);
 
+    // An error left pending by the caller's earlier work on this thread would be read back as
+    // this call's launch status: report it as such, without clearing it, and launch nothing.
+    cudaError_t e = cudaPeekAtLastError();
+    if (e != cudaSuccess) {
+        set_last_error((std::string("a CUDA error from earlier work is pending on this thread: ") +
+                        cudaGetErrorString(e)).c_str(), __FILE__, __LINE__);
+        return AMG_ERR_CUDA;
+    }
     void* scratch = nullptr;
     const int rc = scratch_address(&scratch);
     if (rc != AMG_OK) return rc;
-    launch_restrict0<double, double2>(static_cast<const double2*>(W_dev), static_cast<const double2*>(v_dev),
-                                      static_cast<double2*>(out_dev), static_cast<double2*>(scratch), nx, nt, bx, bt,
-                                      ntest, nrhs, (int)nchunk, static_cast<cudaStream_t>(stream));
-    const cudaError_t e = cudaGetLastError();
+    e = launch_restrict0<double, double2>(static_cast<const double2*>(W_dev), static_cast<const double2*>(v_dev),
+                                          static_cast<double2*>(out_dev), static_cast<double2*>(scratch), nx, nt, bx,
+                                          bt, ntest, nrhs, (int)nchunk, static_cast<cudaStream_t>(stream));
     if (e != cudaSuccess) {
+        cudaGetLastError();  // this call's own launch error: cleared once reported
         set_last_error(cudaGetErrorString(e), __FILE__, __LINE__);
         return AMG_ERR_CUDA;
     }

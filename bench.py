@@ -4,17 +4,20 @@ residual <= 1e-10 (4 levels, Nv = 16, beta = 4, m0 = -0.05), mixed precision wit
 sources against the plain FP64 drop-in, plus the fine D-apply bandwidth.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--rhs R] [--precision mixed|f64]
+                    [--rhs R] [--precision mixed|f64] [--no-cpu] [--no-extras]
 
 One step = one batched solve of R seeded complex-Gaussian sources on one seeded gauge
 field per GPU (inputs resident in HBM; the working set of a step is far above the 126 MB
 L2).  With N GPUs every rank solves its own gauge field and sources (replicas, weak
 scaling); timing is CUDA events on the solver's stream, max over ranks.  Rank 0 prints one
-JSON line.  `--impl reference` times the reference's own CPU code (compiled from its
-sources into oracle/_ref) on the same workload: the reference's set-up with its test-vector
-smoothing skipped, then a bounded sample of outer FGMRES iterations (one K-cycle from the
-fine level plus D_phi each) scaled to the workload's iteration count, run in the
-reference's MPI layout on up to 8 host cores (reference_ranks).
+JSON line.  At N = 1 the line also carries the FP64 forms (one source and the same batch),
+the reference-style blocking at 1024^2, the 256^2 FP64-vs-mixed comparison, and the uneven
+batch of 24 configurations (128^2 / 256^2 / 512^2) x 32 sources.
+
+`--impl reference` times the reference's own CPU code (compiled from its unmodified sources
+into oracle/_ref) on the same workload: its own complete set-up, then complete FGMRES_AMG
+solves (one untimed, then up to K timed within a time budget), run in the reference's MPI
+layout on up to 8 host cores; `steps` states how many solves were timed.
 """
 from __future__ import annotations
 
@@ -35,14 +38,34 @@ sys.path.insert(0, str(ROOT))
 
 NX = NT = 1024
 ROWS = [[0, 8, 8, 16, 32, 32], [1, 4, 4, 16, 4, 4], [2, 2, 2, 16, 2, 2]]
-# DRAM bytes (read + write) of one fine SAP launch per (block, source) it solves, from an ncu
-# capture of this workload at 2 sources (42.02 MB read + 0.37 MB written for 512 blocks x 2
-# sources); the traffic grows with the blocks x sources a launch solves.
-SAP_DRAM_BYTES_PER_BLOCK_SOURCE = 42.391808e6 / 1024
+# the reference-style rows at 1024^2: 4x4 SAP blocks of 256x256 sites
+REF_ROWS = [[0, 8, 8, 16, 4, 4], [1, 4, 4, 16, 4, 4], [2, 2, 2, 16, 2, 2]]
 BETA, M0, TOL = 4.0, -0.05, 1e-10
 METRIC = "1024^2 solves/s at FP64 resid <=1e-10: mixed+batched vs FP64 GPU; D-apply GB/s"
 UNIT = "solves/s"
 WORKLOAD = "schwinger_wilson_1024x1024_L4_Nv16_beta4_m0-0.05"
+# 256x256, 3 levels, aggregation 8x8 then 4x4 blocks, Nv = 12, 4x4 SAP blocks, beta = 3
+C2_NS, C2_ROWS, C2_BETA, C2_SEED = 256, [[0, 8, 8, 12, 4, 4], [1, 4, 4, 12, 4, 4]], 3.0, 51
+# the uneven batch: 8 configurations each at 128^2, 256^2 and 512^2 (beta cycling through 2, 3,
+# 4), 32 sources each, 32x32-site SAP blocks, aggregation 8x8 then 4x4 blocks, Nv = 12
+BATCH_ROWS = {128: [[0, 8, 8, 12, 4, 4], [1, 4, 4, 12, 4, 4]],
+              256: [[0, 8, 8, 12, 8, 8], [1, 4, 4, 12, 4, 4]],
+              512: [[0, 8, 8, 12, 16, 16], [1, 4, 4, 12, 4, 4]]}
+BATCH_PER_SIZE, BATCH_RHS = 8, 32
+
+# Algorithmic FP32 flops of one fine SAP block solve, per site: GMRES(5) restarted 5 times
+# from x0 = b (include/sap.h:27-47; the 1e-3 tolerance is never met on these blocks, so all
+# 25 Arnoldi steps run).  With F_D = 60 flops per site for the block operator (the fine D
+# apply's count), 16 per site for an axpy or a dot over the two spin components, 8 for a
+# norm and 4 for a real scaling: the initial residual b - D_B b with its norm, 72; per
+# restart cycle the Arnoldi steps j = 0..4, sum_j (60 + 32 (j + 1) + 8 + 4) = 840, the update
+# x += sum_j y_j V_j, 80, and the residual with its norm, 72.  72 + 5 * 992 = 5032.
+SAP_FLOPS_PER_SITE = 5032
+# DRAM bytes (read + write) of one fine SAP launch per (block, source) it solves, from the ncu
+# capture of this workload's SAP kernel at 32 sources (profiles/k_sap0_f32_1024x1024_r32.md:
+# 16384 block-sources per launch).
+SAP_DRAM_BYTES_PER_BLOCK_SOURCE = 678268928.0 / 16384
+FP32_LANES_PER_SM = 128
 
 
 def peaks():
@@ -151,82 +174,80 @@ def hierarchy_for_reference(ctx) -> dict:
     return {"tv": tv, "links": links}
 
 
-def reference_ranks() -> int:
-    """Ranks for the reference's CPU runs (its MPI layout as processes on this host, the SAP
-    block solves split among them): the usable cores, at most 8, and no more than half the
-    available memory holds -- a 1024x1024 4-level run of the reference takes about 20 GB
-    for its first rank and about 6 GB for each further rank started after the set-up.
-    AMG_REF_RANKS overrides."""
-    if os.environ.get("AMG_REF_RANKS"):
-        return max(1, int(os.environ["AMG_REF_RANKS"]))
+def _read(path):
+    try:
+        return Path(path).read_text().split()
+    except OSError:
+        return None
 
-    def read(path):
-        try:
-            return Path(path).read_text().split()
-        except OSError:
-            return None
 
+def host_cores() -> int:
+    """Usable host cores: the affinity mask, bounded by a cgroup CPU quota (v2, then v1)."""
     cores = len(os.sched_getaffinity(0))
-    # a CPU quota of this container (cgroup v2, then v1) bounds the cores too
-    q = read("/sys/fs/cgroup/cpu.max")
+    q = _read("/sys/fs/cgroup/cpu.max")
     if q and q[0] != "max":
         cores = min(cores, max(1, int(q[0]) // int(q[1])))
-    q, per = read("/sys/fs/cgroup/cpu/cpu.cfs_quota_us"), read("/sys/fs/cgroup/cpu/cpu.cfs_period_us")
+    q, per = _read("/sys/fs/cgroup/cpu/cpu.cfs_quota_us"), _read("/sys/fs/cgroup/cpu/cpu.cfs_period_us")
     if q and per and int(q[0]) > 0:
         cores = min(cores, max(1, int(q[0]) // int(per[0])))
+    return cores
+
+
+def host_available_bytes() -> int:
+    """MemAvailable, bounded by a cgroup memory limit (v2, then v1); 0 if unknown."""
     try:
         with open("/proc/meminfo") as f:
             avail = next(int(l.split()[1]) * 1024 for l in f if l.startswith("MemAvailable:"))
     except (OSError, StopIteration, ValueError):
-        return 1
-    # and so does a memory limit of this container (cgroup v2, then v1)
+        return 0
     for lim, use in (("/sys/fs/cgroup/memory.max", "/sys/fs/cgroup/memory.current"),
                      ("/sys/fs/cgroup/memory/memory.limit_in_bytes", "/sys/fs/cgroup/memory/memory.usage_in_bytes")):
-        a, b = read(lim), read(use)
+        a, b = _read(lim), _read(use)
         if a and b and a[0] != "max" and int(a[0]) < (1 << 60):
             avail = min(avail, int(a[0]) - int(b[0]))
-    by_mem = int((0.5 * avail - 20e9) // 6e9) + 1
-    return max(1, min(cores, 8, by_mem))
+    return avail
 
 
-def run_reference_job(ranks: int, **kw):
-    """ref_runner.run on the bench workload with `ranks` ranks started after the set-up; if
-    that run fails (a rank lost, e.g. to memory pressure) it is repeated with one rank.
-    Returns (outputs, ranks used)."""
+def reference_layout() -> tuple[int, bool]:
+    """Ranks for the reference's CPU runs (its MPI layout as processes on this host, the SAP
+    block solves split among them) and whether they start before the set-up.  A 1024x1024
+    4-level run of the reference holds about 13 GB per rank when every rank runs the set-up;
+    ranks started after the set-up share its pages, about 20 GB for the first and 6 GB for
+    each further one.  Up to 8 ranks (the usable cores), within half the available memory;
+    the ranks start before the set-up (which it then splits too) when all of them fit that
+    way.  AMG_REF_RANKS overrides the count (ranks then start after the set-up)."""
+    if os.environ.get("AMG_REF_RANKS"):
+        return max(1, int(os.environ["AMG_REF_RANKS"])), False
+    cores = min(host_cores(), 8)
+    avail = host_available_bytes()
+    if avail <= 0:
+        return 1, False
+    early = int((0.5 * avail) // 13e9)
+    if early >= cores:
+        return cores, True
+    late = int((0.5 * avail - 20e9) // 6e9) + 1
+    return max(1, min(cores, late)), False
+
+
+def run_reference_job(ranks: int, early: bool, rows=ROWS, **kw):
+    """ref_runner.run on the bench lattice with `ranks` ranks (started before the set-up if
+    `early`, else after it); if that run fails (a rank lost, e.g. to memory pressure) it is
+    repeated with one rank.  Returns (outputs, ranks used)."""
     from oracle import ref_runner
     if ranks > 1:
         try:
-            return ref_runner.run(NX, NT, ROWS, ranks=ranks, ranks_after_setup=1, **kw), ranks
+            return ref_runner.run(NX, NT, rows, ranks=ranks, ranks_after_setup=0 if early else 1, **kw), ranks
         except RuntimeError as e:
             print(f"reference with {ranks} ranks failed ({str(e)[:200]}); one rank", file=sys.stderr)
-    return ref_runner.run(NX, NT, ROWS, **kw), 1
-
-
-def cpu_reference_sample(U, b0, hierarchy, reps: int, ranks: int = 1, timeout: float = 900):
-    """Times outer FGMRES iterations of the reference's own code (oracle/_ref) on this workload:
-    one preconditioner application (K-cycle from the fine level) plus D_phi per repetition,
-    on `ranks` ranks."""
-    from oracle import ref_runner
-    b = ref_runner.binary(NX, NT, len(ROWS) + 1)
-    if not b.exists():
-        return None, f"{b.name} not built"
-    kw = dict(m0=M0, solve=1, dump_hierarchy=0, dphi_reps=20, outer_iteration_reps=reps, sap_tv_iters=0)
-    if hierarchy is not None:
-        kw["hierarchy"] = hierarchy
-    out, used = run_reference_job(ranks, gauge=U, rhs=b0, timeout=timeout, **kw)
-    if hierarchy is not None:
-        times = [out[f"info:outer_iteration_seconds_{r}"] for r in range(reps)]
-    else:
-        times = [out["info:outer_iteration_seconds"]]
-    return dict(times=times, dphi_s=out.get("info:dphi_seconds_per_apply"),
-                setup_s=out.get("info:setup_seconds"), ranks=used), None
+    return ref_runner.run(NX, NT, rows, **kw), 1
 
 
 def run_reference(args, world, rank):
-    """The reference's own CPU code on this workload: its set-up (test-vector smoothing
-    skipped to bound the run), then warmup + steps outer FGMRES iterations (K-cycle from the
-    fine level + D_phi), each a bounded sample of one solve; solves/s scales the per-iteration
-    time by the outer iteration count of the reference algorithm on this workload."""
+    """The reference's own CPU code on this workload: its complete set-up (test-vector
+    smoothing included, as FGMRES_AMG's constructor runs it), then complete FGMRES_AMG solves
+    from x0 = 0: one untimed, then up to `steps` timed, stopping early once another solve
+    would exceed the time budget (AMG_REF_SOLVE_BUDGET_S, default 240 s).  solves/s = timed
+    solves / their summed time."""
     if rank != 0:
         return
     from amg_schwingermodel_b200.inputs import gauge_field, gaussian_spinor
@@ -237,27 +258,169 @@ def run_reference(args, world, rank):
     gseed, bseed = replica_seeds(0)
     U = gauge_field(NX, NT, BETA, gseed)
     b0 = gaussian_spinor(NX * NT, 2, bseed)
-    reps = args.warmup + args.steps
+    budget = float(os.environ.get("AMG_REF_SOLVE_BUDGET_S", "240"))
+    ranks, early = reference_layout()
     t0 = time.time()
-    out, ranks = run_reference_job(reference_ranks(), gauge=U, rhs=b0, m0=M0, solve=1, dump_hierarchy=0,
-                                   dphi_reps=20, outer_iteration_reps=reps, sap_tv_iters=0, timeout=3600)
-    times = [out[f"info:outer_iteration_seconds_{r}"] for r in range(reps)][args.warmup:]
-    it_s = statistics.mean(times)
-    iters = args.ref_iterations
-    value = 1.0 / (iters * it_s)
-    sample = (f"reference outer FGMRES iterations (K-cycle from the fine level + D_phi) at {NX}x{NT}, 4 levels, "
-              f"after its own set-up with test-vector smoothing skipped; mean of {len(times)} timed of {reps}: "
-              f"{it_s:.2f} s/iteration; solves/s = 1/({iters} iterations x that); {ranks} rank(s) of its MPI "
-              f"layout, one core each (SAP blocks split among them)")
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * iters * it_s, "higher_is_better": True,
+    out, ranks = run_reference_job(ranks, early, gauge=U, rhs=b0, m0=M0, solve=1, dump_hierarchy=0, dphi_reps=20,
+                                   solve_reps=1 + args.steps, solve_budget_seconds=budget, timeout=3 * 3600)
+    done = int(out["info:solves_done"])
+    times = [out[f"info:solve_seconds_{r}"] for r in range(done)]
+    iters = [int(out[f"info:iterations_{r}"]) for r in range(done)]
+    warm = 1 if done > 1 else 0
+    timed = times[warm:]
+    value = len(timed) / sum(timed)
+    sample = (f"complete reference FGMRES_AMG solves (x0 = 0 to FP64 relative residual 1e-10) at {NX}x{NT}, 4 levels, "
+              f"after its own complete set-up ({out['info:setup_seconds']:.1f} s); {warm} untimed + {len(timed)} timed "
+              f"within a {budget:.0f} s budget: {statistics.mean(timed):.2f} s per solve, {iters[-1]} iterations; "
+              f"{ranks} rank(s) of its MPI layout, one core each (SAP blocks split among them"
+              f"{', set-up included' if early and ranks > 1 else '; ranks started after the set-up'})")
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": len(timed),
+            "warmup": warm, "ms_per_step": 1e3 * statistics.mean(timed), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": {"workload": WORKLOAD, "lattice": [NX, NT], "levels": 4, "rows": ROWS, "nrhs": 1},
+            "config": {"workload": WORKLOAD, "lattice": [NX, NT], "levels": 4, "rows": ROWS, "nrhs": 1,
+                       "steps_requested": args.steps, "solve_budget_s": budget},
+            "iterations": iters, "true_rel_residual": out.get("info:true_rel_residual"),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": ranks, "kind": "reference", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "dphi_s_per_apply": out.get("info:dphi_seconds_per_apply"),
             "ref_setup_s": out.get("info:setup_seconds"), "wall_s": time.time() - t0}
     print(json.dumps(line))
+
+
+def cpu_reference_solve(U, b0, hierarchy, timeout: float = 900) -> dict:
+    """Times complete FGMRES_AMG solves of the reference's own code (oracle/_ref) on this
+    workload, on the hierarchy the GPU FP64 set-up built (loaded into the reference's
+    AlgebraicMG, its own set-up skipped): one solve, a second one if both fit 30 s."""
+    from oracle import ref_runner
+    b = ref_runner.binary(NX, NT, len(ROWS) + 1)
+    if not b.exists():
+        return {"error": f"{b.name} not built"}
+    ranks, _ = reference_layout()
+    out, used = run_reference_job(ranks, False, gauge=U, rhs=b0, m0=M0, solve=1, dump_hierarchy=0, dphi_reps=20,
+                                  hierarchy=hierarchy, solve_reps=2, solve_budget_seconds=30, timeout=timeout)
+    done = int(out["info:solves_done"])
+    return dict(t=out[f"info:solve_seconds_{done - 1}"], iterations=int(out["info:iterations"]),
+                residual=out["info:true_rel_residual"], dphi_s=out.get("info:dphi_seconds_per_apply"), ranks=used,
+                solves=done)
+
+
+def timed_solves(ctx, b_ptr, x_ptr, nrhs, steps, warmup):
+    """warmup + steps batched solves on device buffers; returns (ms per step, last infos)."""
+    import torch
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    infos = None
+    for _ in range(warmup):
+        infos = ctx.solve_dev(b_ptr, x_ptr, nrhs)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        infos = ctx.solve_dev(b_ptr, x_ptr, nrhs)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps, infos
+
+
+def line_config2(local):
+    """256x256, 3 levels (aggregation 8x8 then 4x4 blocks, Nv = 12, beta = 3, m0 = -0.05), one
+    source: the FP64 drop-in against the mixed form, iterations beside the reference's."""
+    import torch
+
+    from amg_schwingermodel_b200 import AMGContext
+    from amg_schwingermodel_b200.inputs import gauge_field, gaussian_spinor
+    N = C2_NS * C2_NS
+    U = gauge_field(C2_NS, C2_NS, C2_BETA, C2_SEED)
+    b = torch.from_numpy(gaussian_spinor(N, 2, C2_SEED + 1000).view(np.float64).copy()).to(f"cuda:{local}")
+    res, xs = {}, {}
+    for name, prec in (("f64", 0), ("mixed", 1)):
+        with AMGContext(C2_NS, C2_NS, C2_ROWS, M0, precision=prec, max_rhs=1, device=local) as ctx:
+            ctx.set_gauge(U)
+            setup_ms = ctx.setup()
+            x = torch.empty_like(b)
+            ms, infos = timed_solves(ctx, b.data_ptr(), x.data_ptr(), 1, 10, 3)
+            xs[name] = x.cpu().numpy()
+            res[name] = {"value": 1e3 / ms, "unit": UNIT, "iterations": infos[0]["iterations"],
+                         "rel_residual": infos[0]["rel_residual"], "setup_s": setup_ms / 1e3}
+    res["mixed"]["err_vs_fp64"] = float(np.linalg.norm(xs["mixed"] - xs["f64"]) / np.linalg.norm(xs["f64"]))
+    fx = ROOT / "tests" / "golden" / "solve256_l3.npz"
+    ref_it = json.loads(str(np.load(fx)["meta"]))["iterations"] if fx.exists() else None
+    return {"workload": "schwinger_wilson_256x256_L3_Nv12_beta3_m0-0.05", "rows": C2_ROWS, "nrhs": 1,
+            "reference_iterations": ref_it, **res, "speedup_mixed_vs_f64": res["mixed"]["value"] / res["f64"]["value"]}
+
+
+def line_reference_rows(local, R):
+    """1024x1024 with the reference-style rows (SAP blocks of 256x256 sites, solved by the
+    any-shape block kernel), mixed precision, R sources: iterations and solves/s."""
+    import torch
+
+    from amg_schwingermodel_b200 import AMGContext
+    from amg_schwingermodel_b200.inputs import gauge_field
+    N = NX * NT
+    U = gauge_field(NX, NT, BETA, replica_seeds(0)[0])
+    g = torch.Generator(device=f"cuda:{local}").manual_seed(7)
+    b = torch.randn(R, N, 2, 2, dtype=torch.float64, device=f"cuda:{local}", generator=g)
+    x = torch.empty_like(b)
+    with AMGContext(NX, NT, REF_ROWS, M0, precision=1, max_rhs=R, device=local) as ctx:
+        ctx.set_gauge(U)
+        setup_ms = ctx.setup()
+        ms, infos = timed_solves(ctx, b.data_ptr(), x.data_ptr(), R, 1, 1)
+        tuned = ctx.autotune_info()
+    fx = ROOT / "tests" / "golden" / "solve1024_l4_refrows.npz"
+    ref_it = json.loads(str(np.load(fx)["meta"]))["iterations"] if fx.exists() else None
+    return {"rows": REF_ROWS, "nrhs": R, "precision": "mixed", "value": R * 1e3 / ms, "unit": UNIT,
+            "iterations": sorted({i["iterations"] for i in infos}),
+            "max_rel_residual": max(i["rel_residual"] for i in infos), "setup_s": setup_ms / 1e3,
+            "reference_iterations_fp64_one_source": ref_it, "autotune": tuned}
+
+
+def line_uneven_batch(local, steps):
+    """24 configurations (8 each at 128^2, 256^2 and 512^2, beta cycling through 2, 3, 4,
+    m0 = -0.05), 32 sources each, mixed precision, solved together by amg_solve_many_dev."""
+    import torch
+
+    from amg_schwingermodel_b200 import AMGContext, solve_many_dev
+    from amg_schwingermodel_b200.inputs import gauge_field
+    dev = f"cuda:{local}"
+    ctxs, bufs = [], []
+    setup_s = 0.0
+    try:
+        k = 0
+        for ns, rows in BATCH_ROWS.items():
+            for i in range(BATCH_PER_SIZE):
+                beta = (2.0, 3.0, 4.0)[i % 3]
+                ctx = AMGContext(ns, ns, rows, M0, precision=1, max_rhs=BATCH_RHS, device=local)
+                ctxs.append(ctx)
+                ctx.set_gauge(gauge_field(ns, ns, beta, 3000 + k))
+                setup_s += ctx.setup() / 1e3
+                g = torch.Generator(device=dev).manual_seed(4000 + k)
+                b = torch.randn(BATCH_RHS, ns * ns, 2, 2, dtype=torch.float64, device=dev, generator=g)
+                bufs.append((b, torch.empty_like(b)))
+                k += 1
+        bp = [b.data_ptr() for b, _ in bufs]
+        xp = [x.data_ptr() for _, x in bufs]
+        nr = [BATCH_RHS] * len(ctxs)
+        infos = solve_many_dev(ctxs, bp, xp, nr)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            infos = solve_many_dev(ctxs, bp, xp, nr)
+        torch.cuda.synchronize()
+        dt = (time.perf_counter() - t0) / steps
+    finally:
+        for c in ctxs:
+            c.close()
+    allinfo = [i for inf in infos for i in inf]
+    per_size = {}
+    for (ns, _), inf in zip([(ns, i) for ns in BATCH_ROWS for i in range(BATCH_PER_SIZE)], infos):
+        per_size.setdefault(str(ns), set()).update(i["iterations"] for i in inf)
+    return {"configurations": len(ctxs), "sizes": list(BATCH_ROWS), "nrhs_each": BATCH_RHS,
+            "rows": {str(k): v for k, v in BATCH_ROWS.items()}, "precision": "mixed",
+            "value": len(allinfo) / dt, "unit": UNIT, "s_per_step": dt, "steps": steps,
+            "iterations_by_size": {k: sorted(v) for k, v in per_size.items()},
+            "max_rel_residual": max(i["rel_residual"] for i in allinfo),
+            "converged": all(i["converged"] for i in allinfo), "setup_s_total": setup_s,
+            "timing": "host clock around amg_solve_many_dev calls (the contexts run on their own streams; the call "
+                      "returns after every context's solve has finished)"}
 
 
 def run_ours(args, world, rank, local):
@@ -273,6 +436,7 @@ def run_ours(args, world, rank, local):
     gseed, bseed = replica_seeds(rank)
     U = gauge_field(NX, NT, BETA, gseed)
     b_host = gaussian_spinor(N, 2, bseed, nrhs=R)
+    extras = world == 1 and not args.no_extras
     # ---- the chosen form: mixed precision, R sources per solve
     ctx = AMGContext(NX, NT, ROWS, M0, precision=prec, max_rhs=R, device=local)
     ctx.set_gauge(U)
@@ -327,31 +491,34 @@ def run_ours(args, world, rank, local):
     ms_e2e = max_over_ranks(e2.elapsed_time(e3), world)
     e2e_value = world * R * args.steps / (ms_e2e / 1e3)
     ctx.close()
+    del b_pin, x_pin
 
-    # ---- the plain FP64 drop-in on one source, same gauge field
+    # ---- the plain FP64 drop-in on one source, same gauge field (>= 10 timed solves)
     ctx64 = AMGContext(NX, NT, ROWS, M0, precision=0, max_rhs=1, device=local)
     ctx64.set_gauge(U)
     setup64_ms = ctx64.setup()
     b1 = b_dev[0:1].contiguous()
     x1 = torch.empty_like(b1)
-    for _ in range(max(2, args.warmup)):
-        info64 = ctx64.solve_dev(b1.data_ptr(), x1.data_ptr(), 1)
-    torch.cuda.synchronize()
-    s64 = torch.cuda.ExternalStream(ctx64.stream())
-    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    n64 = max(2, min(args.steps, 3))
-    f0.record(s64)
-    for _ in range(n64):
-        info64 = ctx64.solve_dev(b1.data_ptr(), x1.data_ptr(), 1)
-    f1.record(s64)
-    torch.cuda.synchronize()
-    ms64 = max_over_ranks(f0.elapsed_time(f1), world)
-    fp64_value = world * n64 / (ms64 / 1e3)
+    n64 = max(10, min(args.steps, 20))
+    ms64, info64 = timed_solves(ctx64, b1.data_ptr(), x1.data_ptr(), 1, n64, max(3, args.warmup))
+    ms64 = max_over_ranks(ms64, world)
+    fp64_value = world * 1e3 / ms64
     x64 = x1.cpu().numpy().view(np.complex128).reshape(N, 2)
     tuned64 = ctx64.autotune_info()
     err_vs_fp64 = float(np.linalg.norm(x_chosen[0] - x64) / np.linalg.norm(x64))
-    hierarchy = hierarchy_for_reference(ctx64) if (rank == 0 and world == 1 and not args.no_cpu) else None
+    hierarchy = hierarchy_for_reference(ctx64) if (rank == 0 and extras and not args.no_cpu) else None
     ctx64.close()
+    fp64_batched = None
+    if extras:
+        # ---- FP64 on the same batch of R sources: splits the gain into batching and precision
+        with AMGContext(NX, NT, ROWS, M0, precision=0, max_rhs=R, device=local) as ctx64b:
+            ctx64b.set_gauge(U)
+            ctx64b.setup()
+            ms64b, info64b = timed_solves(ctx64b, b_dev.data_ptr(), x_dev.data_ptr(), R, 3, 1)
+            fp64_batched = {"value": R * 1e3 / ms64b, "unit": UNIT, "nrhs": R, "steps": 3,
+                            "iterations": sorted({i["iterations"] for i in info64b}),
+                            "max_rel_residual": max(i["rel_residual"] for i in info64b),
+                            "autotune": ctx64b.autotune_info()}
 
     # ---- fine D-apply bandwidth (FP64, 8 sources per launch: 768 MB of spinors > L2)
     nd = 8
@@ -375,34 +542,63 @@ def run_ours(args, world, rank, local):
     d_bytes = N * (32 + nd * 64)
     hbm, peak_kind = peaks()
     d_gbs = d_bytes / (d_ms * 1e-3) / 1e9
+    del vin, vout, Ud
 
     # ---- roofline of the dominant kernel class of the step
     dom = max(prof, key=lambda k: prof[k]["ms"])
     pd = prof[dom]
     per_launch_ms = pd["ms"] / max(pd["launches"], 1)
     per_launch_bytes = pd["bytes"] / max(pd["launches"], 1)
-    achieved = per_launch_bytes / (per_launch_ms * 1e-3) / 1e9 if per_launch_ms > 0 else 0.0
+    achieved_gbs = per_launch_bytes / (per_launch_ms * 1e-3) / 1e9 if per_launch_ms > 0 else 0.0
     tot_prof = sum(v["ms"] for v in prof.values())
-    ncol = ROWS[0][4] * ROWS[0][5] // 2
-    sap_traffic = SAP_DRAM_BYTES_PER_BLOCK_SOURCE * ncol * R
+    share = pd["ms"] / tot_prof if tot_prof else None
+    if dom == "sap":
+        # block solves live in shared memory and registers: bound by FP32 issue, not HBM
+        ncol = ROWS[0][4] * ROWS[0][5] // 2
+        sms = torch.cuda.get_device_properties(local).multi_processor_count
+        sm_mhz = clocks.get("sm_mhz") or 1965.0
+        peak_tf = sms * FP32_LANES_PER_SM * 2 * sm_mhz * 1e6 / 1e12
+        flops = SAP_FLOPS_PER_SITE * (N // 2) * R
+        tf = flops / (per_launch_ms * 1e-3) / 1e12
+        roofline = {"kernel": "sap", "bound": "fp32", "achieved": tf, "peak": peak_tf, "unit": "TFLOP/s",
+                    "frac": tf / peak_tf, "traffic": SAP_DRAM_BYTES_PER_BLOCK_SOURCE * ncol * R,
+                    "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch at 32 sources",
+                    "peak_kind": (f"nominal FP32 CUDA-core peak: {sms} SMs x {FP32_LANES_PER_SM} lanes x 2 flop x "
+                                  f"{sm_mhz:.0f} MHz (sampled); no measured FP32 peak exists on this pool"),
+                    "flops_per_launch": flops, "bytes_per_launch": per_launch_bytes,
+                    "ms_per_launch": per_launch_ms, "achieved_gbs": achieved_gbs, "hbm_frac": achieved_gbs / hbm,
+                    "share_of_step": share}
+    else:
+        roofline = {"kernel": dom, "bound": "hbm", "achieved": achieved_gbs, "peak": hbm, "unit": "GB/s",
+                    "frac": achieved_gbs / hbm, "traffic": None, "peak_kind": peak_kind,
+                    "bytes_per_launch": per_launch_bytes, "ms_per_launch": per_launch_ms, "share_of_step": share}
 
-    # ---- CPU baseline: the reference's own outer iteration on this workload (rank 0, N = 1)
+    extra = {}
+    if extras:
+        torch.cuda.empty_cache()
+        for key, fn in (("config2_256", lambda: line_config2(local)),
+                        ("reference_rows", lambda: line_reference_rows(local, R)),
+                        ("uneven_batch", lambda: line_uneven_batch(local, 2))):
+            try:
+                extra[key] = fn()
+            except Exception as e:  # noqa: BLE001 -- a failed side line must not lose the headline
+                extra[key] = {"error": f"{type(e).__name__}: {e}"}
+            torch.cuda.empty_cache()
+
+    # ---- CPU baseline: complete reference solves on this workload (rank 0, N = 1)
     cpu = None
     if hierarchy is not None:
         try:
-            ranks = reference_ranks()
-            # with several ranks the first iteration also pays the first touch of the shared
-            # all-reduce buffers: time two and keep the second
-            res, err = cpu_reference_sample(U, b_host[0], hierarchy, 2 if ranks > 1 else 1, ranks)
-            if res:
-                it_s = res["times"][-1]
-                it_count = info64[0]["iterations"]
-                cpu = {"value": 1.0 / (it_count * it_s), "unit": UNIT, "cores": res["ranks"], "kind": "reference",
-                       "sample": (f"reference K-cycle + D_phi (one outer FGMRES iteration) at {NX}x{NT} L4 on "
-                                  f"this hierarchy, {res['ranks']} rank(s) of its MPI layout: {it_s:.2f} s; "
-                                  f"x {it_count} iterations; D_phi {res['dphi_s'] * 1e3:.1f} ms/apply")}
+            res = cpu_reference_solve(U, b_host[0], hierarchy)
+            if "error" not in res:
+                cpu = {"value": 1.0 / res["t"], "unit": UNIT, "cores": res["ranks"], "kind": "reference",
+                       "sample": (f"complete reference FGMRES_AMG solve (its FGMRES, K-cycle, SAP and D_phi code) "
+                                  f"at {NX}x{NT} L4 on the hierarchy the GPU FP64 set-up built, {res['ranks']} rank(s) "
+                                  f"of its MPI layout: {res['t']:.2f} s, {res['iterations']} iterations, FP64 "
+                                  f"residual {res['residual']:.1e} (solve {res['solves']} of {res['solves']}); "
+                                  f"D_phi {res['dphi_s'] * 1e3:.1f} ms/apply")}
             else:
-                cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": err}
+                cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": res["error"]}
         except Exception as e:  # noqa: BLE001
             cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": f"failed: {e}"}
 
@@ -418,18 +614,13 @@ def run_ours(args, world, rank, local):
             "iterations": iters, "max_rel_residual": resid, "converged": converged,
             "err_vs_fp64": err_vs_fp64,
             "setup_s": setup_ms / 1e3,
-            "fp64_dropin": {"value": fp64_value, "unit": UNIT, "iterations": info64[0]["iterations"],
-                            "rel_residual": info64[0]["rel_residual"], "setup_s": setup64_ms / 1e3,
-                            "autotune": tuned64},
+            "fp64_dropin": {"value": fp64_value, "unit": UNIT, "nrhs": 1, "steps": n64,
+                            "iterations": info64[0]["iterations"], "rel_residual": info64[0]["rel_residual"],
+                            "setup_s": setup64_ms / 1e3, "autotune": tuned64},
             "speedup_vs_fp64_dropin": value / fp64_value,
             "dapply": {"gbs": d_gbs, "frac": d_gbs / hbm, "peak_gbs": hbm, "peak": peak_kind,
                        "ms_per_launch": d_ms, "nrhs": nd, "bytes_per_launch": d_bytes},
-            "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "traffic": sap_traffic if dom == "sap" else None,
-                         "traffic_source": "ncu capture at 2 sources, scaled by blocks x sources" if dom == "sap" else None,
-                         "peak_kind": peak_kind,
-                         "share_of_step": pd["ms"] / tot_prof if tot_prof else None,
-                         "bytes_per_launch": per_launch_bytes, "ms_per_launch": per_launch_ms},
+            "roofline": roofline,
             "kernels": prof,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(R * N * 32),
                     "d2h_bytes_per_step": int(R * N * 32)},
@@ -437,6 +628,11 @@ def run_ours(args, world, rank, local):
             "clocks": clocks,
             "cpu_baseline": cpu,
         }
+        if fp64_batched is not None:
+            line["fp64_batched"] = fp64_batched
+            line["speedup_split"] = {"batching_f64": fp64_batched["value"] / fp64_value,
+                                     "precision_at_batch": value / fp64_batched["value"]}
+        line.update(extra)
         print(json.dumps(line))
 
 
@@ -449,8 +645,8 @@ def main():
     ap.add_argument("--rhs", type=int, default=32, help="sources per batched solve (one step)")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "f64"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
-    ap.add_argument("--ref-iterations", type=int, default=10,
-                    help="outer iterations of the reference algorithm on this workload (FP64 drop-in count)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the side lines (FP64 batch, reference rows, 256^2, uneven batch)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":

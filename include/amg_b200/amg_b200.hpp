@@ -25,6 +25,7 @@
 #include <iomanip>
 #include <iostream>
 #include <memory>
+#include <random>
 #include <sstream>
 #include <stdexcept>
 #include <string>
@@ -104,7 +105,15 @@ inline int SAP_Block_t[AMGV::levels] = {};
 inline int GMRES_restart_len[AMGV::levels] = {};
 inline int GMRES_restarts[AMGV::levels] = {};
 inline double GMRES_tol[AMGV::levels] = {};
+inline int SAP_elements_x[AMGV::levels] = {};
+inline int SAP_elements_t[AMGV::levels] = {};
+inline int SAP_variables_per_block[AMGV::levels] = {};
 }  // namespace LevelV
+
+// bare mass of the reference's main and reports (include/variables.h:20-22)
+namespace mass {
+inline double m0 = 0;
+}  // namespace mass
 
 namespace amg_b200 {
 
@@ -227,6 +236,11 @@ inline void readParameters(const std::string& inputFile) {
         LevelV::NtSites[l] = l == 0 ? LV::Nt : LevelV::BlocksT[l - 1];
         LevelV::DOF[l] = l == 0 ? 2 : 2 * LevelV::Ntest[l - 1];
         LevelV::Colors[l] = l == 0 ? 1 : LevelV::Ntest[l - 1];
+        if (l < maxLevel && LevelV::SAP_Block_x[l] > 0 && LevelV::SAP_Block_t[l] > 0) {
+            LevelV::SAP_elements_x[l] = LevelV::NxSites[l] / LevelV::SAP_Block_x[l];
+            LevelV::SAP_elements_t[l] = LevelV::NtSites[l] / LevelV::SAP_Block_t[l];
+            LevelV::SAP_variables_per_block[l] = LevelV::DOF[l] * LevelV::SAP_elements_x[l] * LevelV::SAP_elements_t[l];
+        }
     }
     LevelV::SAP_Block_x[maxLevel] = 1;
     LevelV::SAP_Block_t[maxLevel] = 1;
@@ -268,6 +282,127 @@ inline void read_rhs(spinor& vec, const std::string& name) {
     int x, t, mu;
     double re, im;
     while (in >> x >> t >> mu >> re >> im) vec[x * LV::Nt + t][mu] = c_double(re, im);
+}
+
+// ---- text output and the experiment reports (src/variables.cpp:101-155, :158-290) --------
+// The file names and column layouts are the reference's, so its plotting scripts read them.
+
+// "index  value" rows, 17 significant digits (src/variables.cpp:101-115)
+inline void save_vec(const std::vector<double>& vec, const std::string& name) {
+    std::ofstream f(name);
+    if (!f) throw amg_b200::Error(AMG_ERR_INVALID, "save_vec: cannot open " + name);
+    for (size_t n = 0; n < vec.size(); n++)
+        f << n << std::setw(30) << std::setprecision(17) << std::scientific << vec[n] << "\n";
+}
+
+// "x t spin re im" rows, the format read_rhs reads (src/variables.cpp:132-155)
+inline void save_rhs(const spinor& rhs, const std::string& name) {
+    std::ofstream f(name);
+    if (!f) throw amg_b200::Error(AMG_ERR_INVALID, "save_rhs: cannot open " + name);
+    for (int n = 0; n < LV::Ntot; n++)
+        for (int spin = 0; spin < 2; spin++)
+            f << n / LV::Nt << std::setw(30) << n % LV::Nt << std::setw(30) << spin << std::setw(30)
+              << std::setprecision(17) << std::scientific << std::real(rhs[n][spin]) << std::setw(30)
+              << std::setprecision(17) << std::scientific << std::imag(rhs[n][spin]) << "\n";
+}
+
+// uniform(-1, 1) complex entries from one generator seeded on the first call, as the
+// reference's function-local static std::mt19937 (src/variables.cpp:158-168); the same
+// expression, so the same compiler draws the parts in the same order.
+inline void random_rhs(spinor& vec, const int seed) {
+    static std::mt19937 gen(seed);
+    std::uniform_real_distribution<double> u(-1.0, 1.0);
+    const c_double I(0, 1);
+    for (int i = 0; i < LV::Ntot; i++) {
+        vec[i][0] = u(gen) + I * u(gen);
+        vec[i][1] = u(gen) + I * u(gen);
+    }
+}
+
+// the run banner (src/variables.cpp:170-222)
+inline void printParameters() {
+    using std::cout;
+    const char* rule = "---------------------------------------------------------------------------------------";
+    cout << "******************* AMG for the Dirac matrix in the Schwinger model *******************\n";
+    cout << "| Nx = " << LV::Nx << " Nt = " << LV::Nt << "\n";
+    cout << "| Lattice dimension = " << LV::Ntot << "\n";
+    cout << "| Number of entries of the Dirac matrix = (" << 2 * LV::Ntot << ")^2\n";
+    cout << "| Bare mass parameter m0 = " << mass::m0 << "\n" << rule << "\n";
+    cout << "* Blocks, aggregates and test vectors at each level\n";
+    for (int l = 0; l < AMGV::levels - 1; l++)
+        cout << "| Level " << l << " Block X " << LevelV::BlocksX[l] << " Block T " << LevelV::BlocksT[l]
+             << " Ntest " << LevelV::Ntest[l] << " Nagg " << LevelV::Nagg[l] << " Number of lattice blocks "
+             << LevelV::NBlocks[l] << " Schwarz Block T " << LevelV::SAP_Block_t[l] << " Schwarz Block X "
+             << LevelV::SAP_Block_x[l] << "\n";
+    cout << rule << "\n* SAP blocks\n";
+    for (int l = 0; l < AMGV::levels - 1; l++)
+        cout << "| Level " << l << " Schwarz Block T " << LevelV::SAP_Block_t[l] << " Schwarz Block X "
+             << LevelV::SAP_Block_x[l] << " Number of blocks " << LevelV::SAP_Block_t[l] * LevelV::SAP_Block_x[l]
+             << " Each block has " << LevelV::SAP_variables_per_block[l] << " variables\n";
+    cout << rule << "\n* Sites and degrees of freedom at each level\n";
+    for (int l = 0; l < AMGV::levels; l++)
+        cout << "| Level " << l << " Nsites " << LevelV::Nsites[l] << " Nxsites " << LevelV::NxSites[l]
+             << " NtSites " << LevelV::NtSites[l] << " DOF " << LevelV::DOF[l] << " Colors " << LevelV::Colors[l]
+             << "\n";
+    cout << rule << "\n";
+    cout << "| GMRES restart length for SAP blocks = " << SAPV::sap_gmres_restart_length << "\n";
+    cout << "| GMRES restarts for SAP blocks = " << SAPV::sap_gmres_restarts << "\n";
+    cout << "| GMRES tolerance for SAP blocks = " << SAPV::sap_gmres_tolerance << "\n" << rule << "\n";
+    cout << "* AMG parameters\n";
+    if (AMGV::cycle == 0) cout << "| Cycle = V-cycle\n";
+    else if (AMGV::cycle == 1) cout << "| Cycle = K-cycle\n";
+    cout << "| Number of levels = " << AMGV::levels << "\n";
+    cout << "| nu1 (pre-smoothing) = " << AMGV::nu1 << " nu2 (post-smoothing) = " << AMGV::nu2 << "\n";
+    cout << "| Number of iterations for improving the interpolator = " << AMGV::Nit << "\n";
+    cout << "| Restart length of GMRES at the coarse level = " << LevelV::GMRES_restart_len[LevelV::maxLevel] << "\n";
+    cout << "| Restarts of GMRES at the coarse level = " << LevelV::GMRES_restarts[LevelV::maxLevel] << "\n";
+    cout << "| GMRES tolerance for the coarse level solution = " << LevelV::GMRES_tol[LevelV::maxLevel] << "\n";
+    cout << "* FGMRES with AMG preconditioning parameters\n";
+    cout << "| FGMRES restart length = " << FGMRESV::fgmres_restart_length << "\n";
+    cout << "| FGMRES restarts = " << FGMRESV::fgmres_restarts << "\n";
+    cout << "| FGMRES tolerance = " << FGMRESV::fgmres_tolerance << "\n";
+    cout << "*****************************************************************************************************"
+         << std::endl;
+}
+
+// The experiment reports of the reference's main (src/variables.cpp:226-290):
+// metadata_<Nx>x<Nt>_Levels<L>_{V,K}cycle.dat (the blocking rows and solver parameters, and
+// the configuration id) and results_<Nx>x<Nt>_Levels<L>_{V,K}cycle.out (one row per bootstrap
+// setting 2i: mean and spread of the iteration count and of the solve time over nMeas).
+inline void saveParameters(double* Iter, double* dIter, double* exTime, double* dexTime, const int nMeas,
+                           const int nconf) {
+    std::ostringstream tag;
+    tag << LV::Nx << "x" << LV::Nt << "_Levels" << AMGV::levels << (AMGV::cycle == 0 ? "_Vcycle" : "_Kcycle");
+    {
+        std::ofstream m("metadata_" + tag.str() + ".dat");
+        if (!m) throw amg_b200::Error(AMG_ERR_INVALID, "saveParameters: cannot open metadata_" + tag.str() + ".dat");
+        m << "#level, blocks_x, blocks_t, Ntest, SAP_blocks_x, SAP_blocks_t\n";
+        for (int l = 0; l < AMGV::levels - 1; l++)
+            m << l << std::setw(5) << LevelV::BlocksX[l] << std::setw(5) << LevelV::BlocksT[l] << std::setw(5)
+              << LevelV::Ntest[l] << std::setw(5) << LevelV::SAP_Block_x[l] << std::setw(5) << LevelV::SAP_Block_t[l]
+              << "\n";
+        m << "#SAP_test_vectors_iterations\n" << AMGV::SAP_test_vectors_iterations << "\n";
+        m << "#cycle (0 = V, 1 = K)\n" << AMGV::cycle << "\n";
+        m << "#Pre-smoothing nu1, Post-smoothing nu2\n" << AMGV::nu1 << std::setw(5) << AMGV::nu2 << "\n";
+        m << "#sap gmres restart length, sap gmres restarts, sap gmres tolerance\n";
+        m << SAPV::sap_gmres_restart_length << std::setw(5) << SAPV::sap_gmres_restarts << std::setw(15)
+          << std::scientific << std::setprecision(7) << SAPV::sap_gmres_tolerance << "\n";
+        m << "#GMRES restart length coarse level, GMRES restarts coarse level, GMRES tolerance coarse level\n";
+        m << LevelV::GMRES_restart_len[LevelV::maxLevel] << std::setw(5) << LevelV::GMRES_restarts[LevelV::maxLevel]
+          << std::setw(15) << std::scientific << std::setprecision(7) << LevelV::GMRES_tol[LevelV::maxLevel] << "\n";
+        m << "#FGMRES restart length, FGMRES restarts, FGMRES tolerance\n";
+        m << FGMRESV::fgmres_restart_length << std::setw(5) << FGMRESV::fgmres_restarts << std::setw(15)
+          << std::scientific << std::setprecision(7) << FGMRESV::fgmres_tolerance << "\n";
+        m << "#Configuration ID analyzed: \n" << nconf << "\n";
+    }
+    std::ofstream r("results_" + tag.str() + ".out");
+    if (!r) throw amg_b200::Error(AMG_ERR_INVALID, "saveParameters: cannot open results_" + tag.str() + ".out");
+    r << "#Nit  Iterations  dIterations  exTime  dexTime\n";
+    for (int i = 0; i < nMeas; i++)
+        r << 2 * i << std::setw(15) << std::scientific << std::setprecision(7) << Iter[i] << std::setw(15)
+          << std::scientific << std::setprecision(7) << dIter[i] << std::setw(15) << std::scientific
+          << std::setprecision(7) << exTime[i] << std::setw(15) << std::scientific << std::setprecision(7)
+          << dexTime[i] << "\n";
 }
 
 // ---- D_phi / D_dagger_phi (include/dirac_operator.h:14-23) ----------------------------

@@ -177,7 +177,10 @@ AMG_API int amg_dirac_apply_host(const double* U, const double* in, double* out,
  * nrhs * bx * bt * 2 * ntest * 16 > 4 MiB are rejected with AMG_ERR_INVALID.  The buffers
  * belong to the current device.  The first call on a device looks up that array's address
  * (make that first call before any stream capture).  All calls on a device share the array,
- * so calls that overlap on the GPU (other streams, other host threads) race; serialise them. */
+ * so calls that overlap on the GPU (other streams, other host threads) race; serialise them.
+ * The looked-up address does not survive cudaDeviceReset: do not call this again on a device
+ * after resetting it.  A CUDA error already pending on the calling thread is reported (and
+ * left pending) as AMG_ERR_CUDA, with nothing launched.  nx * nt * 2 must fit in an int. */
 AMG_API int amg_restrict_raw_noalloc(const void* W_dev, const void* v_dev, void* out_dev, int nx, int nt,
                                      int bx, int bt, int ntest, int nrhs, void* stream);
 
@@ -200,6 +203,14 @@ AMG_API int amg_level_apply(amg_ctx ctx, int level, const double* in, double* ou
 AMG_API int amg_restrict(amg_ctx ctx, int level, const double* in, double* out);
 /* Level::P_v (src/level.cpp:182-209): level l+1 -> l. */
 AMG_API int amg_prolong(amg_ctx ctx, int level, const double* in, double* out);
+/* The mixed form's level-0 Level::Pt_v / Level::P_v (src/level.cpp:182-237) on device buffers
+ * of complex64 values, as its cycles run them (BF16 test vectors, FP32 sources; the tensor-core
+ * kernels where the lattice allows, AMG_TC_TRANSFER=0 for the CUDA-core ones):
+ *   restriction:  out[nrhs][bx*bt][2*Ntest] = P^dagger in[nrhs][N][2]
+ *   prolongation: out[nrhs][N][2] += P in[nrhs][bx*bt][2*Ntest]
+ * The context must be in the mixed form with its set-up done; synchronises its stream. */
+AMG_API int amg_restrict0_mixed_dev(amg_ctx ctx, const void* in_dev, void* out_dev, int nrhs);
+AMG_API int amg_prolong0_mixed_dev(amg_ctx ctx, const void* in_dev, void* out_dev, int nrhs);
 /* SAP_C::SAP (src/sap.cpp:64-174) on level l: nu iterations on D x = v, x in/out.
  * Returns AMG_OK if the SAP tolerance was met, AMG_NOT_CONVERGED otherwise (the
  * reference returns 1 / 0). */

@@ -5,13 +5,14 @@
 #
 #   oracle/build_ref.sh NS NT LEVELS [REFDIR]
 #
-# Reads the sources where they lie (default /root/reference); writes only under
+# Reads the sources where they lie (REFDIR; default $AMG_REFERENCE_DIR, else a directory
+# named `reference` beside the repository root); writes only under
 # oracle/_ref/.  The reference's include/config.h is bypassed by force-including a
 # generated header that defines its include guard (CONFIG_H) first.
 set -euo pipefail
 NS=${1:?NS}; NT=${2:?NT}; LEVELS=${3:?LEVELS}
-REF=${4:-/root/reference}
 HERE=$(cd "$(dirname "$0")" && pwd)
+REF=${4:-${AMG_REFERENCE_DIR:-$(cd "$HERE/../.." && pwd)/reference}}
 OUT="$HERE/_ref"
 TAG="${NS}x${NT}_l${LEVELS}"
 OBJ="$OUT/obj_$TAG"

@@ -237,6 +237,60 @@ void dump_hierarchy(AlgebraicMG& amg, const std::string& tag) {
     }
 }
 
+// FGMRES_AMG's two overrides (include/amg.h:130-144) over an AlgebraicMG given from outside,
+// so that a hierarchy loaded from files instead of built by the constructor's setUpPhase
+// drives the reference's own outer FGMRES (src/fgmres.cpp:5-88) and cycles (src/amg.cpp).
+class LoadedAMGFGMRES : public FGMRES {
+public:
+    LoadedAMGFGMRES(const int& dim1, const int& dim2, const int& m, const int& restarts, const double& tol,
+                    const GaugeConf& g, double m0, AlgebraicMG& amg)
+        : FGMRES(dim1, dim2, m, restarts, tol), g_(g), m0_(m0), amg_(amg) {}
+
+private:
+    const GaugeConf& g_;
+    const double m0_;
+    AlgebraicMG& amg_;
+    void func(const spinor& in, spinor& out) override { D_phi(g_.Conf, in, out, m0_); }
+    void preconditioner(const spinor& in, spinor& out) override {
+        for (auto& row : out)
+            for (auto& v : row) v = 0;
+        if (AMGV::cycle == 0) amg_.v_cycle(0, in, out);
+        else if (AMGV::cycle == 1) amg_.k_cycle(0, in, out);
+    }
+};
+
+// Runs `solve` (one complete outer solve from x0 = 0, returning the reference's iteration
+// count; `last` says whether to print and save the residual history) up to `reps` times, at
+// least once, while rank 0's summed solve time stays below `budget` seconds (0: no budget).
+// With several ranks the stop decision uses rank 0's clock on every rank (an all-reduce sum
+// with zeros elsewhere), so all ranks run the same number of solves.  Writes
+// solve_seconds_<r> / iterations_<r> per solve and solves_done; returns the last count.
+template <class F>
+int timed_solves(F&& solve, int reps, double budget, std::ofstream& info, double& t_last) {
+    double total = 0;
+    int iters = 0, done = 0;
+    for (int r = 0; r < reps; r++) {
+        bool last = r == reps - 1;
+        if (!last && budget > 0) {
+            // would one more solve of the last solve's length still fit the budget (rank 0's
+            // projected total, the same on every rank)?
+            double t0 = oracle_mpi().rank != 0 ? 0.0 : total + t_last;
+            double tsum = t0;
+            if (oracle_mpi().size > 1) MPI_Allreduce(&t0, &tsum, 1, MPI_DOUBLE, MPI_SUM, MPI_COMM_WORLD);
+            if (r > 0 && tsum > budget) break;
+        }
+        const double t1 = now_s();
+        iters = solve(last);
+        t_last = now_s() - t1;
+        total += t_last;
+        done++;
+        info << "solve_seconds_" << r << " " << t_last << "\n";
+        info << "iterations_" << r << " " << iters << "\n";
+    }
+    info << "solves_done " << done << "\n";
+    return iters;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -376,6 +430,32 @@ int main(int argc, char** argv) {
                 }
             }
         }
+        if ((int)jd(job, "solve_reps", 0) > 0) {
+            // complete outer solves (FGMRES_AMG::fgmres, x0 = 0) on the loaded hierarchy
+            static const int dim1 = LV::Ntot, dim2 = 2;
+            LoadedAMGFGMRES fs(dim1, dim2, FGMRESV::fgmres_restart_length, FGMRESV::fgmres_restarts,
+                               FGMRESV::fgmres_tolerance, GConf, m0, amgh);
+            spinor x0(N, c_vector(2, 0)), x(N, c_vector(2, 0));
+            if (late_ranks && !start_ranks(ranks, &info)) return 3;
+            double t_last = 0;
+            const int iters = timed_solves([&](bool last) { return fs.fgmres(rhs, x0, x, last, last); },
+                                           (int)jd(job, "solve_reps", 1), jd(job, "solve_budget_seconds", 0), info,
+                                           t_last);
+            dump_spinor("x", x);
+            spinor Dx(N, c_vector(2, 0));
+            D_phi(GConf.Conf, x, Dx, m0);
+            double rr = 0, bb = 0;
+            for (int n = 0; n < N; n++)
+                for (int a = 0; a < 2; a++) {
+                    rr += std::norm(rhs[n][a] - Dx[n][a]);
+                    bb += std::norm(rhs[n][a]);
+                }
+            info << "true_rel_residual " << std::sqrt(rr / bb) << "\n";
+            info << "iterations " << iters << "\n";
+            info << "solve_seconds " << t_last << "\n";
+            g_manifest.close();
+            return 0;
+        }
         const int reps = std::max(1, (int)jd(job, "outer_iteration_reps", 1));
         spinor v(N, c_vector(2, 0)), z(N, c_vector(2, 0)), w(N, c_vector(2, 0));
         double nb = std::sqrt(std::real(dot(rhs, rhs)));
@@ -478,10 +558,16 @@ int main(int argc, char** argv) {
         return 0;
     }
 
-    // The outer solve (src/tests.cpp:67-82): FGMRES_AMG::fgmres(rhs, x0 = 0, x).
-    t0 = now_s();
-    int iters = f_amg.fgmres(rhs, x0, x, true, true);
-    double t_solve = now_s() - t0;
+    // The outer solve (src/tests.cpp:67-82): FGMRES_AMG::fgmres(rhs, x0 = 0, x).  With
+    // `solve_reps` R > 1 the complete solve is repeated up to R times on the same hierarchy
+    // (each call starts from x0 = 0 and re-zeroes the solver's state, src/fgmres.cpp:6-9),
+    // each one timed, within `solve_budget_seconds`; the ranks of `ranks_after_setup` start
+    // just before the first.
+    const int solve_reps = std::max(1, (int)jd(job, "solve_reps", 1));
+    if (late_ranks && !start_ranks(ranks, &info)) return 3;
+    double t_solve = 0;
+    const int iters = timed_solves([&](bool last) { return f_amg.fgmres(rhs, x0, x, last, last); }, solve_reps,
+                                   jd(job, "solve_budget_seconds", 0), info, t_solve);
     dump_spinor("x", x);
     {
         spinor Dx(N, c_vector(2, 0));

@@ -20,7 +20,9 @@ def binary(ns: int, nt: int, levels: int) -> Path:
     return REF_DIR / f"ref_{ns}x{nt}_l{levels}"
 
 
-DEFAULT_REFDIR = os.environ.get("AMG_REFERENCE_DIR", "/root/reference")
+# The reference checkout: AMG_REFERENCE_DIR, else a directory named `reference` beside this
+# repository's root.
+DEFAULT_REFDIR = os.environ.get("AMG_REFERENCE_DIR", str(HERE.parent.parent / "reference"))
 
 
 def available(ns: int, nt: int, levels: int, refdir: str = DEFAULT_REFDIR) -> bool:
@@ -67,13 +69,19 @@ def run(ns: int, nt: int, rows, gauge: np.ndarray, rhs: np.ndarray, *, m0: float
         solve: int = 1, phases: int = 0, dump_hierarchy: int = 1, dphi_reps: int = 0,
         dphi_only: int = 0, outer_iteration_reps: int = 0, hierarchy: dict | None = None, probes=None,
         workdir: str | None = None, timeout: float = 3600, krylov: int = 0, ranks: int = 1,
-        ranks_after_setup: int = 0, drill_exit_rank: int = -1) -> dict:
+        ranks_after_setup: int = 0, drill_exit_rank: int = -1, solve_reps: int = 0,
+        solve_budget_seconds: float = 0.0) -> dict:
     """Writes the job, runs the binary for (ns, nt, len(rows)+1 levels), returns its dumps
     (rank 0's).  ranks > 1 runs the reference's MPI layout as that many processes on this
     host (oracle/mpi_shim/mpi.h): its SAP block solves split among them; with
     ranks_after_setup = 1 the ranks start after the set-up, just before the timed outer
-    iterations (they then share the set-up's memory).  drill_exit_rank = r > 0 makes rank r
-    leave before its first collective (the stand-in's failure drill)."""
+    iterations (they then share the set-up's memory).  solve_reps = R > 0 runs the complete
+    FGMRES_AMG solve up to R times on the one set-up (or on a loaded `hierarchy`), timing each
+    (info:solve_seconds_<r>, info:iterations_<r>, info:solves_done), stopping early once
+    another solve would take rank 0's total past solve_budget_seconds (0: no budget); 0 runs
+    one solve (no per-solve keys) or, with a loaded hierarchy, the outer-iteration sample.
+    drill_exit_rank = r > 0 makes rank r leave before its first collective (the stand-in's
+    failure drill)."""
     levels = len(rows) + 1
     b = binary(ns, nt, levels)
     if not b.exists():
@@ -89,7 +97,8 @@ def run(ns: int, nt: int, rows, gauge: np.ndarray, rhs: np.ndarray, *, m0: float
                nu2=nu2, solve=solve, phases=phases, dump_hierarchy=dump_hierarchy,
                dphi_reps=dphi_reps, dphi_only=dphi_only,
                outer_iteration_reps=outer_iteration_reps, krylov=krylov, ranks=ranks,
-               ranks_after_setup=ranks_after_setup, drill_exit_rank=drill_exit_rank)
+               ranks_after_setup=ranks_after_setup, drill_exit_rank=drill_exit_rank, solve_reps=solve_reps,
+               solve_budget_seconds=solve_budget_seconds)
     (wd / "job.txt").write_text("".join(f"{k} {v}\n" for k, v in job.items()))
     np.ascontiguousarray(gauge, dtype=np.complex128).tofile(wd / "gauge.bin")
     np.ascontiguousarray(rhs, dtype=np.complex128).tofile(wd / "rhs.bin")

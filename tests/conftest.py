@@ -25,8 +25,9 @@ def load_golden(name: str) -> dict:
 
 def golden_names():
     """The solve-path fixtures (the adjoint fixtures, adj*, hold only the two solves; the
-    krylov* fixtures only the comparison solvers)."""
-    return sorted(p.stem for p in GOLDEN.glob("*.npz") if not p.stem.startswith(("adj", "krylov")))
+    krylov* fixtures only the comparison solvers; the solve* fixtures only complete solves
+    at the workload sizes)."""
+    return sorted(p.stem for p in GOLDEN.glob("*.npz") if not p.stem.startswith(("adj", "krylov", "solve")))
 
 
 def rel(a, b) -> float:

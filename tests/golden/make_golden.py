@@ -16,6 +16,11 @@ conjugate_gradient solution of D D^dagger y = phi, the bi_cgstab solution of D x
 unpreconditioned FGMRES_fine_level(20, 50) solution and the FGMRES_SAP(20, 50) solution (the
 global SAP object given the gauge field by its set_params), with their iteration counts.
 
+The solve fixtures (SOLVES) hold complete reference solves at the workload sizes (256x256,
+512x512, 1024x1024), stored small: the iteration count, the true residual, the residual
+history, |x| and x and D_phi(b) on a strided subsample of the sites; the gauge field and the
+source are regenerated from the seeds in their meta.
+
 The adjoint fixture (ADJOINT) holds the reference's two solves behind the gradient of
 L = Re(eta^dagger D^{-1} b): x = D^{-1} b and y = D^{-1} gamma5 eta (so lambda = gamma5 y),
 each a full FGMRES_AMG run of the reference; the gauge field and the two sources are
@@ -67,6 +72,25 @@ KRYLOV = {
     "krylov64": (64, [[0, 8, 8, 8, 4, 4]], 2.0, -0.05, 43),
 }
 
+# Complete FGMRES_AMG solves (src/tests.cpp:67-82) at the workload configurations:
+# name: (ns, rows, beta, m0, seed); U = gauge_field(ns, ns, beta, seed),
+# b = gaussian_spinor(N, 2, seed + 1000).
+SOLVES = {
+    # 256x256, 3 levels, aggregation 8x8 then 4x4 blocks, Nv = 12, 4x4 SAP blocks, beta = 3
+    "solve256_l3": (256, [[0, 8, 8, 12, 4, 4], [1, 4, 4, 12, 4, 4]], 3.0, -0.05, 51),
+    # 1024x1024, 4 levels, Nv = 16, beta = 4, with the benchmark rows (32x32-site SAP blocks)
+    "solve1024_l4": (1024, [[0, 8, 8, 16, 32, 32], [1, 4, 4, 16, 4, 4], [2, 2, 2, 16, 2, 2]], 4.0, -0.05, 52),
+    # ... and with the reference-style rows (4x4 SAP blocks of 256x256 sites)
+    "solve1024_l4_refrows": (1024, [[0, 8, 8, 16, 4, 4], [1, 4, 4, 16, 4, 4], [2, 2, 2, 16, 2, 2]], 4.0, -0.05, 53),
+    # one configuration per lattice size of the uneven batch (128^2 at beta 2, 256^2 at 3,
+    # 512^2 at 4): 32x32-site SAP blocks, aggregation 8x8 then 4x4 blocks, Nv = 12
+    "solve128_l3_b2": (128, [[0, 8, 8, 12, 4, 4], [1, 4, 4, 12, 4, 4]], 2.0, -0.05, 54),
+    "solve256_l3_b3": (256, [[0, 8, 8, 12, 8, 8], [1, 4, 4, 12, 4, 4]], 3.0, -0.05, 55),
+    "solve512_l3_b4": (512, [[0, 8, 8, 12, 16, 16], [1, 4, 4, 12, 4, 4]], 4.0, -0.05, 56),
+}
+# sites kept of x and D_phi(b) in a solve fixture (every (N // SAMPLE_SITES)-th site)
+SAMPLE_SITES = 16384
+
 SMALL_KEYS_ALWAYS = ("dphi", "ddagphi", "x", "cycle0_rhs")
 
 
@@ -100,6 +124,28 @@ def make(name: str, cfg) -> dict:
                 kfgmres1_iters=int(out.get("info:kfgmres1_iters", -1)))
     arrays["meta"] = np.array(json.dumps(meta))
     return arrays
+
+
+def sample_sites(n: int) -> np.ndarray:
+    """The site indices a solve fixture keeps: every (n // SAMPLE_SITES)-th site."""
+    return np.arange(0, n, max(1, n // SAMPLE_SITES))
+
+
+def make_solve(name: str, cfg) -> dict:
+    ns, rows, beta, m0, seed = cfg
+    ref_runner.build(ns, ns, len(rows) + 1)
+    N = ns * ns
+    U = gauge_field(ns, ns, beta, seed)
+    b = gaussian_spinor(N, 2, seed + 1000)
+    job = dict(cycle=1, nit=0, nu1=0, nu2=2, sap_tv_iters=4, dump_hierarchy=0)
+    out = ref_runner.run(ns, ns, rows, U, b, m0=m0, timeout=4 * 3600, **job)
+    idx = sample_sites(N)
+    meta = dict(ns=ns, nt=ns, rows=rows, beta=beta, m0=m0, seed=seed, job=job,
+                iterations=int(out["info:iterations"]), true_rel_residual=out["info:true_rel_residual"],
+                setup_seconds=out["info:setup_seconds"], solve_seconds=out["info:solve_seconds"],
+                x_norm=float(np.linalg.norm(out["x"])))
+    return {"sites": idx, "x_sample": out["x"][idx], "dphi_sample": out["dphi"][idx],
+            "residual_history": out["residual_history"], "meta": np.array(json.dumps(meta))}
 
 
 def make_adjoint(name: str, cfg) -> dict:
@@ -139,6 +185,12 @@ def make_krylov(name: str, cfg) -> dict:
 
 def main(names=None):
     here = Path(__file__).resolve().parent
+    for name, cfg in SOLVES.items():
+        if names and name not in names:
+            continue
+        arrays = make_solve(name, cfg)
+        np.savez_compressed(here / f"{name}.npz", **arrays)
+        print(name, (here / f"{name}.npz").stat().st_size // 1024, "KiB")
     for name, cfg in KRYLOV.items():
         if names and name not in names:
             continue

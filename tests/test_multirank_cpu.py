@@ -55,14 +55,26 @@ def test_two_gloo_ranks_barrier_max_and_replica_seeds():
 
 
 def test_reference_rank_count(monkeypatch):
-    """The reference's CPU runs take 1..8 ranks, no more than the usable cores, and
-    AMG_REF_RANKS overrides the choice."""
+    """The reference's CPU runs take 1..8 ranks, no more than the usable cores; they start
+    before the set-up only when every rank fits in memory that way; AMG_REF_RANKS overrides
+    the count (ranks then start after the set-up)."""
     sys.path.insert(0, str(ROOT))
     import bench
     monkeypatch.delenv("AMG_REF_RANKS", raising=False)
-    n = bench.reference_ranks()
+    n, early = bench.reference_layout()
     assert 1 <= n <= min(8, len(os.sched_getaffinity(0)))
+    if early:
+        assert n * 13e9 <= 0.5 * bench.host_available_bytes()
+    # memory for every rank to run the set-up: all usable cores, started early
+    monkeypatch.setattr(bench, "host_available_bytes", lambda: int(2 * 8 * 13e9) + 1)
+    monkeypatch.setattr(bench, "host_cores", lambda: 16)
+    assert bench.reference_layout() == (8, True)
+    # memory for 3 ranks started after the set-up only (20 GB + 2 x 6 GB in half of it)
+    monkeypatch.setattr(bench, "host_available_bytes", lambda: int(2 * 32e9) + 1)
+    assert bench.reference_layout() == (3, False)
+    monkeypatch.setattr(bench, "host_available_bytes", lambda: 0)
+    assert bench.reference_layout() == (1, False)
     monkeypatch.setenv("AMG_REF_RANKS", "5")
-    assert bench.reference_ranks() == 5
+    assert bench.reference_layout() == (5, False)
     monkeypatch.setenv("AMG_REF_RANKS", "0")
-    assert bench.reference_ranks() == 1
+    assert bench.reference_layout() == (1, False)

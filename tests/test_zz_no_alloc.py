@@ -75,3 +75,42 @@ def test_restrict_noalloc_matches_context_restriction():
                                       C.c_void_p(stream.cuda_stream))
     assert rc == _lib.AMG_ERR_INVALID
     assert b"4 MiB" in lib.amg_last_error()
+
+
+def test_restrict_noalloc_few_test_vectors_many_sources():
+    """2 test vectors and 128 sources: the tiled kernel's staging (268 KB) exceeds what one
+    block may hold, so the call takes the untiled kernel and still equals the context's
+    one-source restrictions."""
+    import torch
+
+    from amg_schwingermodel_b200 import AMGContext, _lib
+    from amg_schwingermodel_b200.inputs import gauge_field
+
+    nx = nt = 64
+    N = nx * nt
+    with AMGContext(nx, nt, [[0, 4, 4, 2, 4, 4]], -0.1) as ctx:
+        ctx.set_gauge(gauge_field(nx, nt, 3.0, 33))
+        ctx.setup()
+        W = ctx.test_vectors(0)
+        bx, bt, ntest = ctx.info[1]["nx"], ctx.info[1]["nt"], ctx.info[0]["ntest"]
+        assert ntest == 2
+        v = _sources(128, N, 44)
+        want = np.stack([ctx.restrict(0, vi) for vi in v])
+
+    lib = _lib.lib()
+    dev = torch.device("cuda:0")
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream(dev)
+    Wd = torch.from_numpy(W).to(dev)
+    vd = torch.from_numpy(v).to(dev)
+    for _ in range(2):
+        out = torch.full((128, bx * bt, 2 * ntest), complex("nan"), dtype=torch.complex128, device=dev)
+        torch.cuda.synchronize(dev)
+        rc = lib.amg_restrict_raw_noalloc(C.c_void_p(Wd.data_ptr()), C.c_void_p(vd.data_ptr()),
+                                          C.c_void_p(out.data_ptr()), nx, nt, bx, bt, ntest, 128,
+                                          C.c_void_p(stream.cuda_stream))
+        assert rc == _lib.AMG_OK, lib.amg_last_error()
+        torch.cuda.synchronize(dev)
+        got = out.cpu().numpy()
+        assert np.isfinite(got).all()
+        assert rel(got, want.reshape(got.shape)) < TOL
