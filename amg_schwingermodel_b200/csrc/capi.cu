@@ -1875,7 +1875,10 @@ static int transfer0_mixed(amg_ctx c, int op, const void* in_dev, void* out_dev,
     if (nrhs < 1) return fail(AMG_ERR_INVALID, "nrhs < 1");
     if (!in_dev || !out_dev) return fail(AMG_ERR_INVALID, "null device pointer");
     CKR(select_device(c));
-    CKR(ensure_capacity(c, nrhs));
+    // only the mixed set's fine buffers (grow-only; captured cycles are dropped first when
+    // they might move)
+    if (nrhs > c->Rcap) c->drop_graphs();
+    CKR(alloc_fine<float>(c, c->f, nrhs));
     if (op == 0)
         fine_restrict<float>(c, c->f, static_cast<const float2*>(in_dev), static_cast<float2*>(out_dev), nrhs);
     else

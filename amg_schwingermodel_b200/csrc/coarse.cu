@@ -1,6 +1,9 @@
 // The coarse-level engine kernel: one CTA per source runs a whole multigrid operation
 // below the fine level (K-cycle FGMRES, cycles, SAP, coarsest GMRES) without returning
 // to the host, so the data-dependent inner iterations cost no launches or host syncs.
+#include <cstdlib>
+#include <cstring>
+
 #include "kernels.h"
 
 namespace amgb {
@@ -15,8 +18,8 @@ __device__ __forceinline__ unsigned cluster_rank() {
 // keeps its own copy of all vectors in its slab and runs the same control flow; the level
 // operators are split across the cluster.  The entry op reads `in` and (for the in/out ops)
 // `out` into slab copies, and cluster rank 0 writes the result back.
-template <typename T>
-__global__ void __launch_bounds__(kEngineThreads) k_engine(const EngArgs<T>* __restrict__ a, int op, int level,
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT) k_engine(const EngArgs<T>* __restrict__ a, int op, int level,
                                                            int nu, const cx<T>* in, long long in_stride, cx<T>* out,
                                                            long long out_stride, int csize) {
     extern __shared__ __align__(16) unsigned char smraw_e[];
@@ -60,19 +63,30 @@ __global__ void __launch_bounds__(kEngineThreads) k_engine(const EngArgs<T>* __r
     }
 }
 
-template <typename T>
-cudaError_t launch_engine_dev(const EngArgs<T>* dev_args, int op, int level, int nu, const cx<T>* in,
-                              long long in_stride, cx<T>* out, long long out_stride, int nsrc, int smem_bytes,
-                              int csize, cudaStream_t s) {
-    cudaError_t e = cudaFuncSetAttribute(k_engine<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
+// Threads per engine CTA: kEngineThreads, or 256 with AMG_ENGINE_THREADS=256 (read once per
+// process; fewer threads per CTA leave each thread more registers).
+int engine_threads() {
+    static int nt = 0;
+    if (!nt) {
+        const char* e = getenv("AMG_ENGINE_THREADS");
+        nt = (e && !strcmp(e, "256")) ? 256 : kEngineThreads;
+    }
+    return nt;
+}
+
+template <typename T, int NT>
+cudaError_t launch_engine_nt(const EngArgs<T>* dev_args, int op, int level, int nu, const cx<T>* in,
+                             long long in_stride, cx<T>* out, long long out_stride, int nsrc, int smem_bytes,
+                             int csize, cudaStream_t s) {
+    cudaError_t e = cudaFuncSetAttribute(k_engine<T, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
     if (e != cudaSuccess) return e;
     if (csize > 8) {
-        e = cudaFuncSetAttribute(k_engine<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        e = cudaFuncSetAttribute(k_engine<T, NT>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
         if (e != cudaSuccess) return e;
     }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(nsrc * csize);
-    cfg.blockDim = dim3(kEngineThreads);
+    cfg.blockDim = dim3(NT);
     cfg.dynamicSmemBytes = smem_bytes;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
@@ -82,25 +96,37 @@ cudaError_t launch_engine_dev(const EngArgs<T>* dev_args, int op, int level, int
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    e = cudaLaunchKernelEx(&cfg, k_engine<T>, dev_args, op, level, nu, in, in_stride, out, out_stride, csize);
+    e = cudaLaunchKernelEx(&cfg, k_engine<T, NT>, dev_args, op, level, nu, in, in_stride, out, out_stride, csize);
     count_launch(1);
     if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
 
+template <typename T>
+cudaError_t launch_engine_dev(const EngArgs<T>* dev_args, int op, int level, int nu, const cx<T>* in,
+                              long long in_stride, cx<T>* out, long long out_stride, int nsrc, int smem_bytes,
+                              int csize, cudaStream_t s) {
+    if (engine_threads() == 256)
+        return launch_engine_nt<T, 256>(dev_args, op, level, nu, in, in_stride, out, out_stride, nsrc, smem_bytes,
+                                        csize, s);
+    return launch_engine_nt<T, kEngineThreads>(dev_args, op, level, nu, in, in_stride, out, out_stride, nsrc,
+                                               smem_bytes, csize, s);
+}
+
 // Active clusters of `csize` engine CTAs the device can hold at once (0 when that size is
 // not schedulable).
-template <typename T>
-int engine_max_clusters(int csize, int smem_bytes) {
-    if (cudaFuncSetAttribute(k_engine<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes) != cudaSuccess)
+template <typename T, int NT>
+int engine_max_clusters_nt(int csize, int smem_bytes) {
+    if (cudaFuncSetAttribute(k_engine<T, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes) != cudaSuccess)
         return 0;
-    if (csize > 8 && cudaFuncSetAttribute(k_engine<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+    if (csize > 8 &&
+        cudaFuncSetAttribute(k_engine<T, NT>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(csize);
-    cfg.blockDim = dim3(kEngineThreads);
+    cfg.blockDim = dim3(NT);
     cfg.dynamicSmemBytes = smem_bytes;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -110,11 +136,17 @@ int engine_max_clusters(int csize, int smem_bytes) {
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     int n = 0;
-    if (cudaOccupancyMaxActiveClusters(&n, k_engine<T>, &cfg) != cudaSuccess) {
+    if (cudaOccupancyMaxActiveClusters(&n, k_engine<T, NT>, &cfg) != cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
     return n;
+}
+
+template <typename T>
+int engine_max_clusters(int csize, int smem_bytes) {
+    return engine_threads() == 256 ? engine_max_clusters_nt<T, 256>(csize, smem_bytes)
+                                   : engine_max_clusters_nt<T, kEngineThreads>(csize, smem_bytes);
 }
 
 template cudaError_t launch_engine_dev<double>(const EngArgs<double>*, int, int, int, const cx<double>*, long long,

@@ -810,6 +810,24 @@ int sm_count() {
     return v;
 }
 
+// CTAs of `func` (threads per CTA, dynamic shared memory per CTA) resident on one SM of the
+// current device, from its registers and the SM's thread, register and shared-memory limits.
+int resident_ctas(const void* func, int threads, int smem_bytes) {
+    cudaFuncAttributes fa{};
+    int dev = 0, sm_smem = 0, reserve = 0, sm_regs = 0, sm_threads = 0;
+    if (cudaFuncGetAttributes(&fa, func) != cudaSuccess || cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sm_smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&reserve, cudaDevAttrReservedSharedMemoryPerBlock, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sm_regs, cudaDevAttrMaxRegistersPerMultiprocessor, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sm_threads, cudaDevAttrMaxThreadsPerMultiProcessor, dev) != cudaSuccess)
+        return 1;
+    const int regs = ((std::max(fa.numRegs, 1) + 7) / 8) * 8;   // allocated in units of 8 per thread
+    const int by_regs = sm_regs / (regs * threads);
+    const int by_smem = sm_smem / (smem_bytes + (int)fa.sharedSizeBytes + reserve);
+    const int by_threads = sm_threads / threads;
+    return std::max(1, std::min(by_regs, std::min(by_smem, by_threads)));
+}
+
 // Largest dynamic shared memory one block may opt into on the current device, looked up once
 // per device.
 int smem_optin_bytes() {
@@ -842,7 +860,7 @@ int tc_transfer_enabled() {
 // launched) for shapes it does not take.
 template <typename T, typename TW>
 bool launch_restrict0_tc(const TW* W, const cx<T>* v, cx<T>* partial, int nx, int nt, int bx, int bt, int ntest,
-                         int nrhs, int nchunk, cudaStream_t s, cudaError_t* err) {
+                         int nrhs, int nchunk, cudaStream_t s, cudaError_t* err, int* used_chunks) {
     if constexpr (!std::is_same<T, float>::value || !std::is_same<TW, __nv_bfloat162>::value) {
         return false;
     } else {
@@ -850,21 +868,40 @@ bool launch_restrict0_tc(const TW* W, const cx<T>* v, cx<T>* partial, int nx, in
         if (!tc_transfer_enabled() || te % kRtcSites || ntest < 1 || ntest > 32 || nrhs < 1 || nrhs > 256 ||
             nblk > 65535 || nchunk < 1)
             return false;
-        const int NP = (nrhs + 15) / 16 * 16;
-        dim3 grid(nchunk, nblk);
-        if (ntest <= 16) {
-            const int bytes = rtc_smem_bytes(64, NP);
-            if (bytes > smem_optin_bytes()) return false;
-            *err = cudaFuncSetAttribute(k_restrict0_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-            if (*err != cudaSuccess) return true;
-            k_restrict0_tc<64><<<grid, 128, bytes, s>>>(W, v, partial, nx, nt, bt, xe, te, nchunk, ntest, nrhs, NP);
+        const int N = nx * nt;
+        // 32-bit offsets inside the kernel
+        if ((long long)std::max(nrhs, ntest) * N * 2 >= (1ll << 31)) return false;
+        // NP padded sources: a power of two >= 16; NB = NP sources x kRtcSites sites / kTcThreads
+        int NP = 16;
+        while (NP < nrhs) NP *= 2;
+        const int M = ntest <= 16 ? 64 : 128, NB = NP * kRtcSites / kTcThreads;
+        const int nd = rtc_ring(M, NP, smem_optin_bytes());
+        if (nd == 0) return false;
+        const int bytes = rtc_smem_bytes(M, NP, nd);
+        // one wave: as many chunks per block as the resident CTAs allow (at most the caller's
+        // chunk count, which sizes the partial-sum buffer)
+        auto go = [&](auto kern) {
+            *err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+            if (*err != cudaSuccess) return;
+            const int per_sm = resident_ctas(reinterpret_cast<const void*>(kern), kTcThreads, bytes);
+            *used_chunks = std::max(1, std::min(nchunk, per_sm * sm_count() / nblk));
+            dim3 g(*used_chunks, nblk);
+            kern<<<g, kTcThreads, bytes, s>>>(W, v, partial, nx, nt, bt, xe, te, *used_chunks, ntest, nrhs, nd);
+        };
+        if (M == 64) {
+            if (NB == 1) go(k_restrict0_tc<64, 1>);
+            else if (NB == 2) go(k_restrict0_tc<64, 2>);
+            else if (NB == 4) go(k_restrict0_tc<64, 4>);
+            else if (NB == 8) go(k_restrict0_tc<64, 8>);
+            else go(k_restrict0_tc<64, 16>);
         } else {
-            const int bytes = rtc_smem_bytes(128, NP);
-            if (bytes > smem_optin_bytes()) return false;
-            *err = cudaFuncSetAttribute(k_restrict0_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-            if (*err != cudaSuccess) return true;
-            k_restrict0_tc<128><<<grid, 128, bytes, s>>>(W, v, partial, nx, nt, bt, xe, te, nchunk, ntest, nrhs, NP);
+            if (NB == 1) go(k_restrict0_tc<128, 1>);
+            else if (NB == 2) go(k_restrict0_tc<128, 2>);
+            else if (NB == 4) go(k_restrict0_tc<128, 4>);
+            else if (NB == 8) go(k_restrict0_tc<128, 8>);
+            else go(k_restrict0_tc<128, 16>);
         }
+        if (*err != cudaSuccess) return true;
         *err = cudaPeekAtLastError();
         return true;
     }
@@ -878,9 +915,10 @@ cudaError_t launch_restrict0(const TW* W, const cx<T>* v, cx<T>* out, cx<T>* par
     dim3 grid(nchunk, nblk);
     dim3 g2((nblk * 2 * ntest + 127) / 128, nrhs);
     cudaError_t tce = cudaSuccess;
-    if (launch_restrict0_tc<T, TW>(W, v, partial, nx, nt, bx, bt, ntest, nrhs, nchunk, s, &tce)) {
+    int tc_chunks = nchunk;
+    if (launch_restrict0_tc<T, TW>(W, v, partial, nx, nt, bx, bt, ntest, nrhs, nchunk, s, &tce, &tc_chunks)) {
         if (tce != cudaSuccess) return tce;
-        k_restrict0_sum<T><<<g2, 128, 0, s>>>(partial, out, nblk, nchunk, 2 * ntest);
+        k_restrict0_sum<T><<<g2, 128, 0, s>>>(partial, out, nblk, tc_chunks, 2 * ntest);
         return cudaPeekAtLastError();
     }
     // the tiled kernel when its output tiles fit one CTA and its staging fits the device's
@@ -915,15 +953,17 @@ void launch_prolong0_add(const TW* W, const cx<T>* vc, cx<T>* psi, int nx, int n
     const int xe = nx / bx, te = nt / bt;
     if constexpr (std::is_same<T, float>::value && std::is_same<TW, __nv_bfloat162>::value) {
         // tensor cores: 32-site tiles along t, several CTAs per aggregation block
-        const int nblk = bx * bt, NP = (nrhs + 15) / 16 * 16;
+        const int nblk = bx * bt, NP = (nrhs + 31) / 32 * 32;   // two halves of 16-column batches
         const int bytes = ptc_smem_bytes(ntest, NP);
-        if (tc_transfer_enabled() && te % kPtcSites == 0 && ntest >= 1 && ntest <= 32 && nrhs >= 1 && nrhs <= 256 &&
+        if (tc_transfer_enabled() && te % kPtcSites == 0 && ntest >= 1 && ntest <= 32 && nrhs >= 1 && nrhs <= 128 &&
             nblk <= 65535 && bytes <= smem_optin_bytes() &&
             cudaFuncSetAttribute(k_prolong0_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) == cudaSuccess) {
+            // one wave of CTAs over the aggregation blocks
+            const int per_sm = resident_ctas(reinterpret_cast<const void*>(k_prolong0_tc), kTcThreads, bytes);
             const int tiles = xe * (te / kPtcSites);
-            const int nsplit = std::max(1, std::min(tiles, (4 * sm_count() + nblk - 1) / nblk));
+            const int nsplit = std::max(1, std::min(tiles, per_sm * sm_count() / nblk));
             dim3 grid(nsplit, nblk);
-            k_prolong0_tc<<<grid, 128, bytes, s>>>(W, vc, psi, nx, nt, bt, xe, te, ntest, nblk, nrhs, NP, nsplit);
+            k_prolong0_tc<<<grid, kTcThreads, bytes, s>>>(W, vc, psi, nx, nt, bt, xe, te, ntest, nblk, nrhs, NP, nsplit);
             return;
         }
     }

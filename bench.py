@@ -4,7 +4,7 @@ residual <= 1e-10 (4 levels, Nv = 16, beta = 4, m0 = -0.05), mixed precision wit
 sources against the plain FP64 drop-in, plus the fine D-apply bandwidth.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--rhs R] [--precision mixed|f64] [--no-cpu] [--no-extras]
+                    [--rhs R] [--precision mixed|f64] [--no-cpu] [--no-extras] [--transfers]
 
 One step = one batched solve of R seeded complex-Gaussian sources on one seeded gauge
 field per GPU (inputs resident in HBM; the working set of a step is far above the 126 MB
@@ -423,6 +423,60 @@ def line_uneven_batch(local, steps):
                       "returns after every context's solve has finished)"}
 
 
+def run_transfers(args, local):
+    """The mixed form's level-0 transfers alone at the benchmark's shape (1024^2, 8x8
+    aggregation blocks of 128x128 sites, 16 test vectors, R sources): restriction and
+    prolongation through amg_restrict0_mixed_dev / amg_prolong0_mixed_dev on device buffers,
+    warm-up then timed launches with CUDA events on the context's stream; a few GB on the
+    device (no solve buffers), the size an ncu capture of these kernels takes."""
+    import ctypes as C
+
+    import torch
+
+    from amg_schwingermodel_b200 import AMGContext, _lib
+    from amg_schwingermodel_b200.inputs import gauge_field
+    torch.cuda.set_device(local)
+    R, N = args.rhs, NX * NT
+    ctx = AMGContext(NX, NT, ROWS, M0, precision=1, max_rhs=R, device=local)
+    ctx.set_gauge(gauge_field(NX, NT, BETA, replica_seeds(0)[0]))
+    ctx.setup()
+    nblk, ntest = ROWS[0][1] * ROWS[0][2], ROWS[0][3]
+    g = torch.Generator(device=f"cuda:{local}").manual_seed(3)
+    v = torch.randn(R, N, 2, dtype=torch.complex64, device=f"cuda:{local}", generator=g)
+    vc = torch.randn(R, nblk, 2 * ntest, dtype=torch.complex64, device=f"cuda:{local}", generator=g)
+    out = torch.empty_like(vc)
+    psi = torch.zeros_like(v)
+    lib = _lib.lib()
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    hbm, kind = peaks()
+    res = {}
+    for name, fn, a, b, nbytes in (
+            ("restrict", lib.amg_restrict0_mixed_dev, v, out, ntest * N * 2 * 4 + R * N * 2 * 8 + R * nblk * 2 * ntest * 8),
+            ("prolong", lib.amg_prolong0_mixed_dev, vc, psi, ntest * N * 2 * 4 + 2 * R * N * 2 * 8)):
+        def call():
+            rc = fn(ctx._h, C.c_void_p(a.data_ptr()), C.c_void_p(b.data_ptr()), R)
+            if rc != 0:
+                raise RuntimeError(f"{name}: {lib.amg_last_error()}")
+        for _ in range(3):
+            call()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        # each call synchronises its stream, so the events bracket the launches alone
+        ms = 0.0
+        for _ in range(args.steps):
+            e0.record(stream)
+            call()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms += e0.elapsed_time(e1)
+        ms /= args.steps
+        res[name] = {"ms_per_launch": ms, "algorithmic_bytes": nbytes, "gbs": nbytes / (ms * 1e-3) / 1e9,
+                     "frac": nbytes / (ms * 1e-3) / 1e9 / hbm}
+    ctx.close()
+    print(json.dumps({"kernels": "level-0 transfers, mixed form", "tensor_cores": os.environ.get("AMG_TC_TRANSFER", "1") != "0",
+                      "lattice": [NX, NT], "nrhs": R, "ntest": ntest, "peak_gbs": hbm, "peak": kind, **res}))
+
+
 def run_ours(args, world, rank, local):
     import torch
 
@@ -647,10 +701,14 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the side lines (FP64 batch, reference rows, 256^2, uneven batch)")
+    ap.add_argument("--transfers", action="store_true",
+                    help="time the mixed form's level-0 restriction and prolongation alone (no solve)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
         run_reference(args, world, rank)
+    elif args.transfers:
+        run_transfers(args, local)
     else:
         run_ours(args, world, rank, local)
     if world > 1:

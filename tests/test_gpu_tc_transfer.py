@@ -6,8 +6,9 @@ vectors and FP32 sources.
 
 Bars: the CUDA-core kernels multiply in FP32, 1e-5 relative; the tensor cores read their
 inputs as TF32 (10 mantissa bits), 2e-3 relative.  Shapes: 12 and 20 test vectors (64- and
-128-row accumulators), 1 to 40 sources (the source count padded to 16 inside), aggregation
-blocks of 32x32 and 16x32 sites.  Each configuration runs in its own process (the kernel
+128-row accumulators), 1 to 40 sources (the source count padded inside), aggregation
+blocks of 32x32 and 16x32 sites, and 8x8-site blocks, whose 8-site rows the tensor-core
+kernels do not tile (the CUDA-core kernels run).  Each configuration runs in its own process (the kernel
 choice is read from the environment once per process).
 """
 import json
@@ -49,7 +50,8 @@ for nx, nt, rows, nrhs in {cases!r}:
         v = (rng.standard_normal((nrhs, N, 2)) + 1j * rng.standard_normal((nrhs, N, 2))).astype(np.complex64)
         vc = (rng.standard_normal((nrhs, nblk, 2 * ntest)) + 1j * rng.standard_normal((nrhs, nblk, 2 * ntest))).astype(np.complex64)
         psi0 = (rng.standard_normal((nrhs, N, 2)) + 1j * rng.standard_normal((nrhs, N, 2))).astype(np.complex64)
-        # numpy: out[r][b][2k+s] = sum_{n in b} conj(W[k][n][s]) v[r][n][s]; psi[r][n][s] += sum_k W[k][n][s] vc[r][b(n)][2k+s]
+        # numpy: out[r][b][2k+s] = sum over n in b of conj(W[k][n][s]) v[r][n][s];
+        # psi[r][n][s] += sum over k of W[k][n][s] vc[r][b(n)][2k+s]
         want_r = np.zeros((nrhs, nblk, 2 * ntest), np.complex128)
         for k in range(ntest):
             for s in range(2):
@@ -81,7 +83,7 @@ print("RESULT" + json.dumps(out))
 
 CASES = [(128, 128, [[0, 4, 4, 12, 4, 4]], 32), (128, 128, [[0, 4, 4, 12, 4, 4]], 1),
          (128, 128, [[0, 4, 4, 20, 4, 4]], 5), (64, 128, [[0, 4, 4, 12, 2, 4], [1, 2, 2, 8, 2, 2]], 40),
-         (64, 64, [[0, 2, 2, 16, 2, 2]], 17)]
+         (64, 64, [[0, 2, 2, 16, 2, 2]], 17), (64, 64, [[0, 8, 8, 12, 2, 2]], 9)]
 
 
 @pytest.mark.parametrize("tc", [1, 0])
