@@ -26,6 +26,9 @@ AMG_CYCLE_K = 1
 AMG_PRECOND_MG = 0
 AMG_PRECOND_SAP = 1
 AMG_PRECOND_NONE = 2
+AMG_LINKS_F32 = 0
+AMG_LINKS_BF16 = 1
+AMG_LINKS_F16 = 2
 
 
 class AmgParams(C.Structure):
@@ -35,7 +38,7 @@ class AmgParams(C.Structure):
         ("sap_tol", C.c_double), ("kcycle_m", C.c_int), ("kcycle_restarts", C.c_int), ("kcycle_tol", C.c_double),
         ("coarse_m", C.c_int), ("coarse_restarts", C.c_int), ("coarse_tol", C.c_double), ("outer_m", C.c_int),
         ("outer_restarts", C.c_int), ("outer_tol", C.c_double), ("precision", C.c_int), ("max_rhs", C.c_int),
-        ("tv_seed", C.c_ulonglong), ("autotune", C.c_int),
+        ("tv_seed", C.c_ulonglong), ("autotune", C.c_int), ("link_storage", C.c_int),
     ]
 
 

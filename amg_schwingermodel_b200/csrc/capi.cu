@@ -516,6 +516,20 @@ int restrict_chunks(amg_context* c, int R) {
     return std::max(1, std::min(std::max(1, spb / 128), (1184 + nblk - 1) / nblk));
 }
 
+// The fine links of a precision set as its kernels read them: FP64, or in the mixed form FP32,
+// BF16 or FP16 pairs (amg_params.link_storage)
+template <typename T>
+Links<T> fine_links(amg_context* c, PrecSet<T>& ps) {
+    if constexpr (sizeof(T) == 8) {
+        (void)c;
+        return Links<T>(ps.U.template as<cx<T>>());
+    } else {
+        return Links<T>(ps.U.p, c->p.link_storage == AMG_LINKS_BF16 ? LINK_BF16
+                                : c->p.link_storage == AMG_LINKS_F16 ? LINK_F16
+                                                                     : LINK_NATIVE);
+    }
+}
+
 template <typename T>
 void fine_restrict(amg_context* c, PrecSet<T>& ps, const cx<T>* v, cx<T>* out, int R) {
     const LevelHost& h0 = c->lv[0];
@@ -566,7 +580,7 @@ int fine_sap(amg_context* c, PrecSet<T>& ps, const cx<T>* v, long long vstride, 
     double* norm2 = vnorm2 + c->Rcap;
     double* partial = c->partial.as<double>();
     cx<T>* r = ps.sap_r.template as<cx<T>>();
-    const cx<T>* U = ps.U.template as<cx<T>>();
+    const Links<T> U = fine_links<T>(c, ps);
     const T m0 = (T)c->m0;
     k_set_int<<<1, 256, 0, c->stream>>>(act, 1, R);
     k_set_int<<<1, 256, 0, c->stream>>>(conv, 0, R);
@@ -633,7 +647,7 @@ int fine_cycle(amg_context* c, PrecSet<T>& ps, const cx<T>* eta, cx<T>* psi, int
     }
     const cx<T>* r = eta;
     if (!psi_zero) {
-        launch_residual<T>(ps.U.template as<cx<T>>(), eta, len, psi, ps.r0.template as<cx<T>>(), c->nx, c->nt, R,
+        launch_residual<T>(fine_links<T>(c, ps), eta, len, psi, ps.r0.template as<cx<T>>(), c->nx, c->nt, R,
                            (T)c->m0, nullptr, nullptr, nullptr, c->stream);
         r = ps.r0.template as<cx<T>>();
     }
@@ -1173,8 +1187,17 @@ int orthonormalize(amg_context* c, int l) {
 int build_mixed(amg_context* c) {
     PrecSet<float>& f = c->f;
     const long long len = vlen0(c);
-    CKR(f.U.alloc((size_t)len * sizeof(float2)));
-    launch_d2f(f.U.as<float2>(), c->d.U.as<double2>(), len, c->stream);
+    // fine links: FP32, or BF16 / FP16 pairs (amg_params.link_storage)
+    if (c->p.link_storage == AMG_LINKS_BF16) {
+        CKR(f.U.alloc((size_t)len * sizeof(__nv_bfloat162)));
+        launch_d2bf(f.U.as<__nv_bfloat162>(), c->d.U.as<double2>(), len, c->stream);
+    } else if (c->p.link_storage == AMG_LINKS_F16) {
+        CKR(f.U.alloc((size_t)len * sizeof(__half2)));
+        launch_d2h(f.U.as<__half2>(), c->d.U.as<double2>(), len, c->stream);
+    } else {
+        CKR(f.U.alloc((size_t)len * sizeof(float2)));
+        launch_d2f(f.U.as<float2>(), c->d.U.as<double2>(), len, c->stream);
+    }
     const LevelHost& h0 = c->lv[0];
     CKR(f.W0.alloc((size_t)h0.ntest * len * sizeof(__nv_bfloat162)));
     launch_d2bf(f.W0.as<__nv_bfloat162>(), c->d.W0.as<double2>(), h0.ntest * len, c->stream);
@@ -1380,6 +1403,7 @@ void amg_params_default(amg_params* p) {
     p->max_rhs = 1;
     p->tv_seed = 0;
     p->autotune = 1;
+    p->link_storage = AMG_LINKS_F16;
 }
 
 int amg_read_parameters(const char* path, int* rows, int max_rows, int* nrows) {
@@ -1409,6 +1433,8 @@ int amg_create(amg_ctx* out, int nx, int nt, int levels, const int* rows, double
         return fail(AMG_ERR_INVALID, "restart counts must be >= 1");
     if (p.precision != AMG_PREC_F64 && p.precision != AMG_PREC_MIXED) return fail(AMG_ERR_INVALID, "precision");
     if (p.cycle != AMG_CYCLE_K && p.cycle != AMG_CYCLE_V) return fail(AMG_ERR_INVALID, "cycle");
+    if (p.link_storage != AMG_LINKS_F32 && p.link_storage != AMG_LINKS_BF16 && p.link_storage != AMG_LINKS_F16)
+        return fail(AMG_ERR_INVALID, "link_storage");
     if (p.max_rhs < 1) p.max_rhs = 1;
     std::vector<LevelHost> lv;
     CKR(build_levels(nx, nt, levels, rows, lv));

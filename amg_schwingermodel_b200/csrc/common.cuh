@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <stdint.h>
 #include <cstdio>
 
@@ -66,6 +67,24 @@ template <typename To, typename From> __host__ __device__ __forceinline__ cx<To>
 __device__ __forceinline__ float2 load_cx(const __nv_bfloat162* p) { return __bfloat1622float2(*p); }
 __device__ __forceinline__ float2 load_cx(const float2* p) { return *p; }
 __device__ __forceinline__ double2 load_cx(const double2* p) { return *p; }
+
+// Fine-lattice links U[N][2] as a kernel reads them: cx<T> (the FP64 set, and the FP32 copy of
+// the mixed form) or, in the mixed form, BF16 or FP16 pairs; element i converts to cx<T>.
+enum { LINK_NATIVE = 0, LINK_BF16 = 1, LINK_F16 = 2 };
+template <typename T>
+struct Links {
+    const void* p;
+    int fmt;
+    __host__ __device__ Links(const cx<T>* q) : p(q), fmt(LINK_NATIVE) {}
+    __host__ __device__ Links(const void* q, int f) : p(q), fmt(f) {}
+    __device__ __forceinline__ cx<T> operator[](long long i) const {
+        if constexpr (sizeof(T) == 4) {
+            if (fmt == LINK_BF16) return __bfloat1622float2(static_cast<const __nv_bfloat162*>(p)[i]);
+            if (fmt == LINK_F16) return __half22float2(static_cast<const __half2*>(p)[i]);
+        }
+        return static_cast<const cx<T>*>(p)[i];
+    }
+};
 
 // ---------------------------------------------------------------------------------
 // reductions

@@ -60,7 +60,7 @@ __global__ void __launch_bounds__(256) k_dirac_promote(const double2* __restrict
 // r = b - D x, and per-CTA partial sums of |r|^2 (deterministic second stage); sources
 // grouped per thread as in k_dirac.  Inactive sources (act[rhs] == 0) are skipped.
 template <typename T>
-__global__ void __launch_bounds__(256) k_residual(const cx<T>* __restrict__ U, const cx<T>* __restrict__ b,
+__global__ void __launch_bounds__(256) k_residual(const Links<T> U, const cx<T>* __restrict__ b,
                                                   long long bstride, const cx<T>* __restrict__ x,
                                                   cx<T>* __restrict__ r, int nx, int nt, T m0,
                                                   double* __restrict__ partial, const int* __restrict__ act,
@@ -440,7 +440,7 @@ __device__ void fine_block_apply(const FineBlock<T>& B, const cx<T>* in, cx<T>* 
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_sap0_blocks(const cx<T>* __restrict__ U, const cx<T>* __restrict__ r,
+__global__ void __launch_bounds__(256) k_sap0_blocks(const Links<T> U, const cx<T>* __restrict__ r,
                                                      cx<T>* __restrict__ x, const int* __restrict__ blocks, int ncol,
                                                      int nx, int nt, int sbt, int sxe, int ste, T m0, int m,
                                                      int restarts, T tol, int use_smem, cx<T>* gscratch,
@@ -656,6 +656,10 @@ __global__ void k_f2d(double2* __restrict__ y, const float2* __restrict__ x, lon
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
         y[e] = make_double2((double)x[e].x, (double)x[e].y);
 }
+__global__ void k_d2h(__half2* __restrict__ y, const double2* __restrict__ x, long long n) {
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+        y[e] = __floats2half2_rn((float)x[e].x, (float)x[e].y);
+}
 __global__ void k_d2bf(__nv_bfloat162* __restrict__ y, const double2* __restrict__ x, long long n) {
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
         y[e] = __floats2bfloat162_rn((float)x[e].x, (float)x[e].y);
@@ -754,7 +758,7 @@ void launch_dirac_promote(const double2* U, const float2* in, double2* out, doub
 }
 
 template <typename T>
-void launch_residual(const cx<T>* U, const cx<T>* b, long long bstride, const cx<T>* x, cx<T>* r, int nx, int nt,
+void launch_residual(const Links<T> U, const cx<T>* b, long long bstride, const cx<T>* x, cx<T>* r, int nx, int nt,
                      int nrhs, T m0, double* partial, double* norm2_out, const int* act, cudaStream_t s) {
     count_launch(norm2_out ? 2 : 1);
     const int nblk = (nx * nt + 255) / 256;
@@ -981,7 +985,7 @@ int sap0_smem_bytes(int S, int m, int use_smem) {
 }
 
 template <typename T, int SPT, int NW>
-cudaError_t launch_sap0_lean(const cx<T>* U, const cx<T>* r, cx<T>* x, const int* blocks, int ncol, int nrhs, int nx,
+cudaError_t launch_sap0_lean(const Links<T> U, const cx<T>* r, cx<T>* x, const int* blocks, int ncol, int nrhs, int nx,
                              int nt, int sbt, int sxe, int ste, T m0, int restarts, T tol, int* iters, const int* act,
                              cudaStream_t s) {
     const int bytes = sap0_lean_smem<T, 5, SPT, NW>();
@@ -1014,7 +1018,7 @@ static int sap0_f32_enabled() {
 }
 
 template <int SPT, int NW>
-cudaError_t launch_sap0_ca(const float2* U, const float2* r, float2* x, const int* blocks, int ncol, int nrhs, int nx,
+cudaError_t launch_sap0_ca(const Links<float> U, const float2* r, float2* x, const int* blocks, int ncol, int nrhs, int nx,
                            int nt, int sbt, int sxe, int ste, float m0, int restarts, float tol, int* iters,
                            const int* act, cudaStream_t s) {
     const int bytes = sap0_ca_smem<SPT, NW>();
@@ -1027,7 +1031,7 @@ cudaError_t launch_sap0_ca(const float2* U, const float2* r, float2* x, const in
 }
 
 template <int SPT, int NW, bool CGS = false>
-cudaError_t launch_sap0_f32(const float2* U, float2* r, float2* x, const int* blocks, int ncol, int nrhs, int nx,
+cudaError_t launch_sap0_f32(const Links<float> U, float2* r, float2* x, const int* blocks, int ncol, int nrhs, int nx,
                             int nt, int sbt, int sxe, int ste, float m0, int restarts, float tol, int* iters,
                             const int* act, cudaStream_t s, const float2* vsrc, long long vstride) {
     const int bytes = sap0_f32_smem<5, SPT, NW, CGS>();
@@ -1040,7 +1044,7 @@ cudaError_t launch_sap0_f32(const float2* U, float2* r, float2* x, const int* bl
 }
 
 // FP32 solves of 64- to 1024-site blocks take the paired-FP32 kernel.
-static cudaError_t launch_sap0_paired(const float2* U, float2* r, float2* x, const int* blocks, int ncol,
+static cudaError_t launch_sap0_paired(const Links<float> U, float2* r, float2* x, const int* blocks, int ncol,
                                       int nrhs, int nx, int nt, int sbt, int sxe, int ste, float m0, int restarts,
                                       float tol, int* iters, const int* act, cudaStream_t s, bool* done, int v,
                                       const float2* vsrc, long long vstride) {
@@ -1101,7 +1105,7 @@ static cudaError_t launch_sap0_paired(const float2* U, float2* r, float2* x, con
 // kernel (sap_f32.cuh) in FP32 and the lean kernel (sap_lean.cuh) in FP64; any other shape
 // or restart length takes the generic kernel above.
 template <typename T>
-cudaError_t launch_sap0(const cx<T>* U, cx<T>* r, cx<T>* x, const int* blocks, int ncol, int nrhs, int nx,
+cudaError_t launch_sap0(const Links<T> U, cx<T>* r, cx<T>* x, const int* blocks, int ncol, int nrhs, int nx,
                         int nt, int sbt, int sxe, int ste, T m0, int m, int restarts, T tol, int use_smem,
                         cx<T>* gscratch, int* iters, const int* act, cudaStream_t s, int variant, const cx<T>* vfuse,
                         long long vstride) {
@@ -1220,6 +1224,8 @@ void launch_d2f(float2* y, const double2* x, long long n, cudaStream_t s) {
     count_launch(1); k_d2f<<<592, 256, 0, s>>>(y, x, n); }
 void launch_f2d(double2* y, const float2* x, long long n, cudaStream_t s) {
     count_launch(1); k_f2d<<<592, 256, 0, s>>>(y, x, n); }
+void launch_d2h(__half2* y, const double2* x, long long n, cudaStream_t s) {
+    count_launch(1); k_d2h<<<592, 256, 0, s>>>(y, x, n); }
 void launch_d2bf(__nv_bfloat162* y, const double2* x, long long n, cudaStream_t s) {
     count_launch(1); k_d2bf<<<592, 256, 0, s>>>(y, x, n); }
 
@@ -1288,11 +1294,11 @@ void launch_force(const double2* U, const double2* lam, const double2* x, double
 
 #define INST(T)                                                                                                 \
     template void launch_dirac<T>(const cx<T>*, const cx<T>*, cx<T>*, int, int, int, T, int, cudaStream_t);     \
-    template void launch_residual<T>(const cx<T>*, const cx<T>*, long long, const cx<T>*, cx<T>*, int, int, int, T,\
+    template void launch_residual<T>(const Links<T>, const cx<T>*, long long, const cx<T>*, cx<T>*, int, int, int, T,\
                                      double*, double*, const int*, cudaStream_t);                                \
     template void launch_norm2<T>(const cx<T>*, long long, long long, int, double*, double*, cudaStream_t);      \
     template int sap0_smem_bytes<T>(int, int, int);                                                              \
-    template cudaError_t launch_sap0<T>(const cx<T>*, cx<T>*, cx<T>*, const int*, int, int, int, int, int, \
+    template cudaError_t launch_sap0<T>(const Links<T>, cx<T>*, cx<T>*, const int*, int, int, int, int, int, \
                                         int, int, T, int, int, T, int, cx<T>*, int*, const int*, cudaStream_t, int, \
                                         const cx<T>*, long long);
 INST(double)

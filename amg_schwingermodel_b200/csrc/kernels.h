@@ -24,7 +24,7 @@ int fine_error_check(cudaStream_t s);
 // runs the bulk-copy D apply with waits that cannot complete and returns the device flag
 int dirac_tma_wait_test(const double2* U, const double2* in, double2* out, int nx, int nt, int nrhs, cudaStream_t s);
 template <typename T>
-void launch_residual(const cx<T>* U, const cx<T>* b, long long bstride, const cx<T>* x, cx<T>* r, int nx, int nt,
+void launch_residual(const Links<T> U, const cx<T>* b, long long bstride, const cx<T>* x, cx<T>* r, int nx, int nt,
                      int nrhs, T m0, double* partial, double* norm2_out, const int* act, cudaStream_t s);
 template <typename T>
 void launch_norm2(const cx<T>* v, long long len, long long stride, int nrhs, double* partial, double* out,
@@ -49,7 +49,7 @@ template <typename T>
 // vfuse (optional): the SAP right-hand side v; r = v - D x is then formed for the colour's
 // blocks inside the launch (in a separate residual launch where the chosen kernel cannot)
 // and r is written there, instead of r being read as given
-cudaError_t launch_sap0(const cx<T>* U, cx<T>* r, cx<T>* x, const int* blocks, int ncol, int nrhs, int nx,
+cudaError_t launch_sap0(const Links<T> U, cx<T>* r, cx<T>* x, const int* blocks, int ncol, int nrhs, int nx,
                         int nt, int sbt, int sxe, int ste, T m0, int m, int restarts, T tol, int use_smem,
                         cx<T>* gscratch, int* iters, const int* act, cudaStream_t s, int variant = -1,
                         const cx<T>* vfuse = nullptr, long long vstride = 0);
@@ -71,6 +71,7 @@ void launch_axpy_scale_to(double2* y, const double2* w, const double2* V, long l
 void launch_scale(double2* y, const double2* x, long long len, const double* sc, const int* act, int nrhs,
                   cudaStream_t s, float2* yf = nullptr);
 void launch_d2f(float2* y, const double2* x, long long n, cudaStream_t s);
+void launch_d2h(__half2* y, const double2* x, long long n, cudaStream_t s);
 void launch_f2d(double2* y, const float2* x, long long n, cudaStream_t s);
 void launch_d2bf(__nv_bfloat162* y, const double2* x, long long n, cudaStream_t s);
 

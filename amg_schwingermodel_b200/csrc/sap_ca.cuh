@@ -84,7 +84,7 @@ __device__ __forceinline__ float psum1_ca(float a, float2* part, int& buf) {
 }
 
 template <int SPT, int NW>
-__global__ void __launch_bounds__(32 * NW, 2) k_sap0_ca(const float2* __restrict__ U, const float2* __restrict__ r,
+__global__ void __launch_bounds__(32 * NW, 2) k_sap0_ca(const Links<float> U, const float2* __restrict__ r,
                                                          float2* __restrict__ xg, const int* __restrict__ blocks,
                                                          int ncol, int nx, int nt, int sbt, int sxe, int ste, float m0,
                                                          int restarts, float tol, const int* __restrict__ act,

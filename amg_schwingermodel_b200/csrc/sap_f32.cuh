@@ -157,7 +157,7 @@ template <int M, int NW, bool CGS>
 constexpr int sap0_f32_pst() { return CGS ? NW * (M + 2) : NW * 2; }
 
 template <int M, int SPT, int NW, bool CGS = false>
-__global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const float2* __restrict__ U, float2* __restrict__ r,
+__global__ void __launch_bounds__(32 * NW, 2) k_sap0_f32(const Links<float> U, float2* __restrict__ r,
                                                           float2* __restrict__ xg, const int* __restrict__ blocks,
                                                           int ncol, int nx, int nt, int sbt, int sxe, int ste, float m0,
                                                           int restarts, float tol, const int* __restrict__ act,

@@ -50,7 +50,7 @@ __device__ __forceinline__ void lean_sync() {
 }
 
 template <typename T, int M, int SPT, int NW>
-__global__ void __launch_bounds__(32 * NW, (sizeof(T) == 4 ? 16 : 8) / NW) k_sap0_lean(const cx<T>* __restrict__ U, const cx<T>* __restrict__ r,
+__global__ void __launch_bounds__(32 * NW, (sizeof(T) == 4 ? 16 : 8) / NW) k_sap0_lean(const Links<T> U, const cx<T>* __restrict__ r,
                                                        cx<T>* __restrict__ xg, const int* __restrict__ blocks,
                                                        int ncol, int nx, int nt, int sbt, int sxe, int ste, T m0,
                                                        int restarts, T tol, const int* __restrict__ act,

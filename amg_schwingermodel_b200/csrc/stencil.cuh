@@ -25,8 +25,8 @@ struct SiteOp {
     T sR, sL;                  // antiperiodic signs of the two time hops
 };
 
-template <typename T>
-__device__ __forceinline__ SiteOp<T> site_op(const cx<T>* __restrict__ U, int n, int nx, int nt) {
+template <typename T, typename UA>
+__device__ __forceinline__ SiteOp<T> site_op(const UA& U, int n, int nx, int nt) {
     SiteOp<T> o;
     const int x = n / nt, t = n - x * nt;
     o.r0 = x * nt + ((t + 1 == nt) ? 0 : t + 1);

@@ -44,6 +44,10 @@ extern "C" {
 #define AMG_PREC_MIXED 1         /* FP32 cycle (SAP, P, P^dagger, coarse levels) with BF16
                                     test vectors inside the FP64 outer FGMRES */
 
+#define AMG_LINKS_F32 0          /* amg_params.link_storage: fine links of the mixed cycle */
+#define AMG_LINKS_BF16 1
+#define AMG_LINKS_F16 2
+
 #define AMG_CYCLE_V 0            /* AMGV::cycle = 0 (include/variables.h:64) */
 #define AMG_CYCLE_K 1
 
@@ -81,6 +85,10 @@ typedef struct amg_params {
     int autotune;              /* 1 (default): the first solve of a context times the fine SAP
                                   kernel variants and the coarse-engine cluster sizes on its own
                                   data and keeps the fastest; 0: fixed defaults */
+    int link_storage;          /* mixed form: storage of the fine links its cycle reads,
+                                  AMG_LINKS_F16 (default: unit-modulus links in 10 mantissa bits),
+                                  AMG_LINKS_BF16 or AMG_LINKS_F32 (FP32 arithmetic either way);
+                                  the FP64 operator keeps FP64 links */
 } amg_params;
 
 /* Per-source result of a solve. */
