@@ -246,7 +246,7 @@ def run_reference(args, world, rank):
     """The reference's own CPU code on this workload: its complete set-up (test-vector
     smoothing included, as FGMRES_AMG's constructor runs it), then complete FGMRES_AMG solves
     from x0 = 0: one untimed, then up to `steps` timed, stopping early once another solve
-    would exceed the time budget (AMG_REF_SOLVE_BUDGET_S, default 240 s).  solves/s = timed
+    would exceed the time budget (AMG_REF_SOLVE_BUDGET_S, default 150 s).  solves/s = timed
     solves / their summed time."""
     if rank != 0:
         return
@@ -258,7 +258,7 @@ def run_reference(args, world, rank):
     gseed, bseed = replica_seeds(0)
     U = gauge_field(NX, NT, BETA, gseed)
     b0 = gaussian_spinor(NX * NT, 2, bseed)
-    budget = float(os.environ.get("AMG_REF_SOLVE_BUDGET_S", "240"))
+    budget = float(os.environ.get("AMG_REF_SOLVE_BUDGET_S", "150"))
     ranks, early = reference_layout()
     t0 = time.time()
     out, ranks = run_reference_job(ranks, early, gauge=U, rhs=b0, m0=M0, solve=1, dump_hierarchy=0, dphi_reps=20,
