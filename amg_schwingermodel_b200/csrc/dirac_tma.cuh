@@ -71,13 +71,21 @@ __host__ __device__ constexpr int dirac_tma_smem() { return 2 * dirac_tma_buf_by
 // TIN: the spinors' storage type (T, or float for FP32 spinors into the FP64 operator); COPY:
 // also write the promoted input to in_copy; SELF_TEST: issue no copies at all and poll 256
 // times per wait, so the first wait runs out with nothing in flight (the bounded-wait
-// self-test)
-template <typename T, bool DAG, typename TIN = T, bool COPY = false, bool SELF_TEST = false>
-__global__ void __launch_bounds__(kTT, 2) k_dirac_tma(const cx<T>* __restrict__ U, const cx<TIN>* __restrict__ in,
+// self-test); RES: the residual out = b - D in instead (source r's b at bres + r * bstride, the
+// same site arithmetic as k_residual), skipping the sources with act[r] == 0 and, when
+// partial is given, writing each CTA's sum of |out|^2 to partial[r * gridDim.x * gridDim.y +
+// CTA]
+// (UA: the links' type, a plain pointer or the storage-format view of the mixed form's links)
+template <typename T, bool DAG, typename TIN = T, bool COPY = false, bool SELF_TEST = false, bool RES = false,
+          typename UA = const cx<T>* __restrict__>
+__global__ void __launch_bounds__(kTT, 2) k_dirac_tma(UA U, const cx<TIN>* __restrict__ in,
                                                       cx<T>* __restrict__ out, int nx, int nt, T m0, int nrhs,
-                                                      cx<T>* __restrict__ in_copy) {
+                                                      cx<T>* __restrict__ in_copy, const cx<T>* __restrict__ bres,
+                                                      long long bstride, const int* __restrict__ act,
+                                                      double* __restrict__ partial) {
     constexpr int wait_limit = SELF_TEST ? 256 : kTmaSpinLimit;
     extern __shared__ __align__(128) unsigned char smraw_d[];
+    __shared__ double red[kTT / 32 + 1];                // the residual's norm reduction
     constexpr int RS = kTT + 2;                         // sites per staged row segment
     constexpr int SB = 2 * (int)sizeof(cx<TIN>);        // bytes per site (both spins)
     constexpr int BUF = dirac_tma_buf_bytes<TIN>();
@@ -145,18 +153,32 @@ __global__ void __launch_bounds__(kTT, 2) k_dirac_tma(const cx<T>* __restrict__ 
         done = rhs + 1;
         const cx<TIN>* tile = buf0 + (size_t)b * (BUF / sizeof(cx<TIN>));
         cx<T>* o = out + (long long)rhs * N * 2;
+        if (!RES || !act || act[rhs]) {
+            double nrm = 0;
 #pragma unroll
-        for (int r = 0; r < kTX; r++) {
-            const int c = (r + 1) * RS + tid + 1;
-            cx<T> o0, o1;
-            dirac_site<T, DAG, TIN>(L[r], tile, c, mass, o0, o1);
-            const long long n = (long long)(x0 + r) * nt + t0 + tid;
-            o[2 * n] = o0;
-            o[2 * n + 1] = o1;
-            if constexpr (COPY) {
-                cx<T>* ic = in_copy + (long long)rhs * N * 2;
-                ic[2 * n] = ccast<T>(tile[2 * c]);
-                ic[2 * n + 1] = ccast<T>(tile[2 * c + 1]);
+            for (int r = 0; r < kTX; r++) {
+                const int c = (r + 1) * RS + tid + 1;
+                cx<T> o0, o1;
+                dirac_site<T, DAG, TIN>(L[r], tile, c, mass, o0, o1);
+                const long long n = (long long)(x0 + r) * nt + t0 + tid;
+                if constexpr (RES) {
+                    const cx<T>* bb = bres + (long long)rhs * bstride;
+                    o0 = bb[2 * n] - o0;
+                    o1 = bb[2 * n + 1] - o1;
+                    nrm += (double)cnorm2(o0) + (double)cnorm2(o1);
+                }
+                o[2 * n] = o0;
+                o[2 * n + 1] = o1;
+                if constexpr (COPY) {
+                    cx<T>* ic = in_copy + (long long)rhs * N * 2;
+                    ic[2 * n] = ccast<T>(tile[2 * c]);
+                    ic[2 * n + 1] = ccast<T>(tile[2 * c + 1]);
+                }
+            }
+            if (RES && partial) {
+                // the whole CTA takes this branch (act is per source)
+                nrm = cta_sum(nrm, red);
+                if (tid == 0) partial[(long long)rhs * gridDim.x * gridDim.y + blockIdx.y * gridDim.x + blockIdx.x] = nrm;
             }
         }
         __syncthreads();   // every thread is done with buffer b

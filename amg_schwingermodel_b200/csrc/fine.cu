@@ -709,8 +709,8 @@ int dirac_tma_wait_test(const double2* U, const double2* in, double2* out, int n
     if (cudaFuncSetAttribute(k_dirac_tma<double, false, double, false, true>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess)
         return -1;
-    k_dirac_tma<double, false, double, false, true><<<dim3(nt / kTT, nx / kTX), kTT, bytes, s>>>(U, in, out, nx, nt,
-                                                                                                 -0.1, nrhs, nullptr);
+    k_dirac_tma<double, false, double, false, true><<<dim3(nt / kTT, nx / kTX), kTT, bytes, s>>>(
+        U, in, out, nx, nt, -0.1, nrhs, nullptr, nullptr, 0, nullptr, nullptr);
     if (cudaGetLastError() != cudaSuccess) return -1;
     return fine_error_check(s);
 }
@@ -727,10 +727,12 @@ void launch_dirac(const cx<T>* U, const cx<T>* in, cx<T>* out, int nx, int nt, i
         dim3 g(nt / kTT, nx / kTX);
         if (dagger) {
             cudaFuncSetAttribute(k_dirac_tma<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-            k_dirac_tma<T, true><<<g, kTT, bytes, s>>>(U, in, out, nx, nt, m0, nrhs, nullptr);
+            k_dirac_tma<T, true><<<g, kTT, bytes, s>>>(U, in, out, nx, nt, m0, nrhs, nullptr, nullptr, 0, nullptr,
+                                                       nullptr);
         } else {
             cudaFuncSetAttribute(k_dirac_tma<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-            k_dirac_tma<T, false><<<g, kTT, bytes, s>>>(U, in, out, nx, nt, m0, nrhs, nullptr);
+            k_dirac_tma<T, false><<<g, kTT, bytes, s>>>(U, in, out, nx, nt, m0, nrhs, nullptr, nullptr, 0, nullptr,
+                                                        nullptr);
         }
         return;
     }
@@ -750,7 +752,7 @@ void launch_dirac_promote(const double2* U, const float2* in, double2* out, doub
         cudaFuncSetAttribute(k_dirac_tma<double, false, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              bytes);
         k_dirac_tma<double, false, float, true><<<dim3(nt / kTT, nx / kTX), kTT, bytes, s>>>(
-            U, in, out, nx, nt, m0, nrhs, in_copy);
+            U, in, out, nx, nt, m0, nrhs, in_copy, nullptr, 0, nullptr, nullptr);
         return;
     }
     dim3 grid((nx * nt + 255) / 256, source_groups(nx * nt, nrhs));
@@ -761,6 +763,27 @@ template <typename T>
 void launch_residual(const Links<T> U, const cx<T>* b, long long bstride, const cx<T>* x, cx<T>* r, int nx, int nt,
                      int nrhs, T m0, double* partial, double* norm2_out, const int* act, cudaStream_t s) {
     count_launch(norm2_out ? 2 : 1);
+    // lattices the bulk-copy stencil tiles: x staged through shared memory, source after
+    // source, the links in registers (the same site arithmetic as k_residual)
+    if (dirac_tma_enabled() && nrhs >= 1 && nt % kTT == 0 && nx % kTX == 0 && nx >= kTX && x != r &&
+        ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(r)) & 15) == 0) {
+        constexpr int bytes = dirac_tma_smem<T>();
+        const dim3 g(nt / kTT, nx / kTX);
+        if constexpr (sizeof(T) == 8) {   // FP64 links: a plain pointer
+            const cx<T>* Up = static_cast<const cx<T>*>(U.p);
+            cudaFuncSetAttribute(k_dirac_tma<T, false, T, false, false, true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+            k_dirac_tma<T, false, T, false, false, true><<<g, kTT, bytes, s>>>(
+                Up, x, r, nx, nt, m0, nrhs, nullptr, b, bstride, act, norm2_out ? partial : nullptr);
+        } else {
+            cudaFuncSetAttribute(k_dirac_tma<T, false, T, false, false, true, Links<T>>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+            k_dirac_tma<T, false, T, false, false, true, Links<T>><<<g, kTT, bytes, s>>>(
+                U, x, r, nx, nt, m0, nrhs, nullptr, b, bstride, act, norm2_out ? partial : nullptr);
+        }
+        if (norm2_out) k_sum_partials<<<nrhs, 256, 0, s>>>(partial, (int)(g.x * g.y), norm2_out);
+        return;
+    }
     const int nblk = (nx * nt + 255) / 256;
     dim3 grid(nblk, source_groups(nx * nt, nrhs));
     k_residual<T><<<grid, 256, 0, s>>>(U, b, bstride, x, r, nx, nt, m0, norm2_out ? partial : nullptr, act, nrhs);
