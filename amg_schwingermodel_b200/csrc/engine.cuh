@@ -210,11 +210,21 @@ __device__ __forceinline__ void part_range(const Eng<T>& E, int tot, int& e0, in
     e0 = min(tot, E.crank * per);
     e1 = min(tot, e0 + per);
 }
+// The cluster split as plain values, read once per operator call: inside the row loops the
+// fields of the engine context would otherwise be re-read from the caller's stack frame
+// after every store (the stores go through generic pointers that may alias it).
+struct Part {
+    int csize, crank;
+    long long slab;
+};
 template <typename T>
-__device__ __forceinline__ void part_store(const Eng<T>& E, cx<T>* out, int e, cx<T> v) {
-    if (E.csize == 1) { out[e] = v; return; }
-    const long long slab = E.a->slab;
-    for (int q = 0; q < E.csize; q++) out[(long long)(q - E.crank) * slab + e] = v;
+__device__ __forceinline__ Part part_of(const Eng<T>& E) {
+    return Part{E.csize, E.crank, E.a->slab};
+}
+template <typename T>
+__device__ __forceinline__ void part_store(const Part& P, cx<T>* out, int e, cx<T> v) {
+    if (P.csize == 1) { out[e] = v; return; }
+    for (int q = 0; q < P.csize; q++) out[(long long)(q - P.crank) * P.slab + e] = v;
 }
 template <typename T>
 __device__ __forceinline__ void part_begin(const Eng<T>& E) {
@@ -246,7 +256,9 @@ __device__ __forceinline__ cx<T> tpr_sum(cx<T> a) {
 // a slice of the rows and stores it into every CTA's copy of `out`.
 template <typename T>
 __device__ __noinline__ void dc_apply(const Eng<T>& E, const EngLevel<T>& L, T m0, const cx<T>* in, cx<T>* out) {
-    const int K = L.K, tot = L.n * K;
+    const int K = L.K, tot = L.n * K, lnx = L.nx, lnt = L.nt;
+    const cx<T>* const links = L.links;
+    const Part P = part_of(E);
     const T mass = m0 + T(2);
     int e0, e1;
     eng_count(E, L.level, CNT_APPLY);
@@ -259,21 +271,21 @@ __device__ __noinline__ void dc_apply(const Eng<T>& E, const EngLevel<T>& L, T m
         cx<T> acc = czero<T>();
         if (on) {
             const int xs = e / K, i = e - xs * K;
-            const int x = xs / L.nt, t = xs - x * L.nt;
-            const cx<T>* lk = L.links + (long long)xs * 5 * K * K + i;
+            const int x = xs / lnt, t = xs - x * lnt;
+            const cx<T>* lk = links + (long long)xs * 5 * K * K + i;
 #pragma unroll 1
             for (int h = 0; h < 5; h++) {
-                const int nbs = nb_site(x, t, L.nx, L.nt, h);
+                const int nbs = nb_site(x, t, lnx, lnt, h);
                 const cx<T>* v = in + (long long)nbs * K;
                 const cx<T>* a = lk + (long long)h * K * K;
                 cx<T> s = czero<T>();
 #pragma unroll 4
-                for (int j = g; j < K; j += kTPR) cfma(s, a[(long long)j * K], v[j]);
-                if (hop_sign(t, L.nt, h) < 0) acc -= s; else acc += s;
+                for (int j = g; j < K; j += kTPR) cfma(s, __ldg(a + (long long)j * K), v[j]);
+                if (hop_sign(t, lnt, h) < 0) acc -= s; else acc += s;
             }
         }
         acc = tpr_sum<T>(acc);
-        if (on && g == 0) part_store(E, out, e, mass * in[e] - acc);
+        if (on && g == 0) part_store<T>(P, out, e, mass * in[e] - acc);
     }
     part_end(E);
 }
@@ -293,7 +305,11 @@ __device__ __forceinline__ int sap_site(const EngLevel<T>& L, int block, int m, 
 // Level::Pt_v (src/level.cpp:212-237): out[nc][2cc+s] = sum_{n in nc, c} conj(W_cc[n][2c+s]) v[n][2c+s]
 template <typename T>
 __device__ __noinline__ void restrict_v(const Eng<T>& E, const EngLevel<T>& L, const cx<T>* v, cx<T>* out) {
-    const int K = L.K, col = K / 2, nblk = L.bx * L.bt, tot = nblk * 2 * L.ntest, nterm = L.xe * L.te * col;
+    const int K = L.K, col = K / 2, nblk = L.bx * L.bt, ntest = L.ntest, tot = nblk * 2 * ntest;
+    const int xe = L.xe, te = L.te, lbt = L.bt, lnt = L.nt, nterm = xe * te * col;
+    const long long wstride = (long long)L.n * K;
+    const cx<T>* const W = L.W;
+    const Part P = part_of(E);
     int e0, e1;
     part_range(E, tot, e0, e1);
     part_begin(E);
@@ -303,19 +319,19 @@ __device__ __noinline__ void restrict_v(const Eng<T>& E, const EngLevel<T>& L, c
         const bool on = o < e1;
         cx<T> acc = czero<T>();
         if (on) {
-            const int nc = o / (2 * L.ntest), r = o - nc * 2 * L.ntest, cc = r >> 1, s = r & 1;
-            const int bxi = nc / L.bt, bti = nc - bxi * L.bt;
-            const cx<T>* w = L.W + (long long)cc * L.n * K;
+            const int nc = o / (2 * ntest), r = o - nc * 2 * ntest, cc = r >> 1, s = r & 1;
+            const int bxi = nc / lbt, bti = nc - bxi * lbt;
+            const cx<T>* w = W + (long long)cc * wstride;
 #pragma unroll 4
             for (int q = g; q < nterm; q += kTPR) {
                 const int site = q / col, c = q - site * col;
-                const int mx = site / L.te, mt = site - mx * L.te;
-                const long long n = (long long)(bxi * L.xe + mx) * L.nt + (bti * L.te + mt);
-                cfmac(acc, w[n * K + 2 * c + s], v[n * K + 2 * c + s]);
+                const int mx = site / te, mt = site - mx * te;
+                const long long n = (long long)(bxi * xe + mx) * lnt + (bti * te + mt);
+                cfmac(acc, __ldg(w + n * K + 2 * c + s), v[n * K + 2 * c + s]);
             }
         }
         acc = tpr_sum<T>(acc);
-        if (on && g == 0) part_store(E, out, o, acc);
+        if (on && g == 0) part_store<T>(P, out, o, acc);
     }
     part_end(E);
 }
@@ -324,7 +340,10 @@ __device__ __noinline__ void restrict_v(const Eng<T>& E, const EngLevel<T>& L, c
 template <typename T>
 __device__ __noinline__ void prolong_v(const Eng<T>& E, const EngLevel<T>& L, const cx<T>* vc, cx<T>* out,
                                        int accumulate) {
-    const int K = L.K, tot = L.n * K;
+    const int K = L.K, tot = L.n * K, lnt = L.nt, xe = L.xe, te = L.te, lbt = L.bt, ntest = L.ntest;
+    const long long wstride = (long long)L.n * K;
+    const cx<T>* const W = L.W;
+    const Part P = part_of(E);
     int e0, e1;
     part_range(E, tot, e0, e1);
     part_begin(E);
@@ -335,14 +354,14 @@ __device__ __noinline__ void prolong_v(const Eng<T>& E, const EngLevel<T>& L, co
         cx<T> acc = czero<T>();
         if (on) {
             const int n = e / K, d = e - n * K, s = d & 1;
-            const int x = n / L.nt, t = n - x * L.nt;
-            const int nc = (x / L.xe) * L.bt + (t / L.te);
-            const cx<T>* pv = vc + (long long)nc * 2 * L.ntest + s;
+            const int x = n / lnt, t = n - x * lnt;
+            const int nc = (x / xe) * lbt + (t / te);
+            const cx<T>* pv = vc + (long long)nc * 2 * ntest + s;
 #pragma unroll 2
-            for (int cc = g; cc < L.ntest; cc += kTPR) cfma(acc, L.W[(long long)cc * L.n * K + e], pv[2 * cc]);
+            for (int cc = g; cc < ntest; cc += kTPR) cfma(acc, __ldg(W + (long long)cc * wstride + e), pv[2 * cc]);
         }
         acc = tpr_sum<T>(acc);
-        if (on && g == 0) part_store(E, out, e, accumulate ? out[e] + acc : acc);
+        if (on && g == 0) part_store<T>(P, out, e, accumulate ? out[e] + acc : acc);
     }
     part_end(E);
 }
@@ -517,9 +536,10 @@ __device__ int team_fgmres(const Team& tm, T* part, const Eng<T>* E, int cnt_lev
 // block's sites m (local order) from in[m][j]; neighbours outside the block are dropped.
 template <typename T>
 __device__ void dlocal_block(const Team& tm, const EngLevel<T>& L, T m0, int block, const cx<T>* in, cx<T>* out) {
-    const int K = L.K, spb = L.sxe * L.ste, n = spb * K;
+    const int K = L.K, sxe = L.sxe, ste = L.ste, sbt = L.sbt, lnx = L.nx, lnt = L.nt, spb = sxe * ste, n = spb * K;
+    const cx<T>* const links = L.links;
     const T mass = m0 + T(2);
-    const int bxi = block / L.sbt, bti = block - bxi * L.sbt;
+    const int bxi = block / sbt, bti = block - bxi * sbt;
     const int g = tm.tid % kTPR, rows_per_pass = tm.size / kTPR;
     for (int rb = 0; rb < n; rb += rows_per_pass) {
         const int e = rb + tm.tid / kTPR;
@@ -527,29 +547,29 @@ __device__ void dlocal_block(const Team& tm, const EngLevel<T>& L, T m0, int blo
         cx<T> acc = czero<T>();
         if (on) {
             const int m = e / K, i = e - m * K;
-            const int mx = m / L.ste, mt = m - mx * L.ste;
-            const int x = bxi * L.sxe + mx, t = bti * L.ste + mt;
-            const int xs = x * L.nt + t;
-            const cx<T>* lk = L.links + (long long)xs * 5 * K * K + i;
+            const int mx = m / ste, mt = m - mx * ste;
+            const int x = bxi * sxe + mx, t = bti * ste + mt;
+            const int xs = x * lnt + t;
+            const cx<T>* lk = links + (long long)xs * 5 * K * K + i;
 #pragma unroll 1
             for (int h = 0; h < 5; h++) {
                 int nx_ = x, nt_ = t;
                 switch (h) {
-                    case HOP_R0: nt_ = (t + 1 == L.nt) ? 0 : t + 1; break;
-                    case HOP_R1: nx_ = (x + 1 == L.nx) ? 0 : x + 1; break;
-                    case HOP_L0: nt_ = (t == 0) ? L.nt - 1 : t - 1; break;
-                    case HOP_L1: nx_ = (x == 0) ? L.nx - 1 : x - 1; break;
+                    case HOP_R0: nt_ = (t + 1 == lnt) ? 0 : t + 1; break;
+                    case HOP_R1: nx_ = (x + 1 == lnx) ? 0 : x + 1; break;
+                    case HOP_L0: nt_ = (t == 0) ? lnt - 1 : t - 1; break;
+                    case HOP_L1: nx_ = (x == 0) ? lnx - 1 : x - 1; break;
                     default: break;
                 }
-                const int nbx = nx_ / L.sxe, nbt = nt_ / L.ste;
-                if (nbx * L.sbt + nbt != block) continue;
-                const int ml = (nx_ - nbx * L.sxe) * L.ste + (nt_ - nbt * L.ste);
+                const int nbx = nx_ / sxe, nbt = nt_ / ste;
+                if (nbx * sbt + nbt != block) continue;
+                const int ml = (nx_ - nbx * sxe) * ste + (nt_ - nbt * ste);
                 const cx<T>* v = in + (long long)ml * K;
                 const cx<T>* a = lk + (long long)h * K * K;
                 cx<T> s = czero<T>();
 #pragma unroll 4
-                for (int j = g; j < K; j += kTPR) cfma(s, a[(long long)j * K], v[j]);
-                if (hop_sign(t, L.nt, h) < 0) acc -= s; else acc += s;
+                for (int j = g; j < K; j += kTPR) cfma(s, __ldg(a + (long long)j * K), v[j]);
+                if (hop_sign(t, lnt, h) < 0) acc -= s; else acc += s;
             }
         }
         acc = tpr_sum<T>(acc);
@@ -613,7 +633,8 @@ __device__ __noinline__ int eng_sap(const Eng<T>& E, int l, const cx<T>* v, cx<T
                 team_fgmres(tm, tpart, &E, l, CNT_SAP_STEP, lop, ident, bv, xv, Vv, Vv, wv, st, seglen, m,
                             p.sap_restarts, p.sap_gmres_tol);
                 // broadcast the block solution to every CTA of the cluster
-                for (int e = tm.tid; e < seglen; e += tm.size) part_store(E, xall + (long long)bi * seglen, e, xv[e]);
+                const Part P = part_of(E);
+                for (int e = tm.tid; e < seglen; e += tm.size) part_store<T>(P, xall + (long long)bi * seglen, e, xv[e]);
                 team_sync(tm);
             }
             if (E.csize > 1) cluster_barrier(); else __syncthreads();

@@ -14,6 +14,7 @@
 #include "sap_lean.cuh"
 #include "sap_f32.cuh"
 #include "sap_ca.cuh"
+#include "sap_h.cuh"
 #include "tc_transfer.cuh"
 
 namespace amgb {
@@ -1028,12 +1029,17 @@ cudaError_t launch_sap0_lean(const Links<T> U, const cx<T>* r, cx<T>* x, const i
 // a few percent of each other on B200, so the MGS form (the reference's arithmetic) stays
 // the default.  AMG_SAP_KERNEL=cgs selects the paired kernel with classical Gram-Schmidt
 // (one reduction per Arnoldi step instead of j + 2, a second projection on cancellation).
+// AMG_SAP_KERNEL=half selects the FP16-basis kernel (sap_h.cuh; FP16 fine links only).
 static int g_sap0_f32 = -1, g_sap0_spt = -1, g_sap0_f32_variant = -1;
 static int sap0_f32_enabled() {
     if (g_sap0_f32 < 0) {
         const char* e = getenv("AMG_SAP_KERNEL");
         g_sap0_f32 = (e && (!strcmp(e, "generic") || !strcmp(e, "lean"))) ? 0 : 1;
-        g_sap0_f32_variant = !e ? 0 : !strcmp(e, "ca") ? SAP_VARIANT_CA : !strcmp(e, "cgs") ? SAP_VARIANT_CGS : 0;
+        g_sap0_f32_variant = !e                  ? 0
+                             : !strcmp(e, "ca")   ? SAP_VARIANT_CA
+                             : !strcmp(e, "cgs")  ? SAP_VARIANT_CGS
+                             : !strcmp(e, "half") ? SAP_VARIANT_HALF
+                                                  : 0;
         const char* t = getenv("AMG_SAP_SPT");
         g_sap0_spt = (t && atoi(t) == 2) ? 2 : 4;
     }
@@ -1063,6 +1069,25 @@ cudaError_t launch_sap0_f32(const Links<float> U, float2* r, float2* x, const in
     dim3 grid(ncol, nrhs);
     k_sap0_f32<5, SPT, NW, CGS><<<grid, 32 * NW, bytes, s>>>(U, r, x, blocks, ncol, nx, nt, sbt, sxe, ste, m0, restarts,
                                                              tol, act, iters, vsrc, vstride);
+    return cudaGetLastError();
+}
+
+// The FP16-basis kernel for blocks of 256, 512 or 1024 sites (NW = sites / 128 warps of four
+// sites per thread), three CTAs per SM: the largest shared-memory carveout is requested so
+// that three blocks' 73 KB fit.
+template <int NW>
+cudaError_t launch_sap0_h(const __half2* U, float2* r, float2* x, const int* blocks, int ncol, int nrhs, int nx,
+                          int nt, int sbt, int sxe, int ste, float m0, int restarts, float tol, int* iters,
+                          const int* act, cudaStream_t s) {
+    constexpr int bytes = sap0_h_smem<5, 4, NW>();
+    cudaError_t e = cudaFuncSetAttribute(k_sap0_h<5, 4, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_sap0_h<5, 4, NW>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared);
+    if (e != cudaSuccess) return e;
+    dim3 grid(ncol, nrhs);
+    k_sap0_h<5, 4, NW><<<grid, 32 * NW, bytes, s>>>(U, r, x, blocks, ncol, nx, nt, sbt, sxe, ste, m0, restarts, tol,
+                                                    act, iters);
     return cudaGetLastError();
 }
 
@@ -1158,6 +1183,19 @@ cudaError_t launch_sap0(const Links<T> U, cx<T>* r, cx<T>* x, const int* blocks,
         }
     }
     if constexpr (std::is_same<T, float>::value) {
+        if (v == SAP_VARIANT_HALF) {
+            // FP16 basis: FP16 links, restart length 5, four sites per thread in one t row
+            if (m == 5 && U.fmt == LINK_F16 && ste % 4 == 0) {
+                const __half2* Uh = static_cast<const __half2*>(U.p);
+                switch (S) {
+                    case 256: return launch_sap0_h<2>(Uh, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
+                    case 512: return launch_sap0_h<4>(Uh, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
+                    case 1024: return launch_sap0_h<8>(Uh, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
+                    default: break;
+                }
+            }
+            v = SAP_VARIANT_PAIRED;
+        }
         if (m == 5 && (v == SAP_VARIANT_PAIRED || v == SAP_VARIANT_CA || v == SAP_VARIANT_CGS)) {
             bool done = false;
             const cudaError_t e = launch_sap0_paired(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts,
