@@ -316,7 +316,8 @@ class AMGContext:
         """The autotuner's choice (amg_autotune_info)."""
         o = np.zeros(4, dtype=np.int32)
         check(lib().amg_autotune_info(self._h, _cptr(o)), "amg_autotune_info")
-        names = {-1: "default", 0: "generic", 1: "lean", 2: "paired_f32", 3: "ca_f32", 4: "cgs_f32", 5: "half_basis"}
+        names = {-1: "default", 0: "generic", 1: "lean", 2: "paired_f32", 3: "ca_f32", 4: "cgs_f32", 5: "half_basis",
+                 6: "bf16_basis"}
         return dict(tuned=bool(o[0]), sap_kernel=names.get(int(o[1]), str(o[1])), engine_cluster=int(o[2]),
                     tuned_cycle_us=int(o[3]))
 

@@ -1029,7 +1029,8 @@ cudaError_t launch_sap0_lean(const Links<T> U, const cx<T>* r, cx<T>* x, const i
 // a few percent of each other on B200, so the MGS form (the reference's arithmetic) stays
 // the default.  AMG_SAP_KERNEL=cgs selects the paired kernel with classical Gram-Schmidt
 // (one reduction per Arnoldi step instead of j + 2, a second projection on cancellation).
-// AMG_SAP_KERNEL=half selects the FP16-basis kernel (sap_h.cuh; FP16 fine links only).
+// AMG_SAP_KERNEL=half selects the FP16-basis kernel (sap_h.cuh; FP16 fine links only) and
+// AMG_SAP_KERNEL=bf16 the same kernel with a BF16 basis.
 static int g_sap0_f32 = -1, g_sap0_spt = -1, g_sap0_f32_variant = -1;
 static int sap0_f32_enabled() {
     if (g_sap0_f32 < 0) {
@@ -1039,6 +1040,7 @@ static int sap0_f32_enabled() {
                              : !strcmp(e, "ca")   ? SAP_VARIANT_CA
                              : !strcmp(e, "cgs")  ? SAP_VARIANT_CGS
                              : !strcmp(e, "half") ? SAP_VARIANT_HALF
+                             : !strcmp(e, "bf16") ? SAP_VARIANT_BF16B
                                                   : 0;
         const char* t = getenv("AMG_SAP_SPT");
         g_sap0_spt = (t && atoi(t) == 2) ? 2 : 4;
@@ -1075,20 +1077,34 @@ cudaError_t launch_sap0_f32(const Links<float> U, float2* r, float2* x, const in
 // The FP16-basis kernel for blocks of 256, 512 or 1024 sites (NW = sites / 128 warps of four
 // sites per thread), three CTAs per SM: the largest shared-memory carveout is requested so
 // that three blocks' 73 KB fit.
-template <int NW>
+template <int NW, bool BF>
 cudaError_t launch_sap0_h(const __half2* U, float2* r, float2* x, const int* blocks, int ncol, int nrhs, int nx,
                           int nt, int sbt, int sxe, int ste, float m0, int restarts, float tol, int* iters,
                           const int* act, cudaStream_t s) {
     constexpr int bytes = sap0_h_smem<5, 4, NW>();
-    cudaError_t e = cudaFuncSetAttribute(k_sap0_h<5, 4, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaError_t e = cudaFuncSetAttribute(k_sap0_h<5, 4, NW, BF>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_sap0_h<5, 4, NW>, cudaFuncAttributePreferredSharedMemoryCarveout,
+        e = cudaFuncSetAttribute(k_sap0_h<5, 4, NW, BF>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                  cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) return e;
     dim3 grid(ncol, nrhs);
-    k_sap0_h<5, 4, NW><<<grid, 32 * NW, bytes, s>>>(U, r, x, blocks, ncol, nx, nt, sbt, sxe, ste, m0, restarts, tol,
-                                                    act, iters);
+    k_sap0_h<5, 4, NW, BF><<<grid, 32 * NW, bytes, s>>>(U, r, x, blocks, ncol, nx, nt, sbt, sxe, ste, m0, restarts,
+                                                        tol, act, iters);
     return cudaGetLastError();
+}
+template <bool BF>
+static cudaError_t launch_sap0_h_shape(const __half2* U, float2* r, float2* x, const int* blocks, int ncol, int nrhs,
+                                       int nx, int nt, int sbt, int sxe, int ste, float m0, int restarts, float tol,
+                                       int* iters, const int* act, cudaStream_t s, bool* done) {
+    *done = true;
+    switch (sxe * ste) {
+        case 256: return launch_sap0_h<2, BF>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
+        case 512: return launch_sap0_h<4, BF>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
+        case 1024: return launch_sap0_h<8, BF>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
+        default: break;
+    }
+    *done = false;
+    return cudaSuccess;
 }
 
 // FP32 solves of 64- to 1024-site blocks take the paired-FP32 kernel.
@@ -1183,16 +1199,16 @@ cudaError_t launch_sap0(const Links<T> U, cx<T>* r, cx<T>* x, const int* blocks,
         }
     }
     if constexpr (std::is_same<T, float>::value) {
-        if (v == SAP_VARIANT_HALF) {
-            // FP16 basis: FP16 links, restart length 5, four sites per thread in one t row
+        if (v == SAP_VARIANT_HALF || v == SAP_VARIANT_BF16B) {
+            // 16-bit basis: FP16 links, restart length 5, four sites per thread in one t row
             if (m == 5 && U.fmt == LINK_F16 && ste % 4 == 0) {
                 const __half2* Uh = static_cast<const __half2*>(U.p);
-                switch (S) {
-                    case 256: return launch_sap0_h<2>(Uh, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
-                    case 512: return launch_sap0_h<4>(Uh, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
-                    case 1024: return launch_sap0_h<8>(Uh, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s);
-                    default: break;
-                }
+                bool done = false;
+                const cudaError_t e =
+                    v == SAP_VARIANT_BF16B
+                        ? launch_sap0_h_shape<true>(Uh, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s, &done)
+                        : launch_sap0_h_shape<false>(Uh, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s, &done);
+                if (done) return e;
             }
             v = SAP_VARIANT_PAIRED;
         }

@@ -1,4 +1,5 @@
-// FP32 SAP block solve with its Krylov basis stored in FP16: the solve of k_sap0_f32 (MGS
+// FP32 SAP block solve with its Krylov basis stored in 16 bits (FP16, or BF16 with BF = true):
+// the solve of k_sap0_f32 (MGS
 // form; src/sap.cpp:44-62, GMRES_D_B include/sap.h:27-47, FGMRES::fgmres
 // src/fgmres.cpp:5-115 with x0 = b) laid out for three CTAs per SM instead of two.
 //
@@ -14,30 +15,50 @@
 //     t row), and the Givens rotations and g live in shared memory, written by thread 0;
 // which fits 80 registers and 73 KB, three CTAs (24 warps) per SM.
 //
-// Every basis vector is rounded to FP16 when it is stored and the thread's registers are
+// Every basis vector is rounded to 16 bits when it is stored and the thread's registers are
 // rounded the same way, so the operator, the Gram-Schmidt dots and the projections all see
-// the stored vectors; the Arnoldi relation then holds to the FP16 rounding of V_{j+1}
-// (relative 2^-11), while the true residual of every restart cycle is formed in FP32 from
-// the FP32 iterate.
+// the stored vectors; the Arnoldi relation then holds to the rounding of V_{j+1} (relative
+// 2^-11 in FP16, 2^-8 in BF16), while the true residual of every restart cycle is formed in
+// FP32 from the FP32 iterate.
 #pragma once
 #include "common.cuh"
 #include "sap_f32.cuh"
 
 namespace amgb {
 
-// an FP16 basis site: (s0.re, s1.re) and (s0.im, s1.im) as two half2 in a uint2
-__device__ __forceinline__ SiteP h_unpack(uint2 q) {
-    __half2 a, b;
-    memcpy(&a, &q.x, 4);
-    memcpy(&b, &q.y, 4);
-    return {__half22float2(a), __half22float2(b)};
+// a 16-bit basis site: (s0.re, s1.re) and (s0.im, s1.im) as two 16-bit pairs in a uint2,
+// FP16 (BF = false) or BF16 (BF = true).  FP16 keeps 11 significant bits; its conversions to
+// FP32 run on the FMA pipe.  BF16 keeps 8; its conversions are a shift and a mask on the
+// integer pipe.
+template <bool BF>
+__device__ __forceinline__ float2 p16_to_f2(unsigned u) {
+    if constexpr (BF) {
+        return make_float2(__uint_as_float(u << 16), __uint_as_float(u & 0xffff0000u));
+    } else {
+        __half2 a;
+        memcpy(&a, &u, 4);
+        return __half22float2(a);
+    }
 }
+template <bool BF>
+__device__ __forceinline__ unsigned f2_to_p16(float2 v) {
+    unsigned u;
+    if constexpr (BF) {
+        const __nv_bfloat162 a = __float22bfloat162_rn(v);
+        memcpy(&u, &a, 4);
+    } else {
+        const __half2 a = __float22half2_rn(v);
+        memcpy(&u, &a, 4);
+    }
+    return u;
+}
+template <bool BF>
+__device__ __forceinline__ SiteP h_unpack(uint2 q) {
+    return {p16_to_f2<BF>(q.x), p16_to_f2<BF>(q.y)};
+}
+template <bool BF>
 __device__ __forceinline__ uint2 h_pack(const SiteP& s) {
-    const __half2 a = __float22half2_rn(s.re), b = __float22half2_rn(s.im);
-    uint2 q;
-    memcpy(&q.x, &a, 4);
-    memcpy(&q.y, &b, 4);
-    return q;
+    return make_uint2(f2_to_p16<BF>(s.re), f2_to_p16<BF>(s.im));
 }
 __device__ __forceinline__ float2 h2f(unsigned u) {
     __half2 a;
@@ -58,7 +79,7 @@ __host__ __device__ constexpr int sap0_h_smem() {
     return 32 * NW * SPT * (16 + 16 + 8 * M) + ((M * M + 1) & ~1) * 8 + 2 * 2 * NW * 8 + (3 * M + 1) * 8 + 16;
 }
 
-template <int M, int SPT, int NW>
+template <int M, int SPT, int NW, bool BF = false>
 __global__ void __launch_bounds__(32 * NW, 3) k_sap0_h(const __half2* __restrict__ U, float2* __restrict__ r,
                                                         float2* __restrict__ xg, const int* __restrict__ blocks,
                                                         int ncol, int nx, int nt, int sbt, int sxe, int ste, float m0,
@@ -150,10 +171,10 @@ __global__ void __launch_bounds__(32 * NW, 3) k_sap0_h(const __half2* __restrict
         for (int k = 0; k < SPT; k++) {
             const int mi = tid + TPB * k;
             const SiteP c = w[k];
-            const SiteP a = (k < SPT - 1) ? w[k + 1] : h_unpack(v[nbt1]);
-            const SiteP e = (k > 0) ? prev : h_unpack(v[nbt0]);
+            const SiteP a = (k < SPT - 1) ? w[k + 1] : h_unpack<BF>(v[nbt1]);
+            const SiteP e = (k > 0) ? prev : h_unpack<BF>(v[nbt0]);
             prev = c;
-            w[k] = site_op(mi, c, a, e, h_unpack(v[mi + dxp]), h_unpack(v[mi + dxm]));
+            w[k] = site_op(mi, c, a, e, h_unpack<BF>(v[mi + dxp]), h_unpack<BF>(v[mi + dxm]));
         }
     };
     // w = D_B X
@@ -180,9 +201,9 @@ __global__ void __launch_bounds__(32 * NW, 3) k_sap0_h(const __half2* __restrict
     auto store_v = [&](uint2* d, SiteP (&w)[SPT]) {
 #pragma unroll
         for (int k = 0; k < SPT; k++) {
-            const uint2 q = h_pack(w[k]);
+            const uint2 q = h_pack<BF>(w[k]);
             d[tid + TPB * k] = q;
-            w[k] = h_unpack(q);
+            w[k] = h_unpack<BF>(q);
         }
     };
 
@@ -240,7 +261,7 @@ __global__ void __launch_bounds__(32 * NW, 3) k_sap0_h(const __half2* __restrict
                     float2 ar = make_float2(0.f, 0.f), ai = ar, an = ar, nw = ar;
 #pragma unroll
                     for (int k = 0; k < SPT; k++) {
-                        vi[k] = h_unpack(V[i * S + tid + TPB * k]);
+                        vi[k] = h_unpack<BF>(V[i * S + tid + TPB * k]);
                         ar = p_fma(w[k].re, vi[k].re, ar);
                         ar = p_fma(w[k].im, vi[k].im, ar);
                         ai = p_fma(w[k].im, vi[k].re, ai);
@@ -333,7 +354,7 @@ __global__ void __launch_bounds__(32 * NW, 3) k_sap0_h(const __half2* __restrict
                 const float2 ex = p_bc(eta[jj].x), ey = p_bc(eta[jj].y), ney = p_bc(-eta[jj].y);
 #pragma unroll
                 for (int k = 0; k < SPT; k++) {
-                    const SiteP v = h_unpack(V[jj * S + tid + TPB * k]);
+                    const SiteP v = h_unpack<BF>(V[jj * S + tid + TPB * k]);
                     xs[k].re = p_fma(ex, v.re, xs[k].re);
                     xs[k].re = p_fma(ney, v.im, xs[k].re);
                     xs[k].im = p_fma(ex, v.im, xs[k].im);

@@ -1,16 +1,16 @@
-"""The FP16-basis fine SAP kernel (k_sap0_h, csrc/sap_h.cuh; AMG_SAP_KERNEL=half) inside the
-mixed-precision solve, against complete solves of the reference (tests/golden/solve*.npz) on
-the workloads whose SAP blocks are 32x32 sites: 128^2 (beta 2), 256^2 (beta 3), 512^2 (beta 4)
-and the 1024^2 benchmark rows.
+"""The 16-bit-basis fine SAP kernel (k_sap0_h, csrc/sap_h.cuh; AMG_SAP_KERNEL=half for the
+FP16 basis, =bf16 for the BF16 basis) inside the mixed-precision solve, against complete
+solves of the reference (tests/golden/solve*.npz) on the workloads whose SAP blocks are
+32x32 sites: 128^2 (beta 2), 256^2 (beta 3), 512^2 (beta 4) and the 1024^2 benchmark rows.
 
 The kernel runs the reference's block GMRES(5) x 5 restarts (src/sap.cpp:44-62,
-include/sap.h:27-47) in FP32 with the Krylov basis stored in FP16, so the smoother's output
-moves by about the FP16 rounding and the outer FGMRES sees a slightly different
+include/sap.h:27-47) in FP32 with the Krylov basis stored in 16 bits, so the smoother's output
+moves by about that rounding and the outer FGMRES sees a slightly different
 preconditioner.  Bars, as for every mixed solve: at most one outer iteration more than the
 reference, x within 1e-8 of the reference on the fixture's sample, FP64 true residual
 <= 1e-10.  The same solves with the FP32-basis kernel (AMG_SAP_KERNEL=paired) run beside
 them: their outer residual histories must differ after the first preconditioner application
-(the FP16 kernel ran) by less than 10 % (it is the same smoother).  Each kernel choice runs in
+(the 16-bit kernel ran) by less than 10 % (it is the same smoother).  Each kernel choice runs in
 its own process (the choice is read from the environment once per process).
 """
 import json
@@ -63,12 +63,17 @@ def run(kernel):
     return json.loads(p.stdout.split("RESULT", 1)[1])
 
 
-def test_sap_half_basis_solves_match_reference():
-    half = run("half")
-    paired = run("paired")
+@pytest.fixture(scope="module")
+def paired():
+    return run("paired")
+
+
+@pytest.mark.parametrize("kernel", ["half", "bf16"])
+def test_sap_16bit_basis_solves_match_reference(kernel, paired):
+    half = run(kernel)
     for name in NAMES:
         h, p = half[name], paired[name]
-        print(f"{name}: FP16 basis {h['iterations']} iterations, FP32 basis {p['iterations']}, reference "
+        print(f"{name}: {kernel} basis {h['iterations']} iterations, FP32 basis {p['iterations']}, reference "
               f"{h['ref_iterations']}; |x - x_ref|/|x_ref| {h['err']:.2e}; residual {h['resid']:.2e}")
         assert h["iterations"] <= h["ref_iterations"] + 1, h
         assert h["converged"] and h["resid"] < 1e-10, h
