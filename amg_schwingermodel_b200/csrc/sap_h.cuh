@@ -12,7 +12,9 @@
 //   * the folded hop links (sign, 1/2 and the zero outside the block applied; FP16 storage of
 //     the fine links) are staged once per CTA in shared memory (16 KB) instead of registers;
 //   * a thread's neighbour indices reduce to four offsets (its run of SPT sites lies in one
-//     t row), and the Givens rotations and g live in shared memory, written by thread 0;
+//     t row), and the Givens rotations, g, the exit decision and the least-squares solution
+//     live in shared memory: thread 0 computes them while the other threads wait at the
+//     barrier the step takes anyway (the paired kernel repeats them in every thread);
 // which fits 80 registers and 73 KB, three CTAs (24 warps) per SM.
 //
 // Every basis vector is rounded to 16 bits when it is stored and the thread's registers are
@@ -75,8 +77,8 @@ __device__ __forceinline__ unsigned f2h(float2 v) {
 template <int M, int SPT, int NW>
 __host__ __device__ constexpr int sap0_h_smem() {
     // X [S] float4, LK [S] uint4, V [M][S] uint2, H [M][M] float2 (even count), part [2][2 NW]
-    // float2, Givens cs [M], sn [M], g [M + 1] float2
-    return 32 * NW * SPT * (16 + 16 + 8 * M) + ((M * M + 1) & ~1) * 8 + 2 * 2 * NW * 8 + (3 * M + 1) * 8 + 16;
+    // float2, Givens cs [M], sn [M], g [M + 1], eta [M] float2, the exit flag
+    return 32 * NW * SPT * (16 + 16 + 8 * M) + ((M * M + 1) & ~1) * 8 + 2 * 2 * NW * 8 + (4 * M + 1) * 8 + 16;
 }
 
 template <int M, int SPT, int NW, bool BF = false>
@@ -97,6 +99,8 @@ __global__ void __launch_bounds__(32 * NW, 3) k_sap0_h(const __half2* __restrict
     float2* cs_s = part + 2 * PST;                    // [M]
     float2* sn_s = cs_s + M;                          // [M]
     float2* g_s = sn_s + M;                           // [M + 1]
+    float2* eta_s = g_s + M + 1;                      // [M]
+    int* exit_s = reinterpret_cast<int*>(eta_s + M);  // the step's exit decision
     int buf = 0;
     const int tid = threadIdx.x;
     const int block = blocks[seg];
@@ -245,9 +249,6 @@ __global__ void __launch_bounds__(32 * NW, 3) k_sap0_h(const __half2* __restrict
         lean_sync<float, NW>();
 #pragma unroll
         for (int j = 0; j < M; j++) {
-            // g_j as the previous step left it; read before this step's first barrier, which
-            // orders it before thread 0 overwrites it below
-            const float2 gj = g_s[j];
             apply_v(V + j * S, w);   // w held V_j
             float2 col[M + 1];
             // modified Gram-Schmidt (src/fgmres.cpp:24-32); the last projection's reduction
@@ -305,45 +306,54 @@ __global__ void __launch_bounds__(32 * NW, 3) k_sap0_h(const __half2* __restrict
                 }
                 store_v(V + (j + 1) * S, w);
             }
-            // rotation(j) (src/fgmres.cpp:90-104) in every thread from the earlier rotations
-            col[j + 1] = make_float2(hn, 0.f);
-#pragma unroll
-            for (int i = 0; i < j; i++) {
-                const float2 ci = cs_s[i], si = sn_s[i];
-                const float2 temp = cmulc(ci, col[i]) + cmulc(si, col[i + 1]);
-                col[i + 1] = cmul(ci, col[i + 1]) - cmul(si, col[i]);
-                col[i] = temp;
-            }
-            const float rden = rsqrtf(cnorm2(col[j]) + cnorm2(col[j + 1]));
-            const float2 snj = make_float2(col[j + 1].x * rden, col[j + 1].y * rden);
-            const float2 csj = make_float2(col[j].x * rden, col[j].y * rden);
-            col[j] = cmulc(csj, col[j]) + cmulc(snj, col[j + 1]);
-            const float2 gj1 = -cmul(snj, gj);
+            // rotation(j) (src/fgmres.cpp:90-104) and the exit test, by thread 0; the step's
+            // barrier publishes them (the column is the same in every thread after the
+            // reductions, so thread 0's copy is the one the others would have computed)
             if (tid == 0) {
+                col[j + 1] = make_float2(hn, 0.f);
+#pragma unroll
+                for (int i = 0; i < j; i++) {
+                    const float2 ci = cs_s[i], si = sn_s[i];
+                    const float2 temp = cmulc(ci, col[i]) + cmulc(si, col[i + 1]);
+                    col[i + 1] = cmul(ci, col[i + 1]) - cmul(si, col[i]);
+                    col[i] = temp;
+                }
+                const float rden = rsqrtf(cnorm2(col[j]) + cnorm2(col[j + 1]));
+                const float2 snj = make_float2(col[j + 1].x * rden, col[j + 1].y * rden);
+                const float2 csj = make_float2(col[j].x * rden, col[j].y * rden);
+                col[j] = cmulc(csj, col[j]) + cmulc(snj, col[j + 1]);
+                const float2 gj = g_s[j];
+                const float2 gj1 = -cmul(snj, gj);
 #pragma unroll
                 for (int i = 0; i <= j; i++) H[i * M + j] = col[i];
                 cs_s[j] = csj;
                 sn_s[j] = snj;
                 g_s[j] = cmulc(csj, gj);
                 g_s[j + 1] = gj1;
+                *exit_s = cnorm2(gj1) < tolb2;
             }
             lean_sync<float, NW>();
-            if (cnorm2(gj1) < tolb2) {
+            if (*exit_s) {
                 maxit = j + 1;
                 break;
             }
         }
-        // solve_upper_triangular (src/fgmres.cpp:107-115) and x += sum eta_j V_j
-        float2 eta[M];
+        // solve_upper_triangular (src/fgmres.cpp:107-115) by thread 0, then x += sum eta_j V_j
+        if (tid == 0) {
+            float2 eta[M];
 #pragma unroll
-        for (int i = M - 1; i >= 0; i--) {
-            if (i >= maxit) { eta[i] = czero<float>(); continue; }
-            float2 o = g_s[i];
+            for (int i = M - 1; i >= 0; i--) {
+                if (i >= maxit) { eta[i] = czero<float>(); continue; }
+                float2 o = g_s[i];
 #pragma unroll
-            for (int jj = i + 1; jj < M; jj++)
-                if (jj < maxit) o = o - cmul(H[i * M + jj], eta[jj]);
-            eta[i] = cdiv(o, H[i * M + i]);
+                for (int jj = i + 1; jj < M; jj++)
+                    if (jj < maxit) o = o - cmul(H[i * M + jj], eta[jj]);
+                eta[i] = cdiv(o, H[i * M + i]);
+            }
+#pragma unroll
+            for (int i = 0; i < M; i++) eta_s[i] = eta[i];
         }
+        lean_sync<float, NW>();
         {
             SiteP xs[SPT];
 #pragma unroll
@@ -351,7 +361,8 @@ __global__ void __launch_bounds__(32 * NW, 3) k_sap0_h(const __half2* __restrict
 #pragma unroll
             for (int jj = 0; jj < M; jj++) {
                 if (jj >= maxit) break;
-                const float2 ex = p_bc(eta[jj].x), ey = p_bc(eta[jj].y), ney = p_bc(-eta[jj].y);
+                const float2 ej = eta_s[jj];
+                const float2 ex = p_bc(ej.x), ey = p_bc(ej.y), ney = p_bc(-ej.y);
 #pragma unroll
                 for (int k = 0; k < SPT; k++) {
                     const SiteP v = h_unpack<BF>(V[jj * S + tid + TPB * k]);
