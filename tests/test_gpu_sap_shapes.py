@@ -1,10 +1,13 @@
 """The FP32 fine SAP kernels on block shapes the golden fixtures do not have: blocks that
 span the whole lattice in t or in x (so the block operator wraps around periodically inside
-the block), 128-site blocks (one warp, four sites per thread), and blocks whose t extent is
-not a multiple of the sites a thread owns (the dispatcher falls back to the lean kernel).
-Each shape is solved in mixed precision (FP32 cycle inside the FP64 outer FGMRES) with the
-paired MGS kernel and the paired classical Gram-Schmidt kernel, and compared with the FP64
-solve on the same context, whose parity with the reference the fixture tests pin.
+the block), 128- and 256-site blocks (one and two warps, four sites per thread), and blocks
+whose t extent is not a multiple of the sites a thread owns (the dispatcher falls back to
+the lean kernel).  Each shape is solved in mixed precision (FP32 cycle inside the FP64 outer
+FGMRES) with the paired MGS kernel, the paired classical Gram-Schmidt kernel and the
+16-bit-basis kernel with an FP16 and a BF16 basis (which takes the 256- and 512-site
+blocks, the wrap-around ones included, and hands the others to the paired kernel), and
+compared with the FP64 solve on the same context, whose parity with the reference the
+fixture tests pin.
 Bars: FP64 true residual <= 1e-10 for both, mixed x within 1e-8 of the FP64 x, and at most
 one outer iteration more than the FP64 solve."""
 import json
@@ -19,11 +22,13 @@ from conftest import ROOT
 pytestmark = pytest.mark.gpu
 
 # (lattice, rows): fine SAP blocks of 16x32 sites on a 32x32 lattice (t wrap inside the
-# block), 32x16 (x wrap), 8x16 (128 sites) and 64x2 (t extent 2: lean fallback)
+# block), 32x16 (x wrap), 8x16 (128 sites), 16x16 (256 sites) and 64x2 (t extent 2: lean
+# fallback)
 SHAPES = {
     "t_wrap_16x32": (32, [[0, 4, 4, 8, 2, 1], [1, 2, 2, 8, 2, 2]]),
     "x_wrap_32x16": (32, [[0, 4, 4, 8, 1, 2], [1, 2, 2, 8, 2, 2]]),
     "blk_8x16": (64, [[0, 8, 8, 8, 8, 4], [1, 4, 4, 8, 2, 2]]),
+    "blk_16x16": (64, [[0, 8, 8, 8, 4, 4], [1, 4, 4, 8, 2, 2]]),
     "blk_64x2": (64, [[0, 8, 8, 8, 1, 32], [1, 4, 4, 8, 2, 2]]),
 }
 
@@ -55,7 +60,7 @@ print("RESULT" + json.dumps(out))
 """
 
 
-@pytest.mark.parametrize("sap", ["paired", "cgs"])
+@pytest.mark.parametrize("sap", ["paired", "cgs", "half", "bf16"])
 def test_fp32_sap_block_shapes(sap):
     env = dict(os.environ, AMG_SAP_KERNEL=sap)
     code = SCRIPT.format(root=str(ROOT), tests=str(ROOT / "tests"), shapes=SHAPES)

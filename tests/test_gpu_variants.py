@@ -4,7 +4,9 @@ of 4 and 16 CTAs, in FP64; and in the mixed form (FP32 cycle inside the FP64 out
 FGMRES) the paired-FP32 MGS SAP kernel (default) with four or two sites per thread, with
 its residual as a launch of its own (default) or formed inside the block solves
 (AMG_SAP_FUSE=1), the paired kernel with classical Gram-Schmidt, the
-communication-avoiding FP32 kernel and the lean kernel.
+communication-avoiding FP32 kernel, the lean kernel, and the 16-bit-basis kernel with an
+FP16 and a BF16 basis (on the 512- and 1024-site blocks of c64_l2_sap512 and
+c64_l3_sap1024; the other fixtures' blocks go to the paired kernel).
 Each variant runs in its own process (the choice is read from the environment once per
 process).  Mixed-precision bars: FP64 true residual <= 1e-10, x within 1e-8 of the
 reference's, at most one outer iteration more than the reference."""
@@ -51,7 +53,8 @@ print("RESULT" + json.dumps(out))
 @pytest.mark.parametrize("sap,cluster,prec", [
     ("generic", "1", 0), ("lean", "1", 0), ("lean", "4", 0), ("lean", "16", 0),
     ("ca", "16", 1), ("ca", "1", 1), ("paired", "16", 1), ("paired2", "16", 1), ("lean", "16", 1),
-    ("paired", "4", 1), ("cgs", "16", 1), ("cgs", "1", 1), ("paired_fuse", "16", 1)])
+    ("paired", "4", 1), ("cgs", "16", 1), ("cgs", "1", 1), ("paired_fuse", "16", 1), ("half", "16", 1),
+    ("bf16", "4", 1)])
 def test_variant_matches_reference(sap, cluster, prec):
     env = dict(os.environ, AMG_SAP_KERNEL=sap, AMG_ENGINE_CLUSTER=cluster)
     if sap == "paired2":
