@@ -281,6 +281,20 @@ class AMGContext:
         return [dict(iterations=i.iterations, converged=bool(i.converged), rel_residual=i.rel_residual)
                 for i in infos]
 
+    def solve_stream_ptrs(self, b_ptrs, x_ptrs, nrhs: int):
+        """amg_solve_stream: batches of nrhs sources at raw host pointers (page-locked for the
+        copies to overlap the solves), solved one after another; one info list per batch."""
+        nb = len(b_ptrs)
+        if nb != len(x_ptrs) or nb < 1:
+            raise ValueError("need as many output as input batches, at least one")
+        bp = (C.c_void_p * nb)(*b_ptrs)
+        xp = (C.c_void_p * nb)(*x_ptrs)
+        infos = [(AmgSolveInfo * nrhs)() for _ in range(nb)]
+        ip = (C.c_void_p * nb)(*[C.cast(i, C.c_void_p) for i in infos])
+        check(lib().amg_solve_stream(self._h, nb, bp, xp, nrhs, ip), "amg_solve_stream")
+        return [[dict(iterations=i.iterations, converged=bool(i.converged), rel_residual=i.rel_residual)
+                 for i in inf] for inf in infos]
+
     # ---- adjoint
     def solve_adjoint(self, g):
         """lambda = D^{-dagger} g on the same hierarchy; returns (lambda, infos)."""

@@ -93,6 +93,7 @@ SIGNATURES = {
     "amg_kcycle_fgmres": (_I, [_P, _I, _P, _P, C.POINTER(_I)]),
     "amg_solve": (_I, [_P, _P, _P, _I, _P]),
     "amg_solve_dev": (_I, [_P, _P, _P, _I, _P]),
+    "amg_solve_stream": (_I, [_P, _I, _P, _P, _I, _P]),
     "amg_solve_many": (_I, [_I, _P, _P, _P, _P, _P]),
     "amg_solve_many_dev": (_I, [_I, _P, _P, _P, _P, _P]),
     "amg_restrict0_mixed_dev": (_I, [_P, _P, _P, _I]),

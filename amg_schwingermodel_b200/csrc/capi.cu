@@ -230,6 +230,11 @@ struct amg_context {
     // outer FGMRES writes that copy while it normalises the basis vector), or null
     const void* vf_src = nullptr;
     double tuned_us = 0;
+    // amg_solve_stream: the copy stream and the second device slot of b and x (the first is
+    // b, x), created on first use; per slot: inputs copied, solve done, outputs copied
+    cudaStream_t copy_stream = nullptr;
+    DevBuf b1, x1;
+    cudaEvent_t ev_in[2] = {nullptr, nullptr}, ev_solved[2] = {nullptr, nullptr}, ev_out[2] = {nullptr, nullptr};
     void drop_graphs() {
         for (auto& kv : graphs)
             if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
@@ -1480,12 +1485,19 @@ int amg_destroy(amg_ctx c) {
     if (!c) return AMG_OK;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->ev_host) cudaEventDestroy(c->ev_host);
-    cudaStream_t s = c->stream;
+    for (int k = 0; k < 2; k++) {
+        if (c->ev_in[k]) cudaEventDestroy(c->ev_in[k]);
+        if (c->ev_solved[k]) cudaEventDestroy(c->ev_solved[k]);
+        if (c->ev_out[k]) cudaEventDestroy(c->ev_out[k]);
+    }
+    cudaStream_t s = c->stream, cs = c->copy_stream;
     delete c;
     if (s) cudaStreamDestroy(s);
+    if (cs) cudaStreamDestroy(cs);
     return AMG_OK;
 }
 
@@ -2044,6 +2056,66 @@ int amg_solve(amg_ctx c, const double* b, double* x, int nrhs, amg_solve_info* i
     if (rc < 0) return rc;
     CK(cudaMemcpyAsync(x, c->x.p, (size_t)n * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    return rc;
+}
+
+// Batches of host-resident sources solved one after another with the copies hidden: batch i's
+// solve runs on the context's stream while the copy stream brings batch i+1's sources in and
+// takes batch i-1's solutions out, through two device slots (b/x and b1/x1).  Slot k's
+// inputs may be overwritten once the solve that read them is done (ev_solved), and its
+// output once the copy that read it is done (ev_out).
+int amg_solve_stream(amg_ctx c, int nbatch, const double* const* b, double* const* x, int nrhs,
+                     amg_solve_info* const* info) {
+    CKR(check_ready(c, 0, true));
+    if (nbatch < 1 || !b || !x || nrhs < 1) return fail(AMG_ERR_INVALID, "bad argument");
+    for (int i = 0; i < nbatch; i++)
+        if (!b[i] || !x[i]) return fail(AMG_ERR_INVALID, "null vector for batch %d", i);
+    CKR(select_device(c));
+    if (nrhs > c->Rcap) {
+        CKR(ensure_capacity(c, nrhs));
+        CKR(build_engine<double>(c, c->d, std::max(c->d.eng_cap, nrhs)));
+        if (c->p.precision == AMG_PREC_MIXED) CKR(build_engine<float>(c, c->f, std::max(c->f.eng_cap, nrhs)));
+    }
+    if (!c->copy_stream) CK(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+    for (int k = 0; k < 2; k++) {
+        if (!c->ev_in[k]) CK(cudaEventCreateWithFlags(&c->ev_in[k], cudaEventDisableTiming));
+        if (!c->ev_solved[k]) CK(cudaEventCreateWithFlags(&c->ev_solved[k], cudaEventDisableTiming));
+        if (!c->ev_out[k]) CK(cudaEventCreateWithFlags(&c->ev_out[k], cudaEventDisableTiming));
+    }
+    const long long n = (long long)nrhs * vlen0(c);
+    const size_t bytes = (size_t)n * sizeof(double2);
+    CKR(c->b1.alloc(bytes));
+    CKR(c->x1.alloc(bytes));
+    void* bs[2] = {c->b.p, c->b1.p};
+    void* xs[2] = {c->x.p, c->x1.p};
+    cudaStream_t cs = c->copy_stream;
+    // both slots free: nothing of an earlier call may still read or write them
+    CK(cudaStreamSynchronize(c->stream));
+    CK(cudaMemcpyAsync(bs[0], b[0], bytes, cudaMemcpyHostToDevice, cs));
+    CK(cudaEventRecord(c->ev_in[0], cs));
+    int rc = AMG_OK;
+    for (int i = 0; i < nbatch; i++) {
+        const int k = i & 1, kn = k ^ 1;
+        if (i + 1 < nbatch) {
+            // batch i+1's sources into the other slot once batch i-1's solve stopped reading it
+            if (i >= 1) CK(cudaStreamWaitEvent(cs, c->ev_solved[kn], 0));
+            CK(cudaMemcpyAsync(bs[kn], b[i + 1], bytes, cudaMemcpyHostToDevice, cs));
+            CK(cudaEventRecord(c->ev_in[kn], cs));
+        }
+        CK(cudaStreamWaitEvent(c->stream, c->ev_in[k], 0));
+        if (i >= 2) CK(cudaStreamWaitEvent(c->stream, c->ev_out[k], 0));   // batch i-2's solution copied out
+        const int r = amg_solve_dev(c, bs[k], xs[k], nrhs, info ? info[i] : nullptr);
+        if (r < 0) {
+            cudaStreamSynchronize(cs);
+            return r;
+        }
+        if (r == AMG_NOT_CONVERGED) rc = r;
+        CK(cudaEventRecord(c->ev_solved[k], c->stream));
+        CK(cudaStreamWaitEvent(cs, c->ev_solved[k], 0));
+        CK(cudaMemcpyAsync(x[i], xs[k], bytes, cudaMemcpyDeviceToHost, cs));
+        CK(cudaEventRecord(c->ev_out[k], cs));
+    }
+    CK(cudaStreamSynchronize(cs));
     return rc;
 }
 

@@ -238,6 +238,15 @@ AMG_API int amg_kcycle_fgmres(amg_ctx ctx, int level, const double* b, double* x
 AMG_API int amg_solve(amg_ctx ctx, const double* b, double* x, int nrhs, amg_solve_info* info);
 /* Same on device arrays (no host copies). */
 AMG_API int amg_solve_dev(amg_ctx ctx, const void* b_dev, void* x_dev, int nrhs, amg_solve_info* info);
+/* nbatch batches of nrhs sources from host memory, solved one after another (each as
+ * amg_solve): b[i], x[i] are [nrhs][N][2] host arrays, info[i] (optional) [nrhs].  The copies
+ * run on a second stream through two device slots, so batch i+1's sources go in and batch
+ * i-1's solutions come out while batch i is solved; with page-locked host arrays only the
+ * first batch's input and the last batch's output copies are not hidden.  Replaces calling
+ * FGMRES_AMG::fgmres once per right-hand side (src/tests.cpp:67-82).  Returns
+ * AMG_NOT_CONVERGED if any source of any batch did not converge. */
+AMG_API int amg_solve_stream(amg_ctx ctx, int nbatch, const double* const* b, double* const* x, int nrhs,
+                             amg_solve_info* const* info);
 /* Solves on several contexts at once (uneven lattice sizes, different gauge fields): the
  * outer FGMRES of every context advances in turn, each on its context's stream, so one
  * context's kernels run while the host does another's Givens rotations.  Context i solves
