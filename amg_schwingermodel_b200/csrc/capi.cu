@@ -9,6 +9,7 @@
 #include <cstring>
 #include <fstream>
 #include <map>
+#include <memory>
 #include <tuple>
 #include <random>
 #include <string>
@@ -755,6 +756,199 @@ int precondition(amg_context* c, const double2* v, double2* z, int R, bool want_
 }
 
 // ---------------------------------------------------------------------------------
+// The many-configuration solve's preconditioner (amg_solve_many): contexts whose fine SAP
+// runs the 16-bit-basis kernel on blocks of one size go through their K- or V-cycles in
+// lock step, and each colour's block solves of all of them are one launch over a table of
+// (lattice, block) columns instead of one launch per lattice.  Everything else a context
+// launches stays on its own stream; the shared launch runs on the first context's stream,
+// which waits for every context's residual before it, and every stream waits for it after.
+// AMG_SAP_GROUP=0 keeps one launch per lattice (A/B tests).
+// ---------------------------------------------------------------------------------
+bool sap_group_enabled() {
+    static const int on = [] {
+        const char* e = getenv("AMG_SAP_GROUP");
+        return (e && e[0] == '0') ? 0 : 1;
+    }();
+    return on != 0;
+}
+
+// block size of the context's fine SAP if the group can run it, else 0
+int group_block_size(const amg_context* c) {
+    const amg_params& p = c->p;
+    const LevelHost& h = c->lv[0];
+    const int S = h.sxe * h.ste;
+    if (p.precision != AMG_PREC_MIXED || c->precond != AMG_PRECOND_MG || p.nu1 != 0 || c->L < 2 ||
+        p.link_storage != AMG_LINKS_F16 || p.sap_gmres_m != 5 || h.ste % 4 != 0 || sap_fuse_enabled() ||
+        c->prof_on || !sap0_warp_enabled())
+        return 0;
+    return (S == 256 || S == 512 || S == 1024) ? S : 0;
+}
+
+struct SapGroup {
+    std::vector<amg_context*> cs;
+    std::vector<int> R;
+    int S = 0, ncols = 0, max_rhs = 0;
+    bool bf = true;
+    DevBuf tasks, cols;              // SapTask [2][n]; col_task [2][ncols] then col_seg [2][ncols]
+    std::vector<cudaEvent_t> ev;     // per context: its work up to the shared launch
+    cudaEvent_t join = nullptr;      // the shared launch
+    SapGroup() = default;
+    SapGroup(const SapGroup&) = delete;
+    SapGroup& operator=(const SapGroup&) = delete;
+    ~SapGroup() {
+        for (auto e : ev) if (e) cudaEventDestroy(e);
+        if (join) cudaEventDestroy(join);
+    }
+
+    int build(const std::vector<amg_context*>& cs_, const std::vector<int>& R_) {
+        cs = cs_;
+        R = R_;
+        const int n = (int)cs.size();
+        S = group_block_size(cs[0]);
+        bf = false;
+        for (auto* c : cs) bf |= c->sap_variant != SAP_VARIANT_HALF;   // FP16 basis only if every context chose it
+        std::vector<SapTask> t(2 * n);
+        std::vector<int> col_task, col_seg;
+        ncols = 0;
+        max_rhs = 0;
+        for (int i = 0; i < n; i++) ncols += cs[i]->lv[0].ncol;
+        col_task.resize(2 * ncols);
+        col_seg.resize(2 * ncols);
+        for (int q = 0; q < 2; q++) {
+            int col = q * ncols;
+            for (int i = 0; i < n; i++) {
+                amg_context* c = cs[i];
+                const LevelHost& h = c->lv[0];
+                const Links<float> U = fine_links<float>(c, c->f);
+                const int* red = c->f.red_black.template as<int>();
+                SapTask& k = t[q * n + i];
+                k.U = U.p;
+                k.r = c->f.sap_r.as<float2>();
+                k.x = c->zf.as<float2>();
+                k.blocks = q == 0 ? red : red + h.ncol;
+                k.act = c->sap_flags.as<int>();
+                k.ncol = h.ncol;
+                k.nrhs = R[i];
+                k.nx = c->nx;
+                k.nt = c->nt;
+                k.sbt = h.sbt;
+                k.sxe = h.sxe;
+                k.ste = h.ste;
+                k.restarts = c->p.sap_gmres_restarts;
+                k.m0 = (float)c->m0;
+                k.tol = (float)c->p.sap_gmres_tol;
+                for (int s = 0; s < h.ncol; s++, col++) {
+                    col_task[col] = q * n + i;
+                    col_seg[col] = s;
+                }
+                max_rhs = std::max(max_rhs, R[i]);
+            }
+        }
+        amg_context* c0 = cs[0];
+        CKR(tasks.alloc(t.size() * sizeof(SapTask)));
+        CKR(cols.alloc(4 * (size_t)ncols * sizeof(int)));
+        CK(cudaMemcpyAsync(tasks.p, t.data(), t.size() * sizeof(SapTask), cudaMemcpyHostToDevice, c0->stream));
+        CK(cudaMemcpyAsync(cols.p, col_task.data(), 2 * (size_t)ncols * sizeof(int), cudaMemcpyHostToDevice,
+                           c0->stream));
+        CK(cudaMemcpyAsync(cols.as<int>() + 2 * ncols, col_seg.data(), 2 * (size_t)ncols * sizeof(int),
+                           cudaMemcpyHostToDevice, c0->stream));
+        ev.assign(n, nullptr);
+        for (auto& e : ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+        CK(cudaStreamSynchronize(c0->stream));   // the host tables may go
+        return AMG_OK;
+    }
+
+    // one colour's block solves of every context (src/sap.cpp:64-174, the colour loop)
+    int shared_launch(int colour) {
+        const int n = (int)cs.size();
+        cudaStream_t s0 = cs[0]->stream;
+        for (int i = 1; i < n; i++) {
+            CK(cudaEventRecord(ev[i], cs[i]->stream));
+            CK(cudaStreamWaitEvent(s0, ev[i], 0));
+        }
+        const int* ct = cols.as<int>() + colour * ncols;
+        CK(launch_sap0_h_group(tasks.as<SapTask>(), ct, ct + 2 * ncols, ncols, max_rhs, S, bf, s0));
+        CK(cudaEventRecord(join, s0));
+        for (int i = 1; i < n; i++) CK(cudaStreamWaitEvent(cs[i]->stream, join, 0));
+        return AMG_OK;
+    }
+
+    // fine_sap<float>(c, c->f, v, len, x, nu, R, 0) of every context, the block solves shared
+    int sap(const std::vector<const float2*>& v, const std::vector<float2*>& x, int nu) {
+        const int n = (int)cs.size();
+        for (int i = 0; i < n; i++) {
+            amg_context* c = cs[i];
+            const long long len = vlen0(c);
+            int* act = c->sap_flags.as<int>();
+            double* vnorm2 = c->norms.as<double>();
+            k_set_int<<<1, 256, 0, c->stream>>>(act, 1, R[i]);
+            k_set_int<<<1, 256, 0, c->stream>>>(act + c->Rcap, 0, R[i]);
+            count_launch(2);
+            launch_norm2<float>(v[i], len, len, R[i], c->partial.as<double>(), vnorm2, c->stream);
+            launch_residual<float>(fine_links<float>(c, c->f), v[i], len, x[i], c->f.sap_r.as<float2>(), c->nx, c->nt,
+                                   R[i], (float)c->m0, nullptr, nullptr, nullptr, c->stream);
+        }
+        for (int it = 0; it < nu; it++) {
+            for (int colour = 0; colour < 2; colour++) {
+                CKR(shared_launch(colour));
+                if (colour == 1 && it == nu - 1) break;
+                for (int i = 0; i < n; i++) {
+                    amg_context* c = cs[i];
+                    int* act = c->sap_flags.as<int>();
+                    double* vnorm2 = c->norms.as<double>();
+                    double* norm2 = vnorm2 + c->Rcap;
+                    launch_residual<float>(fine_links<float>(c, c->f), v[i], vlen0(c), x[i], c->f.sap_r.as<float2>(),
+                                           c->nx, c->nt, R[i], (float)c->m0, c->partial.as<double>(),
+                                           colour == 1 ? norm2 : nullptr, act, c->stream);
+                    if (colour == 1) {
+                        k_sap_check<<<1, 256, 0, c->stream>>>(norm2, vnorm2, c->p.sap_tol, act, act + c->Rcap, R[i]);
+                        count_launch(1);
+                    }
+                }
+            }
+        }
+        for (auto* c : cs) CKL();
+        return AMG_OK;
+    }
+
+    // z = M v (FGMRES_AMG::preconditioner, include/amg.h:134-144) for every context in the
+    // mixed form, the FP32 result left in each context's zf (as precondition(.., false))
+    int precondition(const std::vector<const double2*>& v) {
+        const int n = (int)cs.size();
+        std::vector<const float2*> vf(n);
+        std::vector<float2*> zf(n);
+        for (int i = 0; i < n; i++) {
+            amg_context* c = cs[i];
+            const long long len = vlen0(c);
+            vf[i] = c->vf.as<float2>();
+            zf[i] = c->zf.as<float2>();
+            if (c->vf_src != v[i]) {
+                launch_d2f(c->vf.as<float2>(), v[i], R[i] * len, c->stream);
+                c->vf_src = v[i];
+            }
+            CK(cudaMemsetAsync(zf[i], 0, (size_t)R[i] * len * sizeof(float2), c->stream));
+            // fine_cycle<float> with psi = 0 on entry and no pre-smoothing: r = eta
+            const LevelHost& h1 = c->lv[1];
+            const long long n1 = (long long)h1.n * h1.K;
+            float2* eta1 = c->f.eta1.as<float2>();
+            float2* psi1 = c->f.psi1.as<float2>();
+            fine_restrict<float>(c, c->f, vf[i], eta1, R[i]);
+            if (c->p.cycle == AMG_CYCLE_K) {
+                CKR(run_engine<float>(c, c->f, ENG_KFGMRES, 1, 0, eta1, n1, psi1, n1, R[i]));
+            } else {
+                CK(cudaMemsetAsync(psi1, 0, (size_t)R[i] * n1 * sizeof(float2), c->stream));
+                CKR(run_engine<float>(c, c->f, ENG_VCYCLE, 1, 0, eta1, n1, psi1, n1, R[i]));
+            }
+            fine_prolong_add<float>(c, c->f, psi1, zf[i], R[i]);
+        }
+        if (cs[0]->p.nu2 > 0) CKR(sap(vf, zf, cs[0]->p.nu2));
+        for (auto* c : cs) CKL();
+        return AMG_OK;
+    }
+};
+
+// ---------------------------------------------------------------------------------
 // Autotuner: on a context's first solve, time one preconditioner application (the first
 // Krylov vector, R sources) for every fine SAP kernel variant that applies (FP32: paired
 // MGS, paired CGS, communication-avoiding, lean, and with FP16 links the FP16- and
@@ -833,7 +1027,10 @@ int autotune(amg_context* c, const double2* v, double2* z, int R) {
 // runs one context's kernels while the host handles another's Givens rotations.
 // ---------------------------------------------------------------------------------
 struct OuterSolve {
-    enum Phase { INIT, STEP, RESTART, DONE };
+    // PRECOND: a step waits for its preconditioner, which the caller runs for several
+    // contexts together (defer set: amg_solve_many's grouped SAP), then issue_step_post
+    enum Phase { INIT, STEP, RESTART, PRECOND, DONE };
+    bool defer = false;
     amg_context* c = nullptr;
     const double2* b = nullptr;
     double2* x = nullptr;
@@ -940,14 +1137,29 @@ struct OuterSolve {
     int issue_step() {
         double2* V = c->V.as<double2>();
         double2* Z = c->Z.as<double2>();
-        double2* w = c->w.as<double2>();
-        double2* dpart = c->partial.as<double2>();
-        double2* dots = c->dots.as<double2>();
         double2* Vj = V + (long long)j * vstride;
         double2* Zj = Z + (long long)j * vstride;
         if (!c->tuned && !c->prof_on && c->precond != AMG_PRECOND_NONE) CKR(autotune(c, Vj, Zj, R));
+        if (defer && group_block_size(c)) {
+            phase = PRECOND;
+            return AMG_OK;
+        }
         const bool mixed = c->p.precision == AMG_PREC_MIXED && c->precond != AMG_PRECOND_NONE;
         CKR(precondition(c, Vj, Zj, R, !mixed));
+        return issue_step_post();
+    }
+    // the basis vector step j preconditions (the grouped preconditioner's input)
+    const double2* step_input() const { return c->V.as<double2>() + (long long)j * vstride; }
+
+    // the rest of Arnoldi step j once z_j is in c->zf (mixed) or Z_j: w = D z_j, CGS2, V_{j+1}
+    int issue_step_post() {
+        double2* V = c->V.as<double2>();
+        double2* Z = c->Z.as<double2>();
+        double2* w = c->w.as<double2>();
+        double2* dpart = c->partial.as<double2>();
+        double2* dots = c->dots.as<double2>();
+        double2* Zj = Z + (long long)j * vstride;
+        const bool mixed = c->p.precision == AMG_PREC_MIXED && c->precond != AMG_PRECOND_NONE;
         {
             ProfScope ps_(c, AMG_PROF_FINE_OP, (double)c->N * (2.0 + 4.0 * R) * sizeof(double2));
             if (mixed)   // w = D z_j from the FP32 preconditioner output, Z_j = its FP64 promotion
@@ -2142,14 +2354,49 @@ int solve_many(int count, const amg_ctx* ctx, const double2* const* b, double2* 
         CK(cudaEventRecord(ctx[i]->ev0, ctx[i]->stream));
         CKR(S[i].init(ctx[i], b[i], x[i], nrhs[i], info ? info[i] : nullptr));
     }
+    // grouped preconditioners (SapGroup): contexts whose steps wait in PRECOND, keyed by
+    // device, block size and post-smoothing count, share their SAP launches
+    const bool group = count > 1 && sap_group_enabled();
+    for (int i = 0; i < count; i++) S[i].defer = group;
+    std::map<std::vector<amg_context*>, std::unique_ptr<SapGroup>> groups;
     for (bool busy = true; busy;) {
         busy = false;
         for (int i = 0; i < count; i++) {
             if (S[i].phase == OuterSolve::DONE) continue;
             busy = true;
+            if (S[i].phase == OuterSolve::PRECOND) continue;
             CKR(select_device(ctx[i]));
             CK(cudaEventSynchronize(ctx[i]->ev_host));
             CKR(S[i].advance());
+        }
+        std::map<std::tuple<int, int, int>, std::vector<int>> waiting;
+        for (int i = 0; i < count; i++)
+            if (S[i].phase == OuterSolve::PRECOND)
+                waiting[std::make_tuple(ctx[i]->device, group_block_size(ctx[i]), ctx[i]->p.nu2)].push_back(i);
+        for (auto& kv : waiting) {
+            const std::vector<int>& ids = kv.second;
+            CKR(select_device(ctx[ids[0]]));
+            if (ids.size() == 1) {
+                // nobody to share with: the context's own (graph-captured) preconditioner
+                OuterSolve& s = S[ids[0]];
+                CKR(precondition(s.c, s.step_input(), nullptr, s.R, false));
+            } else {
+                std::vector<amg_context*> cs;
+                std::vector<int> R;
+                std::vector<const double2*> v;
+                for (int i : ids) {
+                    cs.push_back(ctx[i]);
+                    R.push_back(S[i].R);
+                    v.push_back(S[i].step_input());
+                }
+                std::unique_ptr<SapGroup>& g = groups[cs];
+                if (!g) {
+                    g.reset(new SapGroup());
+                    CKR(g->build(cs, R));
+                }
+                CKR(g->precondition(v));
+            }
+            for (int i : ids) CKR(S[i].issue_step_post());
         }
     }
     int rc = AMG_OK;

@@ -1092,6 +1092,34 @@ cudaError_t launch_sap0_h(const __half2* U, float2* r, float2* x, const int* blo
                                                         tol, act, iters);
     return cudaGetLastError();
 }
+template <int NW, bool BF>
+static cudaError_t launch_sap0_h_group_nw(const SapTask* tasks, const int* col_task, const int* col_seg, int ncols,
+                                          int max_rhs, cudaStream_t s) {
+    constexpr int bytes = sap0_h_smem<5, 4, NW>();
+    cudaError_t e = cudaFuncSetAttribute(k_sap0_h_group<5, 4, NW, BF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_sap0_h_group<5, 4, NW, BF>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared);
+    if (e != cudaSuccess) return e;
+    k_sap0_h_group<5, 4, NW, BF><<<dim3(ncols, max_rhs), 32 * NW, bytes, s>>>(tasks, col_task, col_seg);
+    return cudaGetLastError();
+}
+cudaError_t launch_sap0_h_group(const SapTask* tasks, const int* col_task, const int* col_seg, int ncols, int max_rhs,
+                                int S, bool bf, cudaStream_t s) {
+    count_launch(1);
+    if (ncols < 1 || max_rhs < 1 || max_rhs > 65535) return cudaErrorInvalidValue;
+    switch (S) {
+        case 256: return bf ? launch_sap0_h_group_nw<2, true>(tasks, col_task, col_seg, ncols, max_rhs, s)
+                            : launch_sap0_h_group_nw<2, false>(tasks, col_task, col_seg, ncols, max_rhs, s);
+        case 512: return bf ? launch_sap0_h_group_nw<4, true>(tasks, col_task, col_seg, ncols, max_rhs, s)
+                            : launch_sap0_h_group_nw<4, false>(tasks, col_task, col_seg, ncols, max_rhs, s);
+        case 1024: return bf ? launch_sap0_h_group_nw<8, true>(tasks, col_task, col_seg, ncols, max_rhs, s)
+                             : launch_sap0_h_group_nw<8, false>(tasks, col_task, col_seg, ncols, max_rhs, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
 template <bool BF>
 static cudaError_t launch_sap0_h_shape(const __half2* U, float2* r, float2* x, const int* blocks, int ncol, int nrhs,
                                        int nx, int nt, int sbt, int sxe, int ste, float m0, int restarts, float tol,

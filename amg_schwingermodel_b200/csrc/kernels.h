@@ -54,6 +54,22 @@ cudaError_t launch_sap0(const Links<T> U, cx<T>* r, cx<T>* x, const int* blocks,
                         int nt, int sbt, int sxe, int ste, T m0, int m, int restarts, T tol, int use_smem,
                         cx<T>* gscratch, int* iters, const int* act, cudaStream_t s, int variant = -1,
                         const cx<T>* vfuse = nullptr, long long vstride = 0);
+// One lattice's share of a grouped launch of the 16-bit-basis SAP kernel: its FP16 links, SAP
+// residual r, iterate x, the colour's block list and its per-source active flags.
+struct SapTask {
+    const void* U;
+    float2* r;
+    float2* x;
+    const int* blocks;
+    const int* act;
+    int ncol, nrhs, nx, nt, sbt, sxe, ste, restarts;
+    float m0, tol;
+};
+// The block solves of one colour on several lattices with blocks of S = 256, 512 or 1024
+// sites in one launch: column c of the grid solves block col_seg[c] of task col_task[c]
+// (tasks and both column tables in device memory), row y its source y.
+cudaError_t launch_sap0_h_group(const SapTask* tasks, const int* col_task, const int* col_seg, int ncols,
+                                int max_rhs, int S, bool bf, cudaStream_t s);
 void launch_multidot(const double2* w, const double2* V, long long len, long long vstride, int nv, int nrhs,
                      double2* partial, int nparts, double2* out, const int* act, cudaStream_t s);
 void launch_axpy_multidot(double2* w, const double2* V, long long len, long long vstride, int nv, const double2* h,

@@ -81,16 +81,14 @@ __host__ __device__ constexpr int sap0_h_smem() {
     return 32 * NW * SPT * (16 + 16 + 8 * M) + ((M * M + 1) & ~1) * 8 + 2 * 2 * NW * 8 + (4 * M + 1) * 8 + 16;
 }
 
-template <int M, int SPT, int NW, bool BF = false>
-__global__ void __launch_bounds__(32 * NW, 3) k_sap0_h(const __half2* __restrict__ U, float2* __restrict__ r,
-                                                        float2* __restrict__ xg, const int* __restrict__ blocks,
-                                                        int ncol, int nx, int nt, int sbt, int sxe, int ste, float m0,
-                                                        int restarts, float tol, const int* __restrict__ act,
-                                                        int* __restrict__ iters_out) {
+// the block solve of block blocks[seg] for source rhs (called by every thread of the CTA)
+template <int M, int SPT, int NW, bool BF>
+__device__ __forceinline__ void sap0_h_solve(const __half2* __restrict__ U, float2* __restrict__ r,
+                                             float2* __restrict__ xg, const int* __restrict__ blocks, int ncol,
+                                             int nx, int nt, int sbt, int sxe, int ste, float m0, int restarts,
+                                             float tol, int* __restrict__ iters_out, int seg, int rhs) {
     constexpr int TPB = 32 * NW, S = TPB * SPT, PST = 2 * NW;
     extern __shared__ __align__(16) unsigned char smraw_h[];
-    const int seg = blockIdx.x, rhs = blockIdx.y;
-    if (act && !act[rhs]) return;
     float4* X = reinterpret_cast<float4*>(smraw_h);   // [S] iterate (FP32)
     uint4* LK = reinterpret_cast<uint4*>(X + S);      // [S] folded hop links (FP16)
     uint2* V = reinterpret_cast<uint2*>(LK + S);      // [M][S] basis (FP16)
@@ -407,6 +405,33 @@ __global__ void __launch_bounds__(32 * NW, 3) k_sap0_h(const __half2* __restrict
         xo[gs0 + k] = o;
     }
     if (iters_out && tid == 0) iters_out[rhs * ncol + seg] = ret;
+}
+
+// one launch per colour and lattice: CTA (seg, rhs)
+template <int M, int SPT, int NW, bool BF = false>
+__global__ void __launch_bounds__(32 * NW, 3) k_sap0_h(const __half2* __restrict__ U, float2* __restrict__ r,
+                                                        float2* __restrict__ xg, const int* __restrict__ blocks,
+                                                        int ncol, int nx, int nt, int sbt, int sxe, int ste, float m0,
+                                                        int restarts, float tol, const int* __restrict__ act,
+                                                        int* __restrict__ iters_out) {
+    const int seg = blockIdx.x, rhs = blockIdx.y;
+    if (act && !act[rhs]) return;
+    sap0_h_solve<M, SPT, NW, BF>(U, r, xg, blocks, ncol, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters_out, seg,
+                                 rhs);
+}
+
+// one launch per colour over several lattices (the many-configuration solve): column c of
+// the grid is block col_seg[c] of task col_task[c]; rows beyond a task's sources and
+// inactive sources return at once
+template <int M, int SPT, int NW, bool BF = false>
+__global__ void __launch_bounds__(32 * NW, 3) k_sap0_h_group(const SapTask* __restrict__ tasks,
+                                                              const int* __restrict__ col_task,
+                                                              const int* __restrict__ col_seg) {
+    const SapTask& k = tasks[col_task[blockIdx.x]];
+    const int rhs = blockIdx.y;
+    if (rhs >= k.nrhs || (k.act && !k.act[rhs])) return;
+    sap0_h_solve<M, SPT, NW, BF>(static_cast<const __half2*>(k.U), k.r, k.x, k.blocks, k.ncol, k.nx, k.nt, k.sbt,
+                                 k.sxe, k.ste, k.m0, k.restarts, k.tol, nullptr, col_seg[blockIdx.x], rhs);
 }
 
 }  // namespace amgb
