@@ -951,8 +951,9 @@ struct SapGroup {
 // ---------------------------------------------------------------------------------
 // Autotuner: on a context's first solve, time one preconditioner application (the first
 // Krylov vector, R sources) for every fine SAP kernel variant that applies (FP32: paired
-// MGS, paired CGS, communication-avoiding, lean, and with FP16 links the FP16- and
-// BF16-basis kernels; FP64: lean) and every engine cluster size
+// MGS with four or two sites per thread, paired CGS, communication-avoiding, lean, and with
+// FP16 links the FP16- and BF16-basis kernels at three CTAs per SM; FP64: lean) and every
+// engine cluster size
 // the device can schedule, and keep the fastest.  An environment override (AMG_SAP_KERNEL,
 // AMG_ENGINE_CLUSTER) fixes that dimension instead.
 // ---------------------------------------------------------------------------------
@@ -962,7 +963,7 @@ int autotune(amg_context* c, const double2* v, double2* z, int R) {
     const bool mixed = c->p.precision == AMG_PREC_MIXED;
     std::vector<int> variants{-1};
     if (!getenv("AMG_SAP_KERNEL") && mixed) {
-        variants = {SAP_VARIANT_PAIRED, SAP_VARIANT_CGS, SAP_VARIANT_CA, SAP_VARIANT_LEAN};
+        variants = {SAP_VARIANT_PAIRED, SAP_VARIANT_PAIRED2, SAP_VARIANT_CGS, SAP_VARIANT_CA, SAP_VARIANT_LEAN};
         if (c->p.link_storage == AMG_LINKS_F16) {
             variants.push_back(SAP_VARIANT_HALF);
             variants.push_back(SAP_VARIANT_BF16B);

@@ -1145,7 +1145,8 @@ static cudaError_t launch_sap0_paired(const Links<float> U, float2* r, float2* x
     // the paired kernel gives each thread a run of SPT consecutive t sites (SPT = 2 for 64-site
     // blocks or the MGS form with AMG_SAP_SPT=2, else 4), so the block's t extent must be a
     // multiple of it
-    const int spt = (S == 64 || (v != SAP_VARIANT_CGS && g_sap0_spt == 2)) ? 2 : 4;
+    const bool two = v == SAP_VARIANT_PAIRED2 || (v != SAP_VARIANT_CGS && g_sap0_spt == 2);
+    const int spt = (S == 64 || two) ? 2 : 4;
     if (v != SAP_VARIANT_CA && ste % spt != 0) {
         *done = false;
         return cudaSuccess;
@@ -1170,7 +1171,7 @@ static cudaError_t launch_sap0_paired(const Links<float> U, float2* r, float2* x
             default: break;
         }
     }
-    if (g_sap0_spt == 2) {
+    if (two) {
         switch (S) {
             case 64: return launch_sap0_f32<2, 1>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s, vsrc, vstride);
             case 128: return launch_sap0_f32<2, 2>(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts, tol, iters, act, s, vsrc, vstride);
@@ -1217,8 +1218,10 @@ cudaError_t launch_sap0(const Links<T> U, cx<T>* r, cx<T>* x, const int* blocks,
         // otherwise the residual runs as its own launch first
         bool fused = false;
         if constexpr (std::is_same<T, float>::value) {
-            const int spt = (S == 64 || (v != SAP_VARIANT_CGS && g_sap0_spt == 2)) ? 2 : 4;
-            fused = m == 5 && (v == SAP_VARIANT_PAIRED || v == SAP_VARIANT_CGS) && S >= 64 && S <= 1024 &&
+            const bool two = v == SAP_VARIANT_PAIRED2 || (v != SAP_VARIANT_CGS && g_sap0_spt == 2);
+            const int spt = (S == 64 || two) ? 2 : 4;
+            fused = m == 5 && (v == SAP_VARIANT_PAIRED || v == SAP_VARIANT_PAIRED2 || v == SAP_VARIANT_CGS) &&
+                    S >= 64 && S <= 1024 &&
                     (S & (S - 1)) == 0 && ste % spt == 0 && (nx / sxe) % 2 == 0 && sbt % 2 == 0;
         }
         if (!fused) {
@@ -1240,7 +1243,8 @@ cudaError_t launch_sap0(const Links<T> U, cx<T>* r, cx<T>* x, const int* blocks,
             }
             v = SAP_VARIANT_PAIRED;
         }
-        if (m == 5 && (v == SAP_VARIANT_PAIRED || v == SAP_VARIANT_CA || v == SAP_VARIANT_CGS)) {
+        if (m == 5 && (v == SAP_VARIANT_PAIRED || v == SAP_VARIANT_PAIRED2 || v == SAP_VARIANT_CA ||
+                       v == SAP_VARIANT_CGS)) {
             bool done = false;
             const cudaError_t e = launch_sap0_paired(U, r, x, blocks, ncol, nrhs, nx, nt, sbt, sxe, ste, m0, restarts,
                                                      tol, iters, act, s, &done, v, vfuse, vstride);

@@ -42,10 +42,11 @@ int sap0_smem_bytes(int S, int m, int use_smem);
 int sap0_warp_enabled();
 void set_sap0_warp(int on);
 // fine-level SAP block solvers: generic (any block), lean (MGS, one CTA per block), paired
-// (FP32 MGS with two-wide arithmetic), ca (FP32 communication-avoiding GMRES), cgs (the
-// paired kernel with classical Gram-Schmidt and re-orthogonalisation on demand)
+// (FP32 MGS with two-wide arithmetic, four sites per thread; paired2: two, twice the
+// threads), ca (FP32 communication-avoiding GMRES), cgs (the paired kernel with classical
+// Gram-Schmidt and re-orthogonalisation on demand), half / bf16b (16-bit Krylov basis)
 enum { SAP_VARIANT_GENERIC = 0, SAP_VARIANT_LEAN = 1, SAP_VARIANT_PAIRED = 2, SAP_VARIANT_CA = 3, SAP_VARIANT_CGS = 4,
-       SAP_VARIANT_HALF = 5, SAP_VARIANT_BF16B = 6 };
+       SAP_VARIANT_HALF = 5, SAP_VARIANT_BF16B = 6, SAP_VARIANT_PAIRED2 = 7 };
 template <typename T>
 // vfuse (optional): the SAP right-hand side v; r = v - D x is then formed for the colour's
 // blocks inside the launch (in a separate residual launch where the chosen kernel cannot)
