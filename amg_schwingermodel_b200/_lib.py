@@ -112,7 +112,7 @@ SIGNATURES = {
     "amg_engine_counters": (_I, [_P, _P, _I]),
 }
 
-PROF_SLOTS = {"sap": 0, "engine": 1, "restrict": 2, "prolong": 3, "fine_op": 4, "blas": 5}
+PROF_SLOTS = {"sap": 0, "engine": 1, "restrict": 2, "prolong": 3, "fine_op": 4, "blas": 5, "outer_op": 6}
 
 
 def lib() -> C.CDLL:

@@ -360,6 +360,18 @@ int check_fine_waits(cudaStream_t s) {
     return AMG_OK;
 }
 
+// Teams (concurrent coarse SAP block solves) per engine CTA for blocks of up to 1024 dof:
+// 4, or AMG_ENGINE_SAP_TEAMS = 1 or 2 (fewer, larger teams: a block's links stay in L1 across
+// its GMRES steps, at the price of more rounds per colour)
+int engine_sap_teams() {
+    static const int n = [] {
+        const char* e = getenv("AMG_ENGINE_SAP_TEAMS");
+        const int v = e ? atoi(e) : 4;
+        return (v == 1 || v == 2) ? v : 4;
+    }();
+    return n;
+}
+
 int engine_cluster_limit() {
     const char* e = getenv("AMG_ENGINE_CLUSTER");
     int v = e ? atoi(e) : 16;
@@ -423,7 +435,7 @@ int build_engine(amg_context* c, PrecSet<T>& ps, int nsrc) {
             e.off_cyc = off; off += al(nvec + 2 * ncv);
             const long long seglen = (long long)h.sxe * h.ste * h.K;
             e.off_sap = off; off += al(nvec + (long long)h.ncol * seglen);
-            e.sap_nteam = seglen <= 1024 ? 4 : 1;
+            e.sap_nteam = seglen <= 1024 ? engine_sap_teams() : 1;
             e.sap_vec_smem = 0;
             e.off_sapteam = off; off += al((long long)e.sap_nteam * (p.sap_gmres_m + 4) * seglen);
         }
@@ -1162,7 +1174,9 @@ struct OuterSolve {
         double2* Zj = Z + (long long)j * vstride;
         const bool mixed = c->p.precision == AMG_PREC_MIXED && c->precond != AMG_PRECOND_NONE;
         {
-            ProfScope ps_(c, AMG_PROF_FINE_OP, (double)c->N * (2.0 + 4.0 * R) * sizeof(double2));
+            // algorithmic bytes per site: the links (2 x 16 B) and per source z_j in (FP32:
+            // 16 B, FP64: 32 B) and w out (32 B), plus Z_j out (32 B) in the mixed form
+            ProfScope ps_(c, AMG_PROF_OUTER_OP, (double)c->N * (32.0 + (mixed ? 80.0 : 64.0) * R));
             if (mixed)   // w = D z_j from the FP32 preconditioner output, Z_j = its FP64 promotion
                 launch_dirac_promote(c->d.U.as<double2>(), c->zf.as<float2>(), w, Zj, c->nx, c->nt, R, c->m0,
                                      c->stream);

@@ -630,6 +630,14 @@ def run_ours(args, world, rank, local):
     d_gbs = d_bytes / (d_ms * 1e-3) / 1e9
     del vin, vout, Ud
 
+    po = prof.get("outer_op", {})
+    outer_op = None
+    if po.get("launches"):
+        ms_l = po["ms"] / po["launches"]
+        by_l = po["bytes"] / po["launches"]
+        outer_op = {"gbs": by_l / (ms_l * 1e-3) / 1e9, "frac": by_l / (ms_l * 1e-3) / 1e9 / hbm, "peak": peak_kind,
+                    "ms_per_launch": ms_l, "bytes_per_launch": by_l, "nrhs": R}
+
     # ---- roofline of the dominant kernel class of the step
     dom = max(prof, key=lambda k: prof[k]["ms"])
     pd = prof[dom]
@@ -707,6 +715,9 @@ def run_ours(args, world, rank, local):
             "speedup_vs_fp64_dropin": value / fp64_value,
             "dapply": {"gbs": d_gbs, "frac": d_gbs / hbm, "peak_gbs": hbm, "peak": peak_kind,
                        "ms_per_launch": d_ms, "nrhs": nd, "bytes_per_launch": d_bytes},
+            # the D apply inside the solve: the outer step's w = D z_j from the FP32 z_j, with
+            # z_j's FP64 promotion written by the same pass (R sources per launch)
+            "dapply_outer": outer_op,
             "roofline": roofline,
             "kernels": prof,
             "e2e": {"value": e2e_value, "unit": UNIT, "api": "amg_solve_stream", "same_x_as_device_run": e2e_matches,

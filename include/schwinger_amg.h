@@ -278,14 +278,16 @@ AMG_API int amg_force_dev(amg_ctx ctx, const void* lambda_dev, const void* x_dev
 /* ---- timing and profiling ---------------------------------------------------------- */
 /* Kernel classes timed by amg_profile (CUDA events on the context's stream around each
  * launch): the fine SAP block solves, the coarse-level engine, fine restriction and
- * prolongation, the fine stencil / residual, and the outer FGMRES orthogonalisation. */
+ * prolongation, the fine stencil / residual inside the cycle, the outer FGMRES
+ * orthogonalisation, and the outer step's operator w = D z_j. */
 #define AMG_PROF_SAP 0
 #define AMG_PROF_ENGINE 1
 #define AMG_PROF_RESTRICT 2
 #define AMG_PROF_PROLONG 3
 #define AMG_PROF_FINE_OP 4
 #define AMG_PROF_BLAS 5
-#define AMG_PROF_SLOTS 6
+#define AMG_PROF_OUTER_OP 6
+#define AMG_PROF_SLOTS 7
 /* Enables (1) or disables (0) per-class timing and clears the accumulated values. */
 AMG_API int amg_profile(amg_ctx ctx, int enable);
 /* Accumulated device milliseconds, launch count and algorithmic bytes of one class. */
