@@ -327,13 +327,13 @@ class AMGContext:
               "amg_force_dev")
 
     def autotune_info(self) -> dict:
-        """The autotuner's choice (amg_autotune_info)."""
-        o = np.zeros(4, dtype=np.int32)
-        check(lib().amg_autotune_info(self._h, _cptr(o)), "amg_autotune_info")
+        """The autotuner's choice (amg_autotune_info_n)."""
+        o = np.zeros(5, dtype=np.int32)
+        check(lib().amg_autotune_info_n(self._h, _cptr(o), 5), "amg_autotune_info_n")
         names = {-1: "default", 0: "generic", 1: "lean", 2: "paired_f32", 3: "ca_f32", 4: "cgs_f32", 5: "half_basis",
                  6: "bf16_basis", 7: "paired_f32_spt2"}
         return dict(tuned=bool(o[0]), sap_kernel=names.get(int(o[1]), str(o[1])), engine_cluster=int(o[2]),
-                    tuned_cycle_us=int(o[3]))
+                    engine_sap_teams=int(o[4]), tuned_cycle_us=int(o[3]))
 
     def residual_history(self) -> np.ndarray:
         n = C.c_int(0)

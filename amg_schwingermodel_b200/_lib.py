@@ -105,6 +105,7 @@ SIGNATURES = {
     "amg_force_dev": (_I, [_P, _P, _P, _I, _P]),
     "amg_last_timings": (_I, [_P, C.POINTER(_D), C.POINTER(_D)]),
     "amg_autotune_info": (_I, [_P, _P]),
+    "amg_autotune_info_n": (_I, [_P, _P, _I]),
     "amg_profile": (_I, [_P, _I]),
     "amg_profile_query": (_I, [_P, _I, C.POINTER(_D), C.POINTER(C.c_longlong), C.POINTER(_D)]),
     "amg_launch_count": (C.c_longlong, []),

@@ -184,6 +184,7 @@ struct PrecSet {
     int max_cluster = 1;             // largest engine cluster the slabs are sized for
     int cluster_cache[17] = {0};     // engine_max_clusters(c) + 1, 0 = not queried
     int cluster_pick = 0;            // the autotuner's cluster size (0: largest single-wave size)
+    int sap_teams = 0;               // the autotuner's coarse SAP teams per engine CTA (0: default)
     DevBuf r0, eta1, psi1, rpart, sap_r, sap_scratch;
     int ready = 0;
 };
@@ -360,14 +361,15 @@ int check_fine_waits(cudaStream_t s) {
     return AMG_OK;
 }
 
-// Teams (concurrent coarse SAP block solves) per engine CTA for blocks of up to 1024 dof:
-// 4, or AMG_ENGINE_SAP_TEAMS = 1 or 2 (fewer, larger teams: a block's links stay in L1 across
-// its GMRES steps, at the price of more rounds per colour)
+// Teams (concurrent coarse SAP block solves) per engine CTA for blocks of up to 1024 dof,
+// before the autotuner picks (or fixed by AMG_ENGINE_SAP_TEAMS = 1, 2 or 4): fewer, larger
+// teams keep a block's links in L1 across its GMRES steps and split each step over more
+// threads, at the price of more rounds per colour
 int engine_sap_teams() {
     static const int n = [] {
         const char* e = getenv("AMG_ENGINE_SAP_TEAMS");
-        const int v = e ? atoi(e) : 4;
-        return (v == 1 || v == 2) ? v : 4;
+        const int v = e ? atoi(e) : 2;
+        return (v == 1 || v == 4) ? v : 2;
     }();
     return n;
 }
@@ -435,9 +437,10 @@ int build_engine(amg_context* c, PrecSet<T>& ps, int nsrc) {
             e.off_cyc = off; off += al(nvec + 2 * ncv);
             const long long seglen = (long long)h.sxe * h.ste * h.K;
             e.off_sap = off; off += al(nvec + (long long)h.ncol * seglen);
-            e.sap_nteam = seglen <= 1024 ? engine_sap_teams() : 1;
+            // (team areas are sized for 4 teams, so the autotuner may change the count in place)
+            e.sap_nteam = seglen <= 1024 ? (ps.sap_teams ? ps.sap_teams : engine_sap_teams()) : 1;
             e.sap_vec_smem = 0;
-            e.off_sapteam = off; off += al((long long)e.sap_nteam * (p.sap_gmres_m + 4) * seglen);
+            e.off_sapteam = off; off += al(4LL * (p.sap_gmres_m + 4) * seglen);
         }
     }
     // whole-CTA reduction scratch and the team area of the SAP block solves
@@ -454,7 +457,7 @@ int build_engine(amg_context* c, PrecSet<T>& ps, int nsrc) {
         EngLevel<T>& e = a.lv[l];
         const int seglen = h.sxe * h.ste * h.K;
         const int with_vec = al16(tb_state + (p.sap_gmres_m + 4) * seglen * (int)sizeof(cx<T>));
-        if (sm + e.sap_nteam * std::max(tb, with_vec) <= 200 * 1024) {
+        if (sm + (seglen <= 1024 ? 4 : 1) * std::max(tb, with_vec) <= 200 * 1024) {
             e.sap_vec_smem = 1;
             tb = std::max(tb, with_vec);
         }
@@ -960,14 +963,31 @@ struct SapGroup {
     }
 };
 
+// Coarse SAP teams per engine CTA (1, 2 or 4) for the levels whose block vectors allow more
+// than one, in the active precision's engine arguments (host copy and device block).
+int set_sap_teams(amg_context* c, int t) {
+    auto apply = [&](auto& ps) -> int {
+        if (!ps.eng_args.p) return AMG_OK;
+        ps.sap_teams = t;
+        for (int l = 1; l < c->L; l++)
+            if (!c->lv[l].coarsest && ps.eh.lv[l].sap_nteam > 0 &&
+                (long long)c->lv[l].sxe * c->lv[l].ste * c->lv[l].K <= 1024)
+                ps.eh.lv[l].sap_nteam = t;
+        CK(cudaMemcpyAsync(ps.eng_args.p, &ps.eh, sizeof ps.eh, cudaMemcpyHostToDevice, c->stream));
+        return AMG_OK;
+    };
+    return c->p.precision == AMG_PREC_MIXED ? apply(c->f) : apply(c->d);
+}
+
 // ---------------------------------------------------------------------------------
 // Autotuner: on a context's first solve, time one preconditioner application (the first
 // Krylov vector, R sources) for every fine SAP kernel variant that applies (FP32: paired
 // MGS with four or two sites per thread, paired CGS, communication-avoiding, lean, and with
 // FP16 links the FP16- and BF16-basis kernels at three CTAs per SM; FP64: lean) and every
 // engine cluster size
-// the device can schedule, and keep the fastest.  An environment override (AMG_SAP_KERNEL,
-// AMG_ENGINE_CLUSTER) fixes that dimension instead.
+// the device can schedule, and keep the fastest; then, at that choice, the coarse SAP teams
+// per engine CTA (4, 2, 1).  An environment override (AMG_SAP_KERNEL, AMG_ENGINE_CLUSTER,
+// AMG_ENGINE_SAP_TEAMS) fixes that dimension instead.
 // ---------------------------------------------------------------------------------
 int autotune(amg_context* c, const double2* v, double2* z, int R) {
     c->tuned = 1;
@@ -1016,11 +1036,32 @@ int autotune(amg_context* c, const double2* v, double2* z, int R) {
         }
         if (rc < 0) break;
     }
+    c->sap_variant = bv;
+    *pick = bc;
+    // then the coarse SAP teams per engine CTA at that choice (the engine reads the count
+    // from its argument block, so each candidate is one upload)
+    if (rc >= 0 && !getenv("AMG_ENGINE_SAP_TEAMS")) {
+        int bt = 0;
+        float best_t = 1e30f;
+        for (int t : {4, 2, 1}) {
+            if ((rc = set_sap_teams(c, t)) < 0) break;
+            if ((rc = precondition(c, v, z, R, false)) < 0) break;
+            cudaEventRecord(a, c->stream);
+            if ((rc = precondition(c, v, z, R, false)) < 0) break;
+            cudaEventRecord(b, c->stream);
+            cudaEventSynchronize(b);
+            float ms = 0;
+            cudaEventElapsedTime(&ms, a, b);
+            if (ms < best_t) { best_t = ms; bt = t; }
+        }
+        if (rc >= 0 && bt) {
+            rc = set_sap_teams(c, bt);
+            best = best_t;
+        }
+    }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     c->graphs_off = graphs_was;
-    c->sap_variant = bv;
-    *pick = bc;
     c->tuned_us = best < 1e29f ? 1e3 * best : 0;
     c->drop_graphs();
     return rc;
@@ -2594,6 +2635,16 @@ int amg_autotune_info(amg_ctx c, int* out) {
     out[1] = c->sap_variant;
     out[2] = mixed ? c->f.cluster_pick : c->d.cluster_pick;
     out[3] = (int)c->tuned_us;
+    return AMG_OK;
+}
+
+int amg_autotune_info_n(amg_ctx c, int* out, int n) {
+    if (!c || !out || n < 0) return fail(AMG_ERR_INVALID, "bad argument");
+    int v[5];
+    CKR(amg_autotune_info(c, v));
+    const int t = c->p.precision == AMG_PREC_MIXED ? c->f.sap_teams : c->d.sap_teams;
+    v[4] = t ? t : engine_sap_teams();
+    for (int i = 0; i < std::min(n, 5); i++) out[i] = v[i];
     return AMG_OK;
 }
 

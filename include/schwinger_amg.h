@@ -303,9 +303,14 @@ AMG_API void* amg_get_stream(amg_ctx ctx);
 /* Device milliseconds of the last amg_setup / solve call (CUDA events). */
 AMG_API int amg_last_timings(amg_ctx ctx, double* setup_ms, double* solve_ms);
 /* The autotuner's choice: out[0] = 1 once tuned, out[1] = fine SAP kernel (0 generic,
- * 1 lean, 2 paired FP32, 3 communication-avoiding FP32; -1 default), out[2] = engine cluster
- * size (0 default), out[3] = the tuned preconditioner time in microseconds. */
+ * 1 lean, 2 paired FP32, 3 communication-avoiding FP32, 4 classical Gram-Schmidt FP32,
+ * 5 FP16 basis, 6 BF16 basis, 7 paired FP32 with two sites per thread; -1 default),
+ * out[2] = engine cluster size (0 default), out[3] = the tuned preconditioner time in
+ * microseconds. */
 AMG_API int amg_autotune_info(amg_ctx ctx, int* out4);
+/* The same plus out[4] = the coarse SAP teams per engine CTA (1, 2 or 4); writes the first
+ * min(n, 5) values. */
+AMG_API int amg_autotune_info_n(amg_ctx ctx, int* out, int n);
 
 #ifdef __cplusplus
 }
