@@ -8,7 +8,10 @@
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <condition_variable>
 #include <map>
+#include <mutex>
+#include <thread>
 #include <memory>
 #include <tuple>
 #include <random>
@@ -208,6 +211,7 @@ struct amg_context {
     // outer FGMRES
     DevBuf V, Z, w, x, b, partial, dots, scal, masks, etab, vf, zf, vd, zd, sap_flags, norms;
     PinnedBuf hpin;                // host staging of the outer FGMRES (dots, norms, masks)
+    char* hpin_dev = nullptr;      // hpin's device mapping (null: copy through the copy engines)
     cudaEvent_t ev_host = nullptr; // marks the end of each queued piece of the outer FGMRES
     int Rcap = 0;
     std::vector<double> history;
@@ -237,6 +241,7 @@ struct amg_context {
     cudaStream_t copy_stream = nullptr;
     DevBuf b1, x1;
     cudaEvent_t ev_in[2] = {nullptr, nullptr}, ev_solved[2] = {nullptr, nullptr}, ev_out[2] = {nullptr, nullptr};
+    cudaEvent_t ev_piece[2] = {nullptr, nullptr};   // the batch copies' pieces in flight
     void drop_graphs() {
         for (auto& kv : graphs)
             if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
@@ -301,6 +306,16 @@ __global__ void k_add_d(double2* d, const double2* a, long long n) {
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
         d[e] += a[e];
 }
+// Copies of a few kilobytes between device memory and the outer FGMRES's page-locked staging,
+// through the staging's device mapping by one CTA, so they never queue on the copy engines
+// behind large transfers of other streams (the batches amg_solve_stream moves while a solve
+// runs); the host reads the staging only after an event recorded behind the copy.  Loads
+// are volatile: a host-side source is read where it lies, never from a cached copy.
+__global__ void k_stage_words(unsigned* dst, const volatile unsigned* src, int n) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+    __threadfence_system();
+}
+
 __global__ void k_set_int(int* p, int v, int n) {
     for (int i = threadIdx.x; i < n; i += blockDim.x) p[i] = v;
 }
@@ -1080,6 +1095,24 @@ int autotune(amg_context* c, const double2* v, double2* z, int R) {
 // to the end (outer_fgmres); amg_solve_many drives several contexts in turn, so the GPU
 // runs one context's kernels while the host handles another's Givens rotations.
 // ---------------------------------------------------------------------------------
+// dst = src for `bytes` (a multiple of 4) where one side lies in c->hpin: by k_stage_words
+// through hpin's device mapping, or by cudaMemcpyAsync if there is none
+int stage_copy(amg_context* c, void* dst, const void* src, size_t bytes, cudaMemcpyKind kind) {
+    if (!c->hpin_dev || bytes % 4 || bytes > (size_t(1) << 30)) {
+        CK(cudaMemcpyAsync(dst, src, bytes, kind, c->stream));
+        return AMG_OK;
+    }
+    char* h0 = static_cast<char*>(c->hpin.p);
+    auto dev = [&](const void* hp) { return c->hpin_dev + (static_cast<const char*>(hp) - h0); };
+    unsigned* d = static_cast<unsigned*>(kind == cudaMemcpyDeviceToHost ? static_cast<void*>(dev(dst)) : dst);
+    const unsigned* s =
+        static_cast<const unsigned*>(kind == cudaMemcpyHostToDevice ? static_cast<const void*>(dev(src)) : src);
+    k_stage_words<<<1, 256, 0, c->stream>>>(d, s, (int)(bytes / 4));
+    count_launch(1);
+    CK(cudaGetLastError());
+    return AMG_OK;
+}
+
 struct OuterSolve {
     // PRECOND: a step waits for its preconditioner, which the caller runs for several
     // contexts together (defer set: amg_solve_many's grouped SAP), then issue_step_post
@@ -1152,8 +1185,8 @@ struct OuterSolve {
         launch_residual<double>(c->d.U.as<double2>(), b, len, x, V, c->nx, c->nt, R, c->m0, partial, n2, nullptr,
                                 c->stream);
         launch_norm2<double>(b, len, len, R, partial, n2 + c->Rcap, c->stream);
-        CK(cudaMemcpyAsync(h_norm, n2, R * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaMemcpyAsync(h_norm + R, n2 + c->Rcap, R * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CKR(stage_copy(c, h_norm, n2, R * sizeof(double), cudaMemcpyDeviceToHost));
+        CKR(stage_copy(c, h_norm + R, n2 + c->Rcap, R * sizeof(double), cudaMemcpyDeviceToHost));
         CK(cudaEventRecord(c->ev_host, c->stream));
         phase = INIT;
         return AMG_OK;
@@ -1161,8 +1194,8 @@ struct OuterSolve {
 
     int upload_masks() {
         for (int r = 0; r < R; r++) { h_mask[r] = act[r]; h_mask[R + r] = arn[r]; }
-        CK(cudaMemcpyAsync(act_d(), h_mask, R * sizeof(int), cudaMemcpyHostToDevice, c->stream));
-        CK(cudaMemcpyAsync(arn_d(), h_mask + R, R * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+        CKR(stage_copy(c, act_d(), h_mask, R * sizeof(int), cudaMemcpyHostToDevice));
+        CKR(stage_copy(c, arn_d(), h_mask + R, R * sizeof(int), cudaMemcpyHostToDevice));
         return AMG_OK;
     }
 
@@ -1177,7 +1210,7 @@ struct OuterSolve {
             if (act[r]) g[(size_t)r * (m + 1)] = cd(err[r], 0);
         }
         CKR(upload_masks());
-        CK(cudaMemcpyAsync(c->scal.p, h_scal, R * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        CKR(stage_copy(c, c->scal.p, h_scal, R * sizeof(double), cudaMemcpyHostToDevice));
         double2* V = c->V.as<double2>();
         float2* yf = c->p.precision == AMG_PREC_MIXED ? c->vf.as<float2>() : nullptr;
         launch_scale(V, V, len, c->scal.as<double>(), act_d(), R, c->stream, yf);
@@ -1245,9 +1278,8 @@ struct OuterSolve {
             launch_scale(Vn, w, len, c->scal.as<double>(), sm_d(), R, c->stream, yf);
             c->vf_src = yf ? Vn : nullptr;
         }
-        CK(cudaMemcpyAsync(h_dots, dots, (size_t)R * 2 * (nv + 1) * sizeof(double2), cudaMemcpyDeviceToHost,
-                           c->stream));
-        CK(cudaMemcpyAsync(h_ro, ro_d(), R * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        CKR(stage_copy(c, h_dots, dots, (size_t)R * 2 * (nv + 1) * sizeof(double2), cudaMemcpyDeviceToHost));
+        CKR(stage_copy(c, h_ro, ro_d(), R * sizeof(int), cudaMemcpyDeviceToHost));
         CK(cudaEventRecord(c->ev_host, c->stream));
         phase = STEP;
         return AMG_OK;
@@ -1318,13 +1350,13 @@ struct OuterSolve {
             h_nvr[r] = n;
         }
         double2* eta_d = c->etab.as<double2>();
-        CK(cudaMemcpyAsync(eta_d, h_eta, (size_t)R * m * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
-        CK(cudaMemcpyAsync(nvr_d(), h_nvr, R * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+        CKR(stage_copy(c, eta_d, h_eta, (size_t)R * m * sizeof(double2), cudaMemcpyHostToDevice));
+        CKR(stage_copy(c, nvr_d(), h_nvr, R * sizeof(int), cudaMemcpyHostToDevice));
         launch_multiaxpy_add(x, c->Z.as<double2>(), len, vstride, m, eta_d, m, nvr_d(), act_d(), R, c->stream);
         double* n2 = c->norms.as<double>();
         launch_residual<double>(c->d.U.as<double2>(), b, len, x, c->V.as<double2>(), c->nx, c->nt, R, c->m0,
                                 c->partial.as<double>(), n2, act_d(), c->stream);
-        CK(cudaMemcpyAsync(h_norm, n2, R * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CKR(stage_copy(c, h_norm, n2, R * sizeof(double), cudaMemcpyDeviceToHost));
         CK(cudaEventRecord(c->ev_host, c->stream));
         phase = RESTART;
         return AMG_OK;
@@ -1403,6 +1435,11 @@ int ensure_capacity(amg_context* c, int R) {
     CKR(c->norms.alloc((size_t)2 * Rn * sizeof(double)));
     CKR(c->hpin.alloc((size_t)Rn * (2 * sizeof(double) + (2 * m + 3) * sizeof(double2) + 4 * sizeof(int) +
                                      sizeof(double) + m * sizeof(double2)) + 8 * 16));
+    {
+        void* d = nullptr;
+        c->hpin_dev = cudaHostGetDevicePointer(&d, c->hpin.p, 0) == cudaSuccess ? static_cast<char*>(d) : nullptr;
+        cudaGetLastError();
+    }
     c->Rcap = Rn;
     CKR(alloc_fine<double>(c, c->d, Rn));
     if (c->p.precision == AMG_PREC_F64) {
@@ -1761,6 +1798,7 @@ int amg_destroy(amg_ctx c) {
         if (c->ev_in[k]) cudaEventDestroy(c->ev_in[k]);
         if (c->ev_solved[k]) cudaEventDestroy(c->ev_solved[k]);
         if (c->ev_out[k]) cudaEventDestroy(c->ev_out[k]);
+        if (c->ev_piece[k]) cudaEventDestroy(c->ev_piece[k]);
     }
     cudaStream_t s = c->stream, cs = c->copy_stream;
     delete c;
@@ -2349,6 +2387,7 @@ int amg_solve_stream(amg_ctx c, int nbatch, const double* const* b, double* cons
         if (!c->ev_in[k]) CK(cudaEventCreateWithFlags(&c->ev_in[k], cudaEventDisableTiming));
         if (!c->ev_solved[k]) CK(cudaEventCreateWithFlags(&c->ev_solved[k], cudaEventDisableTiming));
         if (!c->ev_out[k]) CK(cudaEventCreateWithFlags(&c->ev_out[k], cudaEventDisableTiming));
+        if (!c->ev_piece[k]) CK(cudaEventCreateWithFlags(&c->ev_piece[k], cudaEventDisableTiming));
     }
     const long long n = (long long)nrhs * vlen0(c);
     const size_t bytes = (size_t)n * sizeof(double2);
@@ -2359,31 +2398,113 @@ int amg_solve_stream(amg_ctx c, int nbatch, const double* const* b, double* cons
     cudaStream_t cs = c->copy_stream;
     // both slots free: nothing of an earlier call may still read or write them
     CK(cudaStreamSynchronize(c->stream));
-    CK(cudaMemcpyAsync(bs[0], b[0], bytes, cudaMemcpyHostToDevice, cs));
-    CK(cudaEventRecord(c->ev_in[0], cs));
-    int rc = AMG_OK;
-    for (int i = 0; i < nbatch; i++) {
-        const int k = i & 1, kn = k ^ 1;
-        if (i + 1 < nbatch) {
-            // batch i+1's sources into the other slot once batch i-1's solve stopped reading it
-            if (i >= 1) CK(cudaStreamWaitEvent(cs, c->ev_solved[kn], 0));
-            CK(cudaMemcpyAsync(bs[kn], b[i + 1], bytes, cudaMemcpyHostToDevice, cs));
-            CK(cudaEventRecord(c->ev_in[kn], cs));
+
+    // The copies are enqueued by a helper thread, in pieces of kPiece bytes with at most two
+    // in flight (the helper waits for the older one before it enqueues the next): a whole
+    // gigabyte queued at once holds the driver long enough to delay the solve's own launches.
+    // Host-side counters order each event's recording before every wait that refers to it:
+    //   in_done   batches whose input copy (ev_in) is enqueued    (helper -> solver)
+    //   solved    batches whose ev_solved is recorded            (solver -> helper)
+    //   out_done  batches whose output copy (ev_out) is enqueued  (helper -> solver)
+    std::mutex mu;
+    std::condition_variable cv;
+    int in_done = 0, solved = 0, out_done = 0;
+    bool stop = false;
+    cudaError_t copy_err = cudaSuccess;
+    auto wait_for = [&](const int& counter, int need) {
+        std::unique_lock<std::mutex> lk(mu);
+        cv.wait(lk, [&] { return stop || counter >= need; });
+        return !stop;
+    };
+    auto publish = [&](int& counter, int value) {
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            counter = value;
         }
-        CK(cudaStreamWaitEvent(c->stream, c->ev_in[k], 0));
-        if (i >= 2) CK(cudaStreamWaitEvent(c->stream, c->ev_out[k], 0));   // batch i-2's solution copied out
+        cv.notify_all();
+    };
+    auto halt = [&]() {
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            stop = true;
+        }
+        cv.notify_all();
+    };
+    const int device = c->device;
+    constexpr size_t kPiece = size_t(64) << 20;
+    std::thread helper([&] {
+        cudaSetDevice(device);
+        auto ok = [&](cudaError_t e) {
+            if (e != cudaSuccess && copy_err == cudaSuccess) copy_err = e;
+            return e == cudaSuccess;
+        };
+        long long piece = 0;
+        auto paced = [&](void* dst, const void* src, cudaMemcpyKind kind) {
+            for (size_t o = 0; o < bytes; o += kPiece, piece++) {
+                cudaEvent_t ev = c->ev_piece[piece & 1];
+                if (piece >= 2 && !ok(cudaEventSynchronize(ev))) return false;
+                if (!ok(cudaMemcpyAsync(static_cast<char*>(dst) + o, static_cast<const char*>(src) + o,
+                                        std::min(kPiece, bytes - o), kind, cs)) ||
+                    !ok(cudaEventRecord(ev, cs)))
+                    return false;
+            }
+            return true;
+        };
+        for (int s = 0; s <= nbatch; s++) {
+            if (s < nbatch) {
+                // batch s's sources into slot s&1 once batch s-2's solve stopped reading it
+                if (s >= 2) {
+                    if (!wait_for(solved, s - 1)) return;
+                    if (!ok(cudaStreamWaitEvent(cs, c->ev_solved[s & 1], 0))) break;
+                }
+                if (!paced(bs[s & 1], b[s], cudaMemcpyHostToDevice) || !ok(cudaEventRecord(c->ev_in[s & 1], cs)))
+                    break;
+                publish(in_done, s + 1);
+            }
+            if (s >= 1) {
+                // batch s-1's solutions out once its solve is done
+                if (!wait_for(solved, s)) return;
+                if (!ok(cudaStreamWaitEvent(cs, c->ev_solved[(s - 1) & 1], 0)) ||
+                    !paced(x[s - 1], xs[(s - 1) & 1], cudaMemcpyDeviceToHost) ||
+                    !ok(cudaEventRecord(c->ev_out[(s - 1) & 1], cs)))
+                    break;
+                publish(out_done, s);
+            }
+        }
+        if (copy_err != cudaSuccess) halt();
+    });
+    int rc = AMG_OK;
+    for (int i = 0; i < nbatch && rc >= 0; i++) {
+        const int k = i & 1;
+        if (!wait_for(in_done, i + 1)) break;
+        cudaError_t e = cudaStreamWaitEvent(c->stream, c->ev_in[k], 0);
+        if (e == cudaSuccess && i >= 2) {   // batch i-2's solutions copied out of slot k
+            if (!wait_for(out_done, i - 1)) break;
+            e = cudaStreamWaitEvent(c->stream, c->ev_out[k], 0);
+        }
+        if (e != cudaSuccess) {
+            rc = fail(AMG_ERR_CUDA, "%s", cudaGetErrorString(e));
+            break;
+        }
         const int r = amg_solve_dev(c, bs[k], xs[k], nrhs, info ? info[i] : nullptr);
         if (r < 0) {
-            cudaStreamSynchronize(cs);
-            return r;
+            rc = r;
+            break;
         }
         if (r == AMG_NOT_CONVERGED) rc = r;
-        CK(cudaEventRecord(c->ev_solved[k], c->stream));
-        CK(cudaStreamWaitEvent(cs, c->ev_solved[k], 0));
-        CK(cudaMemcpyAsync(x[i], xs[k], bytes, cudaMemcpyDeviceToHost, cs));
-        CK(cudaEventRecord(c->ev_out[k], cs));
+        if ((e = cudaEventRecord(c->ev_solved[k], c->stream)) != cudaSuccess) {
+            rc = fail(AMG_ERR_CUDA, "%s", cudaGetErrorString(e));
+            break;
+        }
+        publish(solved, i + 1);
     }
-    CK(cudaStreamSynchronize(cs));
+    if (rc < 0) halt();
+    helper.join();
+    const cudaError_t es = cudaStreamSynchronize(cs);
+    if (rc < 0) return rc;
+    if (copy_err != cudaSuccess) return fail(AMG_ERR_CUDA, "batch copy: %s", cudaGetErrorString(copy_err));
+    if (stop) return fail(AMG_ERR_CUDA, "batch copies stopped");
+    if (es != cudaSuccess) return fail(AMG_ERR_CUDA, "%s", cudaGetErrorString(es));
     return rc;
 }
 
