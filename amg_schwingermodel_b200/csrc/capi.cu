@@ -2432,7 +2432,7 @@ int amg_solve_stream(amg_ctx c, int nbatch, const double* const* b, double* cons
     };
     const int device = c->device;
     constexpr size_t kPiece = size_t(64) << 20;
-    std::thread helper([&] {
+    auto copy_loop = [&] {
         cudaSetDevice(device);
         auto ok = [&](cudaError_t e) {
             if (e != cudaSuccess && copy_err == cudaSuccess) copy_err = e;
@@ -2472,7 +2472,13 @@ int amg_solve_stream(amg_ctx c, int nbatch, const double* const* b, double* cons
             }
         }
         if (copy_err != cudaSuccess) halt();
-    });
+    };
+    std::thread helper;
+    try {
+        helper = std::thread(copy_loop);
+    } catch (const std::exception& ex) {
+        return fail(AMG_ERR_UNSUPPORTED, "no copy thread: %s", ex.what());
+    }
     int rc = AMG_OK;
     for (int i = 0; i < nbatch && rc >= 0; i++) {
         const int k = i & 1;
