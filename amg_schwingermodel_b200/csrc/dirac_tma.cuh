@@ -159,7 +159,7 @@ __global__ void __launch_bounds__(kTT, 2) k_dirac_tma(UA U, const cx<TIN>* __res
             for (int r = 0; r < kTX; r++) {
                 const int c = (r + 1) * RS + tid + 1;
                 cx<T> o0, o1;
-                dirac_site<T, DAG, TIN>(L[r], tile, c, mass, o0, o1);
+                dirac_site<T, DAG, TIN, true>(L[r], tile, c, mass, o0, o1);
                 const long long n = (long long)(x0 + r) * nt + t0 + tid;
                 if constexpr (RES) {
                     const cx<T>* bb = bres + (long long)rhs * bstride;

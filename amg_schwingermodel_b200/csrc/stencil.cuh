@@ -49,14 +49,37 @@ __device__ __forceinline__ cx<T> promote_cx(const cx<TP>& v) {
     if constexpr (std::is_same<T, TP>::value) return v;
     else return ccast<T>(v);
 }
-template <typename T, bool DAG, typename TP = T>
+// Both spin components of site n.  TILE: psi is a shared-memory tile read by consecutive lanes
+// at consecutive sites.  A FP32 site (16 bytes) is then one 16-byte load.  A FP64 site is two
+// 16-byte halves 32 bytes apart from lane to lane, so eight lanes reading the same half would
+// hit every bank twice; lanes 4-7 of each eight read the second half first, which puts the
+// eight addresses of each load in distinct banks.
+template <typename T, typename TP, bool TILE>
+__device__ __forceinline__ void site_spins(const cx<TP>* __restrict__ psi, int n, cx<T>& s0, cx<T>& s1) {
+    if constexpr (TILE && sizeof(TP) == 4) {
+        const float4 q = reinterpret_cast<const float4*>(psi)[n];
+        s0 = promote_cx<T, TP>(make_float2(q.x, q.y));
+        s1 = promote_cx<T, TP>(make_float2(q.z, q.w));
+    } else if constexpr (TILE) {
+        const int sw = (threadIdx.x >> 2) & 1;
+        const cx<TP> u = psi[2 * n + sw], v = psi[2 * n + 1 - sw];
+        s0 = promote_cx<T, TP>(sw ? v : u);
+        s1 = promote_cx<T, TP>(sw ? u : v);
+    } else {
+        s0 = promote_cx<T, TP>(psi[2 * n]);
+        s1 = promote_cx<T, TP>(psi[2 * n + 1]);
+    }
+}
+
+template <typename T, bool DAG, typename TP = T, bool TILE = false>
 __device__ __forceinline__ void dirac_site(const SiteOp<T>& L, const cx<TP>* __restrict__ psi, int n, T mass,
                                            cx<T>& o0, cx<T>& o1) {
-    const cx<T> a = promote_cx<T, TP>(psi[2 * L.r0]), b = promote_cx<T, TP>(psi[2 * L.r0 + 1]);
-    const cx<T> c = promote_cx<T, TP>(psi[2 * L.r1]), d = promote_cx<T, TP>(psi[2 * L.r1 + 1]);
-    const cx<T> e = promote_cx<T, TP>(psi[2 * L.l0]), f = promote_cx<T, TP>(psi[2 * L.l0 + 1]);
-    const cx<T> g = promote_cx<T, TP>(psi[2 * L.l1]), h = promote_cx<T, TP>(psi[2 * L.l1 + 1]);
-    const cx<T> p0 = promote_cx<T, TP>(psi[2 * n]), p1 = promote_cx<T, TP>(psi[2 * n + 1]);
+    cx<T> a, b, c, d, e, f, g, h, p0, p1;
+    site_spins<T, TP, TILE>(psi, L.r0, a, b);
+    site_spins<T, TP, TILE>(psi, L.r1, c, d);
+    site_spins<T, TP, TILE>(psi, L.l0, e, f);
+    site_spins<T, TP, TILE>(psi, L.l1, g, h);
+    site_spins<T, TP, TILE>(psi, n, p0, p1);
     cx<T> t0, t1, t2, t3;
     if (!DAG) {
         t0 = L.sR * cmul(L.u0, a - b);
