@@ -171,8 +171,10 @@ __global__ void __launch_bounds__(kTT, 2) k_dirac_tma(UA U, const cx<TIN>* __res
                 o[2 * n + 1] = o1;
                 if constexpr (COPY) {
                     cx<T>* ic = in_copy + (long long)rhs * N * 2;
-                    ic[2 * n] = ccast<T>(tile[2 * c]);
-                    ic[2 * n + 1] = ccast<T>(tile[2 * c + 1]);
+                    cx<T> s0, s1;
+                    site_spins<T, TIN, true>(tile, c, s0, s1);
+                    ic[2 * n] = s0;
+                    ic[2 * n + 1] = s1;
                 }
             }
             if (RES && partial) {
