@@ -1,13 +1,14 @@
 // FP32 SAP block solve with its Krylov basis stored in 16 bits (FP16, or BF16 with BF = true):
-// the solve of k_sap0_f32 (MGS
-// form; src/sap.cpp:44-62, GMRES_D_B include/sap.h:27-47, FGMRES::fgmres
-// src/fgmres.cpp:5-115 with x0 = b) laid out for three CTAs per SM instead of two.
+// the solve of k_sap0_f32 (MGS form; src/sap.cpp:44-62, GMRES_D_B include/sap.h:27-47,
+// FGMRES::fgmres src/fgmres.cpp:5-115 with x0 = b) laid out for three CTAs per SM instead
+// of two.  The block body (sap0_h_solve) serves one launch per lattice (k_sap0_h) and one
+// launch over several lattices' blocks (k_sap0_h_group, the many-configuration solve).
 //
 // What sets the SM's share: the paired kernel holds its basis (M + 1 vectors of 16 bytes per
 // site, 98 KB for a 1024-site block) in shared memory and its folded links, neighbour
 // indices and Givens rotations in registers (128 per thread), so two CTAs of 8 warps fill an
 // SM.  Here
-//   * the M basis vectors are FP16 pairs (8 bytes per site, 40 KB); the iterate stays FP32
+//   * the M basis vectors are 16-bit pairs (8 bytes per site, 40 KB); the iterate stays FP32
 //     in its own array (16 KB), and so do every dot, axpy, norm and the solution update;
 //   * the folded hop links (sign, 1/2 and the zero outside the block applied; FP16 storage of
 //     the fine links) are staged once per CTA in shared memory (16 KB) instead of registers;
