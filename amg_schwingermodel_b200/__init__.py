@@ -364,6 +364,13 @@ class AMGContext:
         names = ("apply", "local_apply", "kfgmres_steps", "gmres_steps", "sap_steps", "sap_calls")
         return {l: dict(zip(names, map(int, o[6 * l: 6 * l + 6]))) for l in range(1, self.levels)}
 
+    def setup_timings(self) -> dict:
+        """The last set-up's device milliseconds by phase (amg_setup_timings)."""
+        o = np.zeros(_lib.AMG_SETUP_PHASES, dtype=np.float64)
+        check(lib().amg_setup_timings(self._h, _cptr(o), o.size), "amg_setup_timings")
+        return dict(zip(("initial_vectors", "smoothing", "orthonormalisation", "coarse_links", "bootstrap",
+                         "mixed_copies"), map(float, o)))
+
     def timings(self):
         s, v = C.c_double(0), C.c_double(0)
         check(lib().amg_last_timings(self._h, C.byref(s), C.byref(v)), "amg_last_timings")

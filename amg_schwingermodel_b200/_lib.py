@@ -29,6 +29,13 @@ AMG_PRECOND_NONE = 2
 AMG_LINKS_F32 = 0
 AMG_LINKS_BF16 = 1
 AMG_LINKS_F16 = 2
+AMG_SETUP_INIT = 0
+AMG_SETUP_SMOOTH = 1
+AMG_SETUP_ORTHO = 2
+AMG_SETUP_LINKS = 3
+AMG_SETUP_BOOT = 4
+AMG_SETUP_MIXED = 5
+AMG_SETUP_PHASES = 6
 
 
 class AmgParams(C.Structure):
@@ -106,6 +113,7 @@ SIGNATURES = {
     "amg_last_timings": (_I, [_P, C.POINTER(_D), C.POINTER(_D)]),
     "amg_autotune_info": (_I, [_P, _P]),
     "amg_autotune_info_n": (_I, [_P, _P, _I]),
+    "amg_setup_timings": (_I, [_P, _P, _I]),
     "amg_profile": (_I, [_P, _I]),
     "amg_profile_query": (_I, [_P, _I, C.POINTER(_D), C.POINTER(C.c_longlong), C.POINTER(_D)]),
     "amg_launch_count": (C.c_longlong, []),

@@ -216,6 +216,7 @@ struct amg_context {
     int Rcap = 0;
     std::vector<double> history;
     double last_setup_ms = 0, last_solve_ms = 0;
+    double setup_phase_ms[AMG_SETUP_PHASES] = {0};   // the last set-up by phase (amg_setup_timings)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // per-kernel-class timing with CUDA events on the context's stream (amg_profile)
     struct ProfSlot { double ms = 0; long long n = 0; double bytes = 0; };
@@ -1541,7 +1542,33 @@ int build_mixed(amg_context* c) {
     return AMG_OK;
 }
 
+// Device time of the set-up's phases: events recorded on the context's stream at each phase
+// boundary; the time from one mark to the next is charged to the phase that just ended.
+struct SetupClock {
+    amg_context* c;
+    std::vector<std::pair<int, cudaEvent_t>> marks;   // (phase ended at this mark, event)
+    explicit SetupClock(amg_context* c_) : c(c_) {}
+    ~SetupClock() { for (auto& m : marks) cudaEventDestroy(m.second); }
+    void mark(int phase) {
+        cudaEvent_t e = nullptr;
+        if (cudaEventCreate(&e) != cudaSuccess) { cudaGetLastError(); return; }
+        cudaEventRecord(e, c->stream);
+        marks.emplace_back(phase, e);
+    }
+    void harvest() {
+        for (double& v : c->setup_phase_ms) v = 0;
+        if (marks.empty() || cudaEventSynchronize(marks.back().second) != cudaSuccess) return;
+        for (size_t i = 1; i < marks.size(); i++) {
+            float ms = 0;
+            if (cudaEventElapsedTime(&ms, marks[i - 1].second, marks[i].second) == cudaSuccess)
+                c->setup_phase_ms[marks[i].first] += ms;
+        }
+    }
+};
+
 int do_setup(amg_context* c) {
+    SetupClock clk(c);
+    clk.mark(AMG_SETUP_INIT);
     c->drop_graphs();
     if (!c->gauge_set) return fail(AMG_ERR_STATE, "set the gauge field before the set-up");
     const amg_params& p = c->p;
@@ -1590,6 +1617,7 @@ int do_setup(amg_context* c) {
     }
     CKR(c->hops0.alloc((size_t)c->N * 20 * sizeof(double2)));
     launch_fine_hops<double>(c->d.U.as<double2>(), c->hops0.as<double2>(), c->nx, c->nt, c->stream);
+    clk.mark(AMG_SETUP_INIT);
     // smoothing, orthonormalisation and coarse links, level by level
     for (int l = 0; l < L - 1; l++) {
         const LevelHost& h = c->lv[l];
@@ -1603,8 +1631,11 @@ int do_setup(amg_context* c) {
                                        c->d.W[l].as<double2>(), nv, h.ntest));
             }
         }
+        clk.mark(AMG_SETUP_SMOOTH);
         CKR(orthonormalize(c, l));
+        clk.mark(AMG_SETUP_ORTHO);
         CKR(coarse_links(c, l));
+        clk.mark(AMG_SETUP_LINKS);
     }
     // bootstrap passes (src/amg.cpp:52-84)
     for (int it = 0; it < p.nit; it++) {
@@ -1635,14 +1666,17 @@ int do_setup(amg_context* c) {
             CKR(coarse_links(c, l));
         }
     }
+    clk.mark(AMG_SETUP_BOOT);
     CK(cudaStreamSynchronize(c->stream));
     int flags = 0;
     CK(cudaMemcpy(&flags, c->d.eh.flags, sizeof(int), cudaMemcpyDeviceToHost));
     if (flags) return fail(AMG_ERR_UNSUPPORTED, "engine reported flags %d", flags);
     c->f.ready = 0;
     if (p.precision == AMG_PREC_MIXED) CKR(build_mixed(c));
+    clk.mark(AMG_SETUP_MIXED);
     c->setup_done = 1;
     CK(cudaStreamSynchronize(c->stream));
+    clk.harvest();
     return AMG_OK;
 }
 
@@ -2772,6 +2806,12 @@ int amg_autotune_info_n(amg_ctx c, int* out, int n) {
     const int t = c->p.precision == AMG_PREC_MIXED ? c->f.sap_teams : c->d.sap_teams;
     v[4] = t ? t : engine_sap_teams();
     for (int i = 0; i < std::min(n, 5); i++) out[i] = v[i];
+    return AMG_OK;
+}
+
+int amg_setup_timings(amg_ctx c, double* ms, int n) {
+    if (!c || !ms || n < 0) return fail(AMG_ERR_INVALID, "bad argument");
+    for (int i = 0; i < std::min(n, (int)AMG_SETUP_PHASES); i++) ms[i] = c->setup_phase_ms[i];
     return AMG_OK;
 }
 

@@ -302,6 +302,19 @@ AMG_API long long amg_launch_count(void);
 AMG_API void* amg_get_stream(amg_ctx ctx);
 /* Device milliseconds of the last amg_setup / solve call (CUDA events). */
 AMG_API int amg_last_timings(amg_ctx ctx, double* setup_ms, double* solve_ms);
+/* The last amg_setup by phase (device milliseconds between CUDA events at the phase
+ * boundaries): the initial test vectors and the fine operator's hop table, the test-vector
+ * smoothing (SAP), the orthonormalisation, the coarse links (all levels), the bootstrap
+ * passes, and the mixed form's FP32/BF16/FP16 copies with its engine.  ms[i] for
+ * i < min(n, AMG_SETUP_PHASES). */
+#define AMG_SETUP_INIT 0
+#define AMG_SETUP_SMOOTH 1
+#define AMG_SETUP_ORTHO 2
+#define AMG_SETUP_LINKS 3
+#define AMG_SETUP_BOOT 4
+#define AMG_SETUP_MIXED 5
+#define AMG_SETUP_PHASES 6
+AMG_API int amg_setup_timings(amg_ctx ctx, double* ms, int n);
 /* The autotuner's choice: out[0] = 1 once tuned, out[1] = fine SAP kernel (0 generic,
  * 1 lean, 2 paired FP32, 3 communication-avoiding FP32, 4 classical Gram-Schmidt FP32,
  * 5 FP16 basis, 6 BF16 basis, 7 paired FP32 with two sites per thread; -1 default),
