@@ -1238,6 +1238,9 @@ struct OuterSolve {
     }
     // the basis vector step j preconditions (the grouped preconditioner's input)
     const double2* step_input() const { return c->V.as<double2>() + (long long)j * vstride; }
+    // the mixed form keeps Z_k = M V_k as the preconditioner wrote it, in FP32 (its FP64 value
+    // is the exact promotion), in the first half of the Z buffer with the FP64 slots' strides
+    float2* zslot_f32(int k) const { return c->Z.as<float2>() + (long long)k * vstride; }
 
     // the rest of Arnoldi step j once z_j is in c->zf (mixed) or Z_j: w = D z_j, CGS2, V_{j+1}
     int issue_step_post() {
@@ -1250,11 +1253,11 @@ struct OuterSolve {
         const bool mixed = c->p.precision == AMG_PREC_MIXED && c->precond != AMG_PRECOND_NONE;
         {
             // algorithmic bytes per site: the links (2 x 16 B) and per source z_j in (FP32:
-            // 16 B, FP64: 32 B) and w out (32 B), plus Z_j out (32 B) in the mixed form
-            ProfScope ps_(c, AMG_PROF_OUTER_OP, (double)c->N * (32.0 + (mixed ? 80.0 : 64.0) * R));
-            if (mixed)   // w = D z_j from the FP32 preconditioner output, Z_j = its FP64 promotion
-                launch_dirac_promote(c->d.U.as<double2>(), c->zf.as<float2>(), w, Zj, c->nx, c->nt, R, c->m0,
-                                     c->stream);
+            // 16 B, FP64: 32 B) and w out (32 B), plus Z_j out (FP32, 16 B) in the mixed form
+            ProfScope ps_(c, AMG_PROF_OUTER_OP, (double)c->N * (32.0 + 64.0 * R));
+            if (mixed)   // w = D z_j from the FP32 preconditioner output, copied into Z_j (FP32)
+                launch_dirac_promote(c->d.U.as<double2>(), c->zf.as<float2>(), w, zslot_f32(j), c->nx, c->nt, R,
+                                     c->m0, c->stream);
             else
                 launch_dirac<double>(c->d.U.as<double2>(), Zj, w, c->nx, c->nt, R, c->m0, 0, c->stream);
         }
@@ -1353,7 +1356,10 @@ struct OuterSolve {
         double2* eta_d = c->etab.as<double2>();
         CKR(stage_copy(c, eta_d, h_eta, (size_t)R * m * sizeof(double2), cudaMemcpyHostToDevice));
         CKR(stage_copy(c, nvr_d(), h_nvr, R * sizeof(int), cudaMemcpyHostToDevice));
-        launch_multiaxpy_add(x, c->Z.as<double2>(), len, vstride, m, eta_d, m, nvr_d(), act_d(), R, c->stream);
+        if (c->p.precision == AMG_PREC_MIXED && c->precond != AMG_PRECOND_NONE)
+            launch_multiaxpy_add(x, zslot_f32(0), len, vstride, m, eta_d, m, nvr_d(), act_d(), R, c->stream);
+        else
+            launch_multiaxpy_add(x, c->Z.as<double2>(), len, vstride, m, eta_d, m, nvr_d(), act_d(), R, c->stream);
         double* n2 = c->norms.as<double>();
         launch_residual<double>(c->d.U.as<double2>(), b, len, x, c->V.as<double2>(), c->nx, c->nt, R, c->m0,
                                 c->partial.as<double>(), n2, act_d(), c->stream);

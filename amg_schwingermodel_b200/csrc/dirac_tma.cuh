@@ -69,7 +69,7 @@ template <typename TIN>
 __host__ __device__ constexpr int dirac_tma_smem() { return 2 * dirac_tma_buf_bytes<TIN>() + 16; }
 
 // TIN: the spinors' storage type (T, or float for FP32 spinors into the FP64 operator); COPY:
-// also write the promoted input to in_copy; SELF_TEST: issue no copies at all and poll 256
+// also copy the input (as stored, FP32) to in_copy; SELF_TEST: issue no copies at all and poll 256
 // times per wait, so the first wait runs out with nothing in flight (the bounded-wait
 // self-test); RES: the residual out = b - D in instead (source r's b at bres + r * bstride, the
 // same site arithmetic as k_residual), skipping the sources with act[r] == 0 and, when
@@ -80,7 +80,7 @@ template <typename T, bool DAG, typename TIN = T, bool COPY = false, bool SELF_T
           typename UA = const cx<T>* __restrict__>
 __global__ void __launch_bounds__(kTT, 2) k_dirac_tma(UA U, const cx<TIN>* __restrict__ in,
                                                       cx<T>* __restrict__ out, int nx, int nt, T m0, int nrhs,
-                                                      cx<T>* __restrict__ in_copy, const cx<T>* __restrict__ bres,
+                                                      cx<TIN>* __restrict__ in_copy, const cx<T>* __restrict__ bres,
                                                       long long bstride, const int* __restrict__ act,
                                                       double* __restrict__ partial) {
     constexpr int wait_limit = SELF_TEST ? 256 : kTmaSpinLimit;
@@ -170,11 +170,9 @@ __global__ void __launch_bounds__(kTT, 2) k_dirac_tma(UA U, const cx<TIN>* __res
                 o[2 * n] = o0;
                 o[2 * n + 1] = o1;
                 if constexpr (COPY) {
-                    cx<T>* ic = in_copy + (long long)rhs * N * 2;
-                    cx<T> s0, s1;
-                    site_spins<T, TIN, true>(tile, c, s0, s1);
-                    ic[2 * n] = s0;
-                    ic[2 * n + 1] = s1;
+                    static_assert(sizeof(TIN) == 4, "the copy moves one FP32 site (16 bytes)");
+                    reinterpret_cast<float4*>(in_copy + (long long)rhs * N * 2)[n] =
+                        reinterpret_cast<const float4*>(tile)[c];
                 }
             }
             if (RES && partial) {

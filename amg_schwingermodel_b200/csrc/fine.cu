@@ -38,10 +38,10 @@ __global__ void __launch_bounds__(256) k_dirac(const cx<T>* __restrict__ U, cons
     }
 }
 
-// out = D in in FP64 for FP32 spinors in (promoted exactly), with the promoted copy of in
-// written to in_copy: the outer FGMRES's w = D z_j and its FP64 z_j in one pass
+// out = D in in FP64 for FP32 spinors in (promoted exactly), with in copied to in_copy: the
+// outer FGMRES's w = D z_j and its basis slot Z_j (kept in FP32) in one pass
 __global__ void __launch_bounds__(256) k_dirac_promote(const double2* __restrict__ U, const float2* __restrict__ in,
-                                                       double2* __restrict__ out, double2* __restrict__ in_copy, int nx,
+                                                       double2* __restrict__ out, float2* __restrict__ in_copy, int nx,
                                                        int nt, double m0, int nrhs) {
     const int N = nx * nt;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
@@ -53,8 +53,8 @@ __global__ void __launch_bounds__(256) k_dirac_promote(const double2* __restrict
         dirac_site<double, false, float>(L, in + off, n, m0 + 2.0, o0, o1);
         out[off + 2 * n] = o0;
         out[off + 2 * n + 1] = o1;
-        in_copy[off + 2 * n] = ccast<double>(in[off + 2 * n]);
-        in_copy[off + 2 * n + 1] = ccast<double>(in[off + 2 * n + 1]);
+        in_copy[off + 2 * n] = in[off + 2 * n];
+        in_copy[off + 2 * n + 1] = in[off + 2 * n + 1];
     }
 }
 
@@ -612,8 +612,10 @@ __global__ void __launch_bounds__(256, (NV <= 8 ? 2 : 1)) k_axpy_dots(double2* _
     }
 }
 
-// x[rhs] += sum_k c[rhs][k] Z_k[rhs]  (masked)
-__global__ void __launch_bounds__(256) k_multiaxpy_add(double2* __restrict__ x, const double2* __restrict__ Z,
+// x[rhs] += sum_k c[rhs][k] Z_k[rhs]  (masked; Z in FP64, or in FP32 promoted exactly: the
+// mixed form's basis of preconditioner outputs)
+template <typename TZ>
+__global__ void __launch_bounds__(256) k_multiaxpy_add(double2* __restrict__ x, const TZ* __restrict__ Z,
                                                        long long len, long long vstride, int nv,
                                                        const double2* __restrict__ c, int cstride,
                                                        const int* __restrict__ nvr, const int* __restrict__ act) {
@@ -625,7 +627,7 @@ __global__ void __launch_bounds__(256) k_multiaxpy_add(double2* __restrict__ x, 
         double2 a = xx[e];
         for (int k = 0; k < n; k++) {
             const double2 ck = c[(long long)rhs * cstride + k];
-            const double2 b = Z[(long long)k * vstride + (long long)rhs * len + e];
+            const double2 b = ccast<double>(Z[(long long)k * vstride + (long long)rhs * len + e]);
             a.x += ck.x * b.x - ck.y * b.y;
             a.y += ck.x * b.y + ck.y * b.x;
         }
@@ -742,8 +744,8 @@ void launch_dirac(const cx<T>* U, const cx<T>* in, cx<T>* out, int nx, int nt, i
     else k_dirac<T, false><<<grid, 256, 0, s>>>(U, in, out, nx, nt, m0, nrhs);
 }
 
-// out = D in (FP64) for FP32 spinors in, and in_copy = in promoted to FP64
-void launch_dirac_promote(const double2* U, const float2* in, double2* out, double2* in_copy, int nx, int nt,
+// out = D in (FP64) for FP32 spinors in, and in_copy = in (FP32)
+void launch_dirac_promote(const double2* U, const float2* in, double2* out, float2* in_copy, int nx, int nt,
                           int nrhs, double m0, cudaStream_t s) {
     count_launch(1);
     if (dirac_tma_enabled() && nrhs >= 1 && nt % kTT == 0 && nx % kTX == 0 && nx >= kTX &&
@@ -1317,12 +1319,17 @@ void launch_multiaxpy(double2* w, const double2* V, long long len, long long vst
     dim3 grid(592, nrhs);
     k_multiaxpy<<<grid, 256, 0, s>>>(w, V, len, vstride, nv, h, hstride, act);
 }
-void launch_multiaxpy_add(double2* x, const double2* Z, long long len, long long vstride, int nv, const double2* c,
+template <typename TZ>
+void launch_multiaxpy_add(double2* x, const TZ* Z, long long len, long long vstride, int nv, const double2* c,
                           int cstride, const int* nvr, const int* act, int nrhs, cudaStream_t s) {
     count_launch(1);
     dim3 grid(592, nrhs);
-    k_multiaxpy_add<<<grid, 256, 0, s>>>(x, Z, len, vstride, nv, c, cstride, nvr, act);
+    k_multiaxpy_add<TZ><<<grid, 256, 0, s>>>(x, Z, len, vstride, nv, c, cstride, nvr, act);
 }
+template void launch_multiaxpy_add<double2>(double2*, const double2*, long long, long long, int, const double2*, int,
+                                            const int*, const int*, int, cudaStream_t);
+template void launch_multiaxpy_add<float2>(double2*, const float2*, long long, long long, int, const double2*, int,
+                                           const int*, const int*, int, cudaStream_t);
 void launch_scale(double2* y, const double2* x, long long len, const double* sc, const int* act, int nrhs,
                   cudaStream_t s, float2* yf) {
     count_launch(1);

@@ -15,8 +15,8 @@ inline void count_launch(int n = 1) { __atomic_add_fetch(&g_launches, (long long
 template <typename T>
 void launch_dirac(const cx<T>* U, const cx<T>* in, cx<T>* out, int nx, int nt, int nrhs, T m0, int dagger,
                   cudaStream_t s);
-// out = D in (FP64) for FP32 spinors in (promoted exactly), and in_copy = in promoted to FP64
-void launch_dirac_promote(const double2* U, const float2* in, double2* out, double2* in_copy, int nx, int nt,
+// out = D in (FP64) for FP32 spinors in (promoted exactly), and in_copy = in (FP32)
+void launch_dirac_promote(const double2* U, const float2* in, double2* out, float2* in_copy, int nx, int nt,
                           int nrhs, double m0, cudaStream_t s);
 // reads and clears the fine kernels' device error flag (bit 0: a bulk-copy wait of the D
 // apply gave up); synchronises the stream; -1 on a CUDA error
@@ -78,7 +78,9 @@ void launch_axpy_multidot(double2* w, const double2* V, long long len, long long
                           cudaStream_t s);
 void launch_multiaxpy(double2* w, const double2* V, long long len, long long vstride, int nv, const double2* h,
                       int hstride, const int* act, int nrhs, cudaStream_t s);
-void launch_multiaxpy_add(double2* x, const double2* Z, long long len, long long vstride, int nv, const double2* c,
+// x += sum_k c_k Z_k with Z in FP64 (double2) or FP32 (float2, promoted exactly)
+template <typename TZ>
+void launch_multiaxpy_add(double2* x, const TZ* Z, long long len, long long vstride, int nv, const double2* c,
                           int cstride, const int* nvr, const int* act, int nrhs, cudaStream_t s);
 // y = (w - sum_{k<nv} h[k] V_k) * sc for the sources with act (w unchanged; partial receives
 // unused |w|^2 partials)
