@@ -583,19 +583,20 @@ void fine_restrict(amg_context* c, PrecSet<T>& ps, const cx<T>* v, cx<T>* out, i
                                     h0.bx, h0.bt, h0.ntest, R, nchunk, c->stream);
 }
 
+// psi += P vc, or psi = P vc with add = false (psi not read: the cycle's first write of it)
 template <typename T>
-void fine_prolong_add(amg_context* c, PrecSet<T>& ps, const cx<T>* vc, cx<T>* psi, int R) {
+void fine_prolong_add(amg_context* c, PrecSet<T>& ps, const cx<T>* vc, cx<T>* psi, int R, bool add = true) {
     const LevelHost& h0 = c->lv[0];
     ProfScope ps_(c, AMG_PROF_PROLONG,
                   (double)h0.ntest * c->N * 2 * (ps.w0_bf16 ? 4.0 : (double)sizeof(cx<T>)) +
-                      (double)R * c->N * 2 * 2 * sizeof(cx<T>));
+                      (double)R * c->N * 2 * (add ? 2 : 1) * sizeof(cx<T>));
     if (ps.w0_bf16)
         launch_prolong0_add<float, __nv_bfloat162>(ps.W0.template as<__nv_bfloat162>(), (const cx<float>*)vc,
                                                     (cx<float>*)psi, c->nx, c->nt, h0.bx, h0.bt, h0.ntest, R,
-                                                    c->stream);
+                                                    c->stream, add);
     else
         launch_prolong0_add<T, cx<T>>(ps.W0.template as<cx<T>>(), vc, psi, c->nx, c->nt, h0.bx, h0.bt, h0.ntest, R,
-                                       c->stream);
+                                       c->stream, add);
 }
 
 // ---------------------------------------------------------------------------------
@@ -697,7 +698,9 @@ int fine_cycle(amg_context* c, PrecSet<T>& ps, const cx<T>* eta, cx<T>* psi, int
         CK(cudaMemsetAsync(psi1, 0, (size_t)R * n1 * sizeof(cx<T>), c->stream));
         CKR(run_engine<T>(c, ps, ENG_VCYCLE, 1, 0, eta1, n1, psi1, n1, R));
     }
-    fine_prolong_add<T>(c, ps, psi1, psi, R);
+    // with psi = 0 on entry and no pre-smoothing psi has not been read yet: the prolongation
+    // stores into it (the caller need not clear it)
+    fine_prolong_add<T>(c, ps, psi1, psi, R, !psi_zero);
     if (p.nu2 > 0) CKR(fine_sap<T>(c, ps, eta, len, psi, p.nu2, R, 0));
     CKL();
     return AMG_OK;
@@ -763,7 +766,9 @@ int precondition(amg_context* c, const double2* v, double2* z, int R, bool want_
         double2* zs = c->zd.as<double2>();
         CK(cudaMemcpyAsync(vs, v, (size_t)R * len * sizeof(double2), cudaMemcpyDeviceToDevice, c->stream));
         CKR(run_graph(c, std::make_tuple(0, R, (const void*)vs, (void*)zs), [&]() -> int {
-            CK(cudaMemsetAsync(zs, 0, (size_t)R * len * sizeof(double2), c->stream));
+            // the cycle without pre-smoothing writes z before reading it
+            if (c->precond == AMG_PRECOND_SAP || c->p.nu1 > 0)
+                CK(cudaMemsetAsync(zs, 0, (size_t)R * len * sizeof(double2), c->stream));
             if (c->precond == AMG_PRECOND_SAP) return fine_sap<double>(c, c->d, vs, len, zs, 1, R, 0);
             return fine_cycle<double>(c, c->d, vs, zs, R, true);
         }));
@@ -777,7 +782,8 @@ int precondition(amg_context* c, const double2* v, double2* z, int R, bool want_
         c->vf_src = v;
     }
     CKR(run_graph(c, std::make_tuple(1, R, (const void*)vf, (void*)zf), [&]() -> int {
-        CK(cudaMemsetAsync(zf, 0, (size_t)R * len * sizeof(float2), c->stream));
+        if (c->precond == AMG_PRECOND_SAP || c->p.nu1 > 0)
+            CK(cudaMemsetAsync(zf, 0, (size_t)R * len * sizeof(float2), c->stream));
         if (c->precond == AMG_PRECOND_SAP) return fine_sap<float>(c, c->f, vf, len, zf, 1, R, 0);
         return fine_cycle<float>(c, c->f, vf, zf, R, true);
     }));
@@ -958,8 +964,8 @@ struct SapGroup {
                 launch_d2f(c->vf.as<float2>(), v[i], R[i] * len, c->stream);
                 c->vf_src = v[i];
             }
-            CK(cudaMemsetAsync(zf[i], 0, (size_t)R[i] * len * sizeof(float2), c->stream));
-            // fine_cycle<float> with psi = 0 on entry and no pre-smoothing: r = eta
+            // fine_cycle<float> with psi = 0 on entry and no pre-smoothing: r = eta, and the
+            // prolongation is the first write of z
             const LevelHost& h1 = c->lv[1];
             const long long n1 = (long long)h1.n * h1.K;
             float2* eta1 = c->f.eta1.as<float2>();
@@ -971,7 +977,7 @@ struct SapGroup {
                 CK(cudaMemsetAsync(psi1, 0, (size_t)R[i] * n1 * sizeof(float2), c->stream));
                 CKR(run_engine<float>(c, c->f, ENG_VCYCLE, 1, 0, eta1, n1, psi1, n1, R[i]));
             }
-            fine_prolong_add<float>(c, c->f, psi1, zf[i], R[i]);
+            fine_prolong_add<float>(c, c->f, psi1, zf[i], R[i], false);
         }
         if (cs[0]->p.nu2 > 0) CKR(sap(vf, zf, cs[0]->p.nu2));
         for (auto* c : cs) CKL();

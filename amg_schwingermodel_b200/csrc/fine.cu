@@ -338,8 +338,8 @@ __global__ void k_restrict0_sum(const cx<T>* __restrict__ partial, cx<T>* __rest
     out[(long long)rhs * nblk * K1 + o] = s;
 }
 
-// Level::P_v at level 0 (src/level.cpp:182-209) added into psi:
-//   psi[rhs][n][s] += sum_cc W[cc][n][s] vc[rhs][nc(n)][2cc+s]
+// Level::P_v at level 0 (src/level.cpp:182-209) added into psi (add = 1) or stored (add = 0):
+//   psi[rhs][n][s] (+)= sum_cc W[cc][n][s] vc[rhs][nc(n)][2cc+s]
 // Level::P_v at level 0 added into psi (src/level.cpp:182-209): psi[n][s] += sum_k W_k[n][s]
 // vc[nc][2k+s].  One thread per site; the site's KT >= ntest test-vector entries are loaded
 // once (BF16 -> T) and kept in registers for every source, so W streams from HBM once per
@@ -348,7 +348,7 @@ __global__ void k_restrict0_sum(const cx<T>* __restrict__ partial, cx<T>* __rest
 template <typename T, typename TW, int KT>
 __global__ void __launch_bounds__(256) k_prolong0_add(const TW* __restrict__ W, const cx<T>* __restrict__ vc,
                                                       cx<T>* __restrict__ psi, int nx, int nt, int bt, int xe,
-                                                      int te, int ntest, int nblk, int nrhs) {
+                                                      int te, int ntest, int nblk, int nrhs, int add) {
     const int N = nx * nt;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= N) return;
@@ -381,7 +381,7 @@ __global__ void __launch_bounds__(256) k_prolong0_add(const TW* __restrict__ W, 
                 }
             }
             float4* o4 = reinterpret_cast<float4*>(o);
-            float4 q = *o4;
+            float4 q = add ? *o4 : make_float4(0.f, 0.f, 0.f, 0.f);
             q.x += a0.x; q.y += a0.y; q.z += a1.x; q.w += a1.y;
             *o4 = q;
         } else {
@@ -392,8 +392,13 @@ __global__ void __launch_bounds__(256) k_prolong0_add(const TW* __restrict__ W, 
                     cfma(a1, w1[k], pv[2 * k + 1]);
                 }
             }
-            o[0] += a0;
-            o[1] += a1;
+            if (add) {
+                o[0] += a0;
+                o[1] += a1;
+            } else {
+                o[0] = a0;
+                o[1] = a1;
+            }
         }
     }
 }
@@ -978,7 +983,7 @@ cudaError_t launch_restrict0(const TW* W, const cx<T>* v, cx<T>* out, cx<T>* par
 
 template <typename T, typename TW>
 void launch_prolong0_add(const TW* W, const cx<T>* vc, cx<T>* psi, int nx, int nt, int bx, int bt, int ntest,
-                         int nrhs, cudaStream_t s) {
+                         int nrhs, cudaStream_t s, bool add) {
     count_launch(1);
     const int xe = nx / bx, te = nt / bt;
     if constexpr (std::is_same<T, float>::value && std::is_same<TW, __nv_bfloat162>::value) {
@@ -993,14 +998,15 @@ void launch_prolong0_add(const TW* W, const cx<T>* vc, cx<T>* psi, int nx, int n
             const int tiles = xe * (te / kPtcSites);
             const int nsplit = std::max(1, std::min(tiles, per_sm * sm_count() / nblk));
             dim3 grid(nsplit, nblk);
-            k_prolong0_tc<<<grid, kTcThreads, bytes, s>>>(W, vc, psi, nx, nt, bt, xe, te, ntest, nblk, nrhs, NP, nsplit);
+            k_prolong0_tc<<<grid, kTcThreads, bytes, s>>>(W, vc, psi, nx, nt, bt, xe, te, ntest, nblk, nrhs, NP, nsplit,
+                                                          add);
             return;
         }
     }
     const int grid = (nx * nt + 255) / 256;
-    if (ntest <= 8) k_prolong0_add<T, TW, 8><<<grid, 256, 0, s>>>(W, vc, psi, nx, nt, bt, xe, te, ntest, bx * bt, nrhs);
-    else if (ntest <= 16) k_prolong0_add<T, TW, 16><<<grid, 256, 0, s>>>(W, vc, psi, nx, nt, bt, xe, te, ntest, bx * bt, nrhs);
-    else k_prolong0_add<T, TW, 32><<<grid, 256, 0, s>>>(W, vc, psi, nx, nt, bt, xe, te, ntest, bx * bt, nrhs);
+    if (ntest <= 8) k_prolong0_add<T, TW, 8><<<grid, 256, 0, s>>>(W, vc, psi, nx, nt, bt, xe, te, ntest, bx * bt, nrhs, add);
+    else if (ntest <= 16) k_prolong0_add<T, TW, 16><<<grid, 256, 0, s>>>(W, vc, psi, nx, nt, bt, xe, te, ntest, bx * bt, nrhs, add);
+    else k_prolong0_add<T, TW, 32><<<grid, 256, 0, s>>>(W, vc, psi, nx, nt, bt, xe, te, ntest, bx * bt, nrhs, add);
 }
 
 template <typename T>
@@ -1426,10 +1432,10 @@ template cudaError_t launch_restrict0<float, float2>(const float2*, const cx<flo
 template cudaError_t launch_restrict0<float, __nv_bfloat162>(const __nv_bfloat162*, const cx<float>*, cx<float>*,
                                                        cx<float>*, int, int, int, int, int, int, int, cudaStream_t);
 template void launch_prolong0_add<double, double2>(const double2*, const cx<double>*, cx<double>*, int, int, int,
-                                                    int, int, int, cudaStream_t);
+                                                    int, int, int, cudaStream_t, bool);
 template void launch_prolong0_add<float, float2>(const float2*, const cx<float>*, cx<float>*, int, int, int, int,
-                                                  int, int, cudaStream_t);
+                                                  int, int, cudaStream_t, bool);
 template void launch_prolong0_add<float, __nv_bfloat162>(const __nv_bfloat162*, const cx<float>*, cx<float>*, int,
-                                                          int, int, int, int, int, cudaStream_t);
+                                                          int, int, int, int, int, cudaStream_t, bool);
 
 }  // namespace amgb

@@ -34,9 +34,10 @@ template <typename T, typename TW>
 cudaError_t launch_restrict0(const TW* W, const cx<T>* v, cx<T>* out, cx<T>* partial, int nx, int nt, int bx,
                              int bt, int ntest, int nrhs, int nchunk, cudaStream_t s);
 int smem_optin_bytes();
+// psi += P vc at level 0, or psi = P vc with add = false (psi is then written, never read)
 template <typename T, typename TW>
 void launch_prolong0_add(const TW* W, const cx<T>* vc, cx<T>* psi, int nx, int nt, int bx, int bt, int ntest,
-                         int nrhs, cudaStream_t s);
+                         int nrhs, cudaStream_t s, bool add = true);
 template <typename T>
 int sap0_smem_bytes(int S, int m, int use_smem);
 int sap0_warp_enabled();

@@ -373,7 +373,7 @@ __host__ __device__ constexpr int ptc_smem_bytes(int ntest, int NP) {
 __global__ void __launch_bounds__(kTcThreads) k_prolong0_tc(const __nv_bfloat162* __restrict__ W,
                                                      const float2* __restrict__ vc, float2* __restrict__ psi, int nx,
                                                      int nt, int bt, int xe, int te, int ntest, int nblk, int nrhs,
-                                                     int NP, int nsplit) {
+                                                     int NP, int nsplit, int add) {
     extern __shared__ __align__(128) unsigned char smraw_p[];
     constexpr int TPB = kTcThreads, KS = kPtcSites;
     const int N = nx * nt;
@@ -449,7 +449,7 @@ __global__ void __launch_bounds__(kTcThreads) k_prolong0_tc(const __nv_bfloat162
             float* p = pf;
 #pragma unroll
             for (int i = 0; i < 16; i++) {
-                old[i] = (c0 + i < c_hi) ? *p : 0.f;
+                old[i] = (add && c0 + i < c_hi) ? *p : 0.f;   // add = 0: psi is stored, not read
                 p += rs;
             }
             p = pf;
