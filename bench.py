@@ -61,9 +61,9 @@ BATCH_PER_SIZE, BATCH_RHS = 8, 32
 # restart cycle the Arnoldi steps j = 0..4, sum_j (60 + 32 (j + 1) + 8 + 4) = 840, the update
 # x += sum_j y_j V_j, 80, and the residual with its norm, 72.  72 + 5 * 992 = 5032.
 SAP_FLOPS_PER_SITE = 5032
-# DRAM bytes (read + write) of one fine SAP launch per (block, source) it solves, from the ncu
-# capture of this workload's SAP kernel at 32 sources (profiles/k_sap0_f32_dram_1024x1024_r32.md:
-# 542.37 MB read + 227.01 MB written by a launch of 16384 block-sources).
+# DRAM bytes (read + write) of one fine SAP launch per (block, source) it solves, from an ncu
+# capture (dram__bytes_read.sum, dram__bytes_write.sum) of this workload's SAP kernel at 32
+# sources: 542.37 MB read + 227.01 MB written by a launch of 16384 block-sources.
 SAP_DRAM_BYTES_PER_BLOCK_SOURCE = (542.37e6 + 227.01e6) / 16384
 FP32_LANES_PER_SM = 128
 
